@@ -1,0 +1,181 @@
+"""imops_b200 -- B200 (sm_100a) raw-development path of DavRack/imops.
+
+The product is the C-ABI shared library ``libimops_b200.so`` built from
+``imops_b200/csrc`` (see ``include/imops_b200.h``).  This module loads it
+with ctypes and offers thin torch wrappers over the device entry points.
+There is no CPU fallback: without the library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libimops_b200.so")
+_lib = None
+
+OK = 0
+ERRORS = {
+    1: "invalid argument", 2: "unsupported CFA", 3: "unsupported size", 4: "CUDA error", 5: "out of memory",
+    6: "wrong color space", 7: "invalid dimensions", 8: "invalid stock", 9: "config error", 10: "not implemented",
+    11: "timeout",
+}
+CS_CAMERA, CS_XYZD65, CS_LINEAR_SRGB, CS_SRGB, CS_ACESCG = -1, 0, 1, 2, 3
+DEMOSAIC_AMAZE, DEMOSAIC_MARKESTEIJN, DEMOSAIC_FAST, DEMOSAIC_SUPERFAST, DEMOSAIC_SUPERSUPERFAST = range(5)
+
+
+class ImopsError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"imops_b200 error {code} ({ERRORS.get(code, '?')}): {message}")
+        self.code = code
+        self.message = message
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C-ABI library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python imops_b200/build.py` (or __graft_entry__.build())")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.imops_last_error.restype = ctypes.c_char_p
+        _lib.imops_version.restype = ctypes.c_char_p
+    return _lib
+
+
+def last_error() -> str:
+    return (lib().imops_last_error() or b"").decode()
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise ImopsError(rc, last_error())
+
+
+def version() -> str:
+    return lib().imops_version().decode()
+
+
+def _stream(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _require_cuda_f32(t, name: str):
+    import torch
+    if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+        raise ValueError(f"{name} must be a contiguous float32 CUDA tensor")
+
+
+def _cfa(pattern: str) -> bytes:
+    return pattern.encode()
+
+
+def demosaic_amaze(mosaic, cfa: str = "RGGB", shift=(0, 0), clip_pt: float = 1.0, out=None, stream=None):
+    """AMaZE (demosaic.rs:358-1379) on a (H, W) float32 CUDA mosaic -> (H, W, 3)."""
+    import torch
+    _require_cuda_f32(mosaic, "mosaic")
+    H, W = mosaic.shape
+    out = out if out is not None else torch.empty((H, W, 3), device=mosaic.device, dtype=torch.float32)
+    f = lib().imops_demosaic_amaze
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(mosaic), W, H, _cfa(cfa), shift[0], shift[1], clip_pt, _ptr(out), _stream(stream)))
+    return out
+
+
+def amaze_size_supported(W: int, H: int) -> bool:
+    f = lib().imops_amaze_size_supported
+    f.argtypes = [ctypes.c_int, ctypes.c_int]
+    return bool(f(W, H))
+
+
+def demosaic_markesteijn(mosaic, cfa: str, shift=(0, 0), out=None, stream=None):
+    import torch
+    _require_cuda_f32(mosaic, "mosaic")
+    H, W = mosaic.shape
+    out = out if out is not None else torch.empty((H, W, 3), device=mosaic.device, dtype=torch.float32)
+    f = lib().imops_demosaic_markesteijn
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(mosaic), W, H, _cfa(cfa), shift[0], shift[1], _ptr(out), _stream(stream)))
+    return out
+
+
+def demosaic_quad(mosaic, cfa: str, factor: int, shift=(0, 0), stream=None):
+    import torch
+    _require_cuda_f32(mosaic, "mosaic")
+    H, W = mosaic.shape
+    out = torch.empty((H // factor, W // factor, 3), device=mosaic.device, dtype=torch.float32)
+    f = lib().imops_demosaic_quad
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(mosaic), W, H, _cfa(cfa), shift[0], shift[1], factor, _ptr(out), _stream(stream)))
+    return out
+
+
+def scale_u16(raw, crop, black, white, period=(2, 2), out=None, stream=None):
+    """raw: (Hr, Wr) uint16 CUDA tensor (stored as int16/uint16); crop = (x, y, w, h)."""
+    import torch
+    x, y, w, h = crop
+    pw, ph = period
+    n = pw * ph
+    bl = (ctypes.c_float * n)(*([float(b) for b in black] if hasattr(black, "__len__") else [float(black)] * n))
+    wh = (ctypes.c_float * n)(*([float(v) for v in white] if hasattr(white, "__len__") else [float(white)] * n))
+    out = out if out is not None else torch.empty((h, w), device=raw.device, dtype=torch.float32)
+    f = lib().imops_scale_u16
+    f.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 6 + [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                           ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(raw), raw.shape[1], raw.shape[0], x, y, w, h, bl, wh, pw, ph, _ptr(out), _stream(stream)))
+    return out
+
+
+def cfa_coeffs(rgb, wb, stream=None):
+    _require_cuda_f32(rgb, "rgb")
+    c = (ctypes.c_float * 4)(*(list(wb) + [0.0] * (4 - len(wb))))
+    f = lib().imops_cfa_coeffs
+    f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(rgb), rgb.numel() // 3, c, _stream(stream)))
+    return rgb
+
+
+def exp(rgb, ev: float, stream=None):
+    _require_cuda_f32(rgb, "rgb")
+    f = lib().imops_exp
+    f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_float, ctypes.c_void_p]
+    check(f(_ptr(rgb), rgb.numel() // 3, ev, _stream(stream)))
+    return rgb
+
+
+def baseline_exposure(rgb, baseline_ev: float, shutter: float, f_number: float, iso: float, stream=None) -> bool:
+    _require_cuda_f32(rgb, "rgb")
+    applied = ctypes.c_int(0)
+    f = lib().imops_baseline_exposure
+    f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                  ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
+    check(f(_ptr(rgb), rgb.numel() // 3, baseline_ev, shutter, f_number, iso, ctypes.byref(applied),
+            _stream(stream)))
+    return bool(applied.value)
+
+
+def camera_forward_matrix(calib):
+    c = (ctypes.c_float * 9)(*[float(v) for v in calib])
+    out = (ctypes.c_float * 9)()
+    f = lib().imops_camera_forward_matrix
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    check(f(c, out))
+    return [out[i] for i in range(9)]
+
+
+def camera_cst(rgb, calib, target: int, stream=None):
+    _require_cuda_f32(rgb, "rgb")
+    c = (ctypes.c_float * 9)(*[float(v) for v in calib])
+    f = lib().imops_camera_cst
+    f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    check(f(_ptr(rgb), rgb.numel() // 3, c, target, _stream(stream)))
+    return rgb

@@ -1,0 +1,63 @@
+// common.cuh -- shared helpers of the imops_b200 CUDA library: status codes,
+// the thread-local last-error string, CUDA checks and the CFA descriptor
+// handed to kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "imops_b200.h"
+
+namespace imops {
+
+// Thread-local last error (the reference keeps one in LAST_ERROR,
+// pichromatic-pipeline/src/extern_pipeline.rs:18-38).
+void set_error(const std::string& msg);
+void clear_error();
+const char* last_error();
+
+// Returns `code` after recording `msg`.
+int fail(int code, const std::string& msg);
+
+// Converts a CUDA error into IMOPS_ERR_CUDA (or OK).
+int cuda_status(cudaError_t e, const char* what);
+
+#define IMOPS_CUDA_TRY(call, what)                                  \
+    do {                                                            \
+        cudaError_t _e = (call);                                    \
+        if (_e != cudaSuccess) return ::imops::cuda_status(_e, what); \
+    } while (0)
+
+// Device-side CFA period (up to 12x12 cells, colour 0=R 1=G 2=B).
+struct CfaDev {
+    int pw, ph;
+    uint8_t col[144];
+    __host__ __device__ __forceinline__ int at(int r, int c) const {
+        int rr = r % ph;
+        if (rr < 0) rr += ph;
+        int cc = c % pw;
+        if (cc < 0) cc += pw;
+        return col[rr * pw + cc];
+    }
+};
+
+// Parses a CFA pattern string the way CFA::new does (cfa.rs:98-129) and
+// applies CFA::shift (cfa.rs:204-233).  Returns IMOPS_OK or an error code.
+int parse_cfa(const char* pattern, int shift_x, int shift_y, CfaDev* out);
+
+// Whether a CFA is a 2x2 Bayer period with greens on one diagonal.
+bool cfa_is_bayer(const CfaDev& c);
+
+// Current stream as a cudaStream_t.
+inline cudaStream_t as_stream(imops_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+// Host-side fault injection for failure-path tests: when the environment
+// variable IMOPS_FAULT_INJECT names `site` ("alloc", "launch"), the call
+// reports a failure instead of touching the GPU.
+bool fault_injected(const char* site);
+
+}  // namespace imops

@@ -1,0 +1,131 @@
+/*
+ * imops_b200.h -- C-ABI of the B200 (sm_100a) raw-development library.
+ *
+ * Drop-in boundary for the hot path of DavRack/imops (a Rust project): each
+ * entry point replaces one stage the reference runs on the CPU and names the
+ * reference interface (file:line, paths inside the reference project) whose
+ * behaviour it reproduces.  Plain pointers and sizes only.
+ *
+ * Conventions
+ *  - Every call returns an int status (IMOPS_OK == 0).  On failure the
+ *    reason is kept in a thread-local string read by imops_last_error(), the
+ *    counterpart of get_last_error_c (pichromatic-pipeline/src/extern_pipeline.rs:27-38).
+ *  - Stage entry points (imops_*) take DEVICE pointers and run on the
+ *    caller's CUDA stream (imops_stream_t is a cudaStream_t; NULL = legacy
+ *    default stream).  They allocate nothing unless documented.
+ *  - Images are row-major; RGB is interleaved f32 [r,g,b] per pixel, the
+ *    reference's Image.rgb_data layout (pichromatic/src/pixel.rs:23-27);
+ *    mosaics are one f32 per site, Image.raw_data.
+ *  - CFA patterns are strings as CFA::new takes them ("RGGB", 36-char
+ *    X-Trans, ...; pichromatic/src/cfa.rs:98-129); shift_x/shift_y apply
+ *    CFA::shift (cfa.rs:204-233) for a crop origin.
+ */
+#ifndef IMOPS_B200_H
+#define IMOPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *imops_stream_t;
+
+/* Status codes. */
+#define IMOPS_OK 0
+#define IMOPS_ERR_INVALID_ARGUMENT 1
+#define IMOPS_ERR_UNSUPPORTED_CFA 2
+#define IMOPS_ERR_UNSUPPORTED_SIZE 3
+#define IMOPS_ERR_CUDA 4
+#define IMOPS_ERR_OUT_OF_MEMORY 5
+#define IMOPS_ERR_WRONG_COLOR_SPACE 6   /* FilmError::WrongColorSpace (film/error.rs:5-13) */
+#define IMOPS_ERR_INVALID_DIMENSIONS 7  /* FilmError::InvalidDimensions */
+#define IMOPS_ERR_INVALID_STOCK 8       /* FilmError::InvalidStock */
+#define IMOPS_ERR_CONFIG 9              /* config::parse_config failures (config.rs:13-34) */
+#define IMOPS_ERR_NOT_IMPLEMENTED 10    /* a module that stays on the reference (BM3D, ...) */
+#define IMOPS_ERR_TIMEOUT 11            /* a bounded device wait gave up */
+
+/* Colour spaces (subset of the `color` crate's ColorSpaceTag used on the path). */
+#define IMOPS_CS_CAMERA (-1)            /* Image.metadata.color_space == None */
+#define IMOPS_CS_XYZD65 0
+#define IMOPS_CS_LINEAR_SRGB 1
+#define IMOPS_CS_SRGB 2
+#define IMOPS_CS_ACESCG 3
+
+/* Demosaic algorithms: DemosaicAlgorithmType (pichromatic-pipeline/src/modules.rs:72-104). */
+#define IMOPS_DEMOSAIC_AMAZE 0
+#define IMOPS_DEMOSAIC_MARKESTEIJN 1
+#define IMOPS_DEMOSAIC_FAST 2
+#define IMOPS_DEMOSAIC_SUPERFAST 3
+#define IMOPS_DEMOSAIC_SUPERSUPERFAST 4
+
+/* Thread-local message of the last failed call (or "" after a success).
+ * Replaces get_last_error_c (extern_pipeline.rs:27-38); the string is owned
+ * by the library and valid until the next call on the same thread. */
+const char *imops_last_error(void);
+
+/* Library version string. */
+const char *imops_version(void);
+
+/* ---- decode-side normalisation ------------------------------------------
+ * Black/white scaling of a u16 sensor frame plus the crop copy.  Replaces
+ * RawImage::apply_scaling (rawler 0.7, called at extern_pipeline.rs:263) and
+ * demosaic::crop_and_normalize (pichromatic/src/demosaic.rs:61-91):
+ * out[y][x] = (raw[cy+y][cx+x] - black[s]) / (white[s] - black[s]),
+ * s = ((cy+y) % period_h) * period_w + (cx+x) % period_w (full-frame CFA cell).
+ * black/white are HOST arrays of period_w*period_h values. */
+int imops_scale_u16(const uint16_t *raw, int raw_w, int raw_h, int crop_x, int crop_y, int crop_w, int crop_h,
+                    const float *black, const float *white, int period_w, int period_h, float *out,
+                    imops_stream_t stream);
+
+/* ---- demosaic -------------------------------------------------------------
+ * AMaZE, bit-identical to demosaic_algorithms::Amaze (demosaic.rs:358-1379)
+ * including its 128x128/96-stride tiling.  Requires a 2x2 Bayer CFA;
+ * returns IMOPS_ERR_UNSUPPORTED_SIZE for image sizes where the reference's
+ * tile fill writes past its tile buffer (the reference panics there).
+ * mosaic: w*h f32; rgb: w*h*3 f32. */
+int imops_demosaic_amaze(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y, float clip_pt,
+                         float *rgb, imops_stream_t stream);
+
+/* Whether imops_demosaic_amaze accepts a w x h image (host-only check). */
+int imops_amaze_size_supported(int w, int h);
+
+/* 3x3 same-colour mean, demosaic_algorithms::Markesteijn (demosaic.rs:108-186);
+ * any CFA period up to 12x12 (Bayer, X-Trans). */
+int imops_demosaic_markesteijn(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y,
+                               float *rgb, imops_stream_t stream);
+
+/* Quad-sampling previews Fast / SuperFast / SuperSuperFast (demosaic.rs:189-356):
+ * factor 2, 4 or 8; rgb holds (w/factor)*(h/factor)*3 floats. */
+int imops_demosaic_quad(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y, int factor,
+                        float *rgb, imops_stream_t stream);
+
+/* ---- per-pixel colour ------------------------------------------------------ */
+
+/* White balance after demosaic: rgb *= wb[0..3] (cfa_coeffs.rs:4-12). */
+int imops_cfa_coeffs(float *rgb, size_t n_pixels, const float wb[4], imops_stream_t stream);
+
+/* Exposure: rgb *= 2^ev (exp.rs:4-11). */
+int imops_exp(float *rgb, size_t n_pixels, float ev, imops_stream_t stream);
+
+/* BaselineExposureCompensation (pichromatic-pipeline/src/modules.rs:335-373):
+ * 2^baseline_ev when |ev| > 1e-6, then the absolute-luminance gain
+ * 12.5*N^2/(t*S) when shutter, f_number and iso are all > 0.  *applied
+ * (may be NULL) receives 1 when the gain was applied. */
+int imops_baseline_exposure(float *rgb, size_t n_pixels, float baseline_ev, float shutter_seconds, float f_number,
+                            float iso, int *applied, imops_stream_t stream);
+
+/* Camera RGB -> XYZ(D65) forward matrix of camera_cst (cst.rs:12-38, 51-95),
+ * computed on the host in f32 exactly as the reference does. */
+int imops_camera_forward_matrix(const float calib_d65[9], float forward[9]);
+
+/* camera_cst (cst.rs:12-48): xyz = forward * rgb, then XYZ(D65) -> target
+ * (IMOPS_CS_*).  calib_d65: the 3x3 row-major calibration matrix. */
+int imops_camera_cst(float *rgb, size_t n_pixels, const float calib_d65[9], int target, imops_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMOPS_B200_H */

@@ -1,0 +1,1160 @@
+/*
+ * film.c -- CPU oracle for the spectral film simulation.
+ *
+ * TEST INFRASTRUCTURE (see oracle_common.h).
+ *
+ * Part 1 restates the reference's film::process (pichromatic/src/film/mod.rs:77-129)
+ * for the stocks ColorNeg200 (film/stock/color_neg_200.rs:38-208) and BwStub
+ * (film/stock/bw_stub.rs:18-82), keeping the reference's precision mix:
+ * per-pixel spectral work in f64 (exposure/mod.rs:68-81, scan/densitometry.rs:13-73),
+ * planes, blurs, development and grain in f32.  With ORACLE_F32 the f32 parts
+ * run in f32 (reference order); without it every step runs in f64 (the FP64
+ * oracle used for error reporting).
+ *
+ * Part 2 is the "baseline" preset: the 81-bin (380-780 nm, 5 nm), 3-layer,
+ * logistic-curve, red-highlight-halation, seeded-grain stock this library
+ * defines for the throughput workload.  The reference has no such stock, so
+ * its only oracle is this file; it integrates every pixel over all 81 bins
+ * (no rank-3 collapse), which checks the GPU's collapsed exposure.
+ */
+#include "oracle_common.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef ORACLE_F32
+#define REXP expf
+#define RPOW powf
+#define RSQRT sqrtf
+#define RCEIL ceilf
+#else
+#define REXP exp
+#define RPOW pow
+#define RSQRT sqrt
+#define RCEIL ceil
+#endif
+
+#define NB 16          /* reference grid: 400..700 nm step 20 */
+#define MAXL 8
+
+/* ----------------------------------------------------------------------- */
+/* constants (film/constants.rs:14-67, upsample.rs:17-45, pixel.rs:33-36)   */
+
+static const double CMF_X[NB] = {0.01431, 0.13438, 0.34828, 0.29080, 0.09564, 0.00490, 0.06327, 0.29040,
+                                 0.59450, 0.91630, 1.06220, 0.85445, 0.44790, 0.16490, 0.04677, 0.01136};
+static const double CMF_Y[NB] = {0.000396, 0.004000, 0.023000, 0.060000, 0.139020, 0.323000, 0.710000, 0.954000,
+                                 0.995000, 0.870000, 0.631000, 0.381000, 0.175000, 0.061000, 0.017000, 0.004100};
+static const double CMF_Z[NB] = {0.06785, 0.64560, 1.74706, 1.66920, 0.81295, 0.27200, 0.07825, 0.02030,
+                                 0.00390, 0.00165, 0.00080, 0.00019, 0.00002, 0.00000, 0.00000, 0.00000};
+static const double XYZ2AP1[3][3] = {{1.6410233797, -0.3248032942, -0.2364246952},
+                                     {-0.6636628587, 1.6153315917, 0.0167563477},
+                                     {0.0117218943, -0.0082844165, 0.9883948585}};
+#define LUM_R K(0.2722287168)
+#define LUM_G K(0.6740817658)
+#define LUM_B K(0.0536895174)
+#define MIDDLE_GRAY K(0.185)
+
+static double grid_nm(int i) { return 400.0 + 20.0 * i; }
+
+static void matvec3(const double m[3][3], const double v[3], double o[3])
+{
+    for (int i = 0; i < 3; i++) o[i] = m[i][0] * v[0] + m[i][1] * v[1] + m[i][2] * v[2];
+}
+
+/* inv3 of upsample.rs:57-79 (cofactor form). */
+static void inv3(const double m[3][3], double r[3][3])
+{
+    double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                 m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    double id = 1.0 / det;
+    r[0][0] = (m[1][1] * m[2][2] - m[1][2] * m[2][1]) * id;
+    r[0][1] = (m[0][2] * m[2][1] - m[0][1] * m[2][2]) * id;
+    r[0][2] = (m[0][1] * m[1][2] - m[0][2] * m[1][1]) * id;
+    r[1][0] = (m[1][2] * m[2][0] - m[1][0] * m[2][2]) * id;
+    r[1][1] = (m[0][0] * m[2][2] - m[0][2] * m[2][0]) * id;
+    r[1][2] = (m[0][2] * m[1][0] - m[0][0] * m[1][2]) * id;
+    r[2][0] = (m[1][0] * m[2][1] - m[1][1] * m[2][0]) * id;
+    r[2][1] = (m[0][1] * m[2][0] - m[0][0] * m[2][1]) * id;
+    r[2][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) * id;
+}
+
+static double integrate_cmf(const double *s, const double *cmf)
+{
+    double acc = 0.0;
+    for (int i = 0; i < NB - 1; i++) {
+        double a = s[i] * cmf[i];
+        double b = s[i + 1] * cmf[i + 1];
+        acc += 0.5 * (a + b) * 20.0;
+    }
+    return acc;
+}
+
+/* spectrum_to_acescg (upsample.rs:101-112). */
+static void spectrum_to_ap1(const double *s, double out[3])
+{
+    double xyz[3] = {integrate_cmf(s, CMF_X), integrate_cmf(s, CMF_Y), integrate_cmf(s, CMF_Z)};
+    matvec3(XYZ2AP1, xyz, out);
+}
+
+/* UpsampleBasis (upsample.rs:114-158): three Gaussians 450/550/650, sigma 40. */
+typedef struct { double b[3][NB]; double minv[3][3]; } Basis;
+
+static void basis_build(Basis *B)
+{
+    const double peaks[3] = {450.0, 550.0, 650.0};
+    double cols[3][3], m[3][3];
+    for (int k = 0; k < 3; k++) {
+        for (int i = 0; i < NB; i++) {
+            double d = (grid_nm(i) - peaks[k]) / 40.0;
+            B->b[k][i] = exp(-0.5 * d * d);
+        }
+        spectrum_to_ap1(B->b[k], cols[k]);
+    }
+    for (int r = 0; r < 3; r++)
+        for (int k = 0; k < 3; k++) m[r][k] = cols[k][r];
+    inv3(m, B->minv);
+}
+
+/* upsample_acescg + pixel_fluence_spectrum (upsample.rs:136-170,
+ * exposure/mod.rs:124-137). */
+static void fluence_spectrum(const Basis *B, const real rgb[3], double out[NB])
+{
+    double v[3] = {(double)(float)rgb[0], (double)(float)rgb[1], (double)(float)rgb[2]};
+#ifndef ORACLE_F32
+    v[0] = rgb[0]; v[1] = rgb[1]; v[2] = rgb[2];
+#endif
+    double w[3];
+    matvec3(B->minv, v, w);
+    for (int k = 0; k < 3; k++)
+        if (w[k] < 0.0) w[k] = 0.0;
+    for (int i = 0; i < NB; i++) {
+        double s = w[0] * B->b[0][i] + w[1] * B->b[1][i] + w[2] * B->b[2][i];
+        double e_rel = 550.0 / grid_nm(i);
+        out[i] = s / e_rel;
+    }
+}
+
+/* ----------------------------------------------------------------------- */
+/* stocks                                                                   */
+
+enum { LK_EMULSION, LK_FILTER, LK_OVERCOAT, LK_AH, LK_SUPPORT };
+
+typedef struct {
+    int kind;
+    float thickness;
+    int has_sens;
+    double sens[NB];
+    double mu_ln, sigma_ln;
+    float fraction;
+    double eps[NB];
+    int has_mask;
+    double mask_eps[NB];
+    float dmax;
+    float gamma;
+    double capture_k;
+    float recip_p;
+    int reversal;
+    double lut_log[64], lut_frac[64];
+    float kappa;
+} OLayer;
+
+typedef struct {
+    float box_iso;
+    int nl;
+    OLayer l[MAXL];
+    double refl[NB];
+    float psf_local, psf_halation;
+    float dev_diff, adj_beta, dir_diff;
+    int dir_n;
+    float dir[MAXL][MAXL];
+    double scanner[NB];
+} OStock;
+
+static void gaussian_curve(double peak, double sigma, double amp, double *s)
+{
+    for (int i = 0; i < NB; i++) {
+        double d = (grid_nm(i) - peak) / sigma;
+        s[i] = amp * exp(-0.5 * d * d);
+    }
+}
+
+static void orange_mask(double *s)
+{
+    for (int i = 0; i < NB; i++) {
+        double l = grid_nm(i);
+        double bd = (l - 450.0) / 50.0, gd = (l - 520.0) / 60.0;
+        double blue = exp(-0.5 * (bd * bd));
+        double green = 0.6 * exp(-0.5 * (gd * gd));
+        s[i] = 0.35 * blue + 0.25 * green + 0.05;
+    }
+}
+
+/* E_s[exp(-k s^2 phi)] with 64-node trapezoid over z (capture.rs:91-106). */
+static double expected_survival(double mu, double sig, double k, double phi)
+{
+    const int N = 64;
+    const double ZMAX = 8.0;
+    double dz = (2.0 * ZMAX) / (double)N;
+    double isq = 1.0 / sqrt(2.0 * 3.14159265358979323846);
+    double acc = 0.0;
+    for (int i = 0; i <= N; i++) {
+        double z = -ZMAX + (double)i * dz;
+        double tw = (i == 0 || i == N) ? 0.5 : 1.0;
+        double pdf = isq * exp(-0.5 * z * z);
+        double s = exp(mu + sig * z);
+        double g = exp(-k * s * s * phi);
+        acc += tw * pdf * g * dz;
+    }
+    return acc;
+}
+
+/* DevelopableFractionLut::build (capture.rs:37-58). */
+static void lut_build(OLayer *L)
+{
+    for (int i = 0; i < 64; i++) {
+        double t = (double)i / 63.0;
+        double lp = -4.0 + t * (8.0 - -4.0);
+        double phi = pow(10.0, lp);
+        double f = 1.0 - expected_survival(L->mu_ln, L->sigma_ln, L->capture_k, phi);
+        if (f < 0.0) f = 0.0;
+        if (f > 1.0) f = 1.0;
+        L->lut_log[i] = lp;
+        L->lut_frac[i] = f;
+    }
+}
+
+/* DevelopableFractionLut::sample (capture.rs:61-88). */
+static double lut_sample(const OLayer *L, double phi)
+{
+    if (!(phi > 0.0)) return L->lut_frac[0];
+    double lp = log10(phi);
+    if (lp <= L->lut_log[0]) return L->lut_frac[0];
+    if (lp >= L->lut_log[63]) return L->lut_frac[63];
+    int lo = 0, hi = 63;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) / 2;
+        if (L->lut_log[mid] <= lp) lo = mid; else hi = mid;
+    }
+    double t = (lp - L->lut_log[lo]) / (L->lut_log[hi] - L->lut_log[lo]);
+    return L->lut_frac[lo] * (1.0 - t) + L->lut_frac[hi] * t;
+}
+
+/* FilmStock::finalize grain kappa (stock/mod.rs:193-211). */
+static float layer_kappa(const OLayer *L)
+{
+    double mean_s = exp(L->mu_ln + 0.5 * L->sigma_ln * L->sigma_ln);
+    double r = mean_s * 0.5;
+    if (r < 1e-6) r = 1e-6;
+    double vol = 1.04719755119659774615421446109316763 * 4.0 * r * r * r; /* FRAC_PI_3 */
+    double rho = (double)L->fraction * (double)L->thickness / (vol > 1e-18 ? vol : 1e-18);
+    return (float)(1.0 / sqrt(rho));
+}
+
+static void finalize(OStock *S)
+{
+    for (int i = 0; i < S->nl; i++)
+        if (S->l[i].kind == LK_EMULSION) {
+            lut_build(&S->l[i]);
+            S->l[i].kappa = layer_kappa(&S->l[i]);
+        }
+}
+
+static void absorber(OLayer *L, int kind, float thick, double peak, double sig, double amp)
+{
+    memset(L, 0, sizeof(*L));
+    L->kind = kind;
+    L->thickness = thick;
+    L->has_sens = 1;
+    gaussian_curve(peak, sig, amp, L->sens);
+    L->gamma = 1.0f;
+    L->capture_k = 1.0;
+    L->recip_p = 1.0f;
+}
+
+static void emulsion(OLayer *L, float thick, double speak, double ssig, double mean_um, double sig_ln, double epeak,
+                     double esig, float gamma, double k, float p)
+{
+    memset(L, 0, sizeof(*L));
+    L->kind = LK_EMULSION;
+    L->thickness = thick;
+    L->has_sens = 1;
+    gaussian_curve(speak, ssig, 1.0, L->sens);
+    L->mu_ln = log(mean_um);
+    L->sigma_ln = sig_ln;
+    L->fraction = 0.18f;
+    gaussian_curve(epeak, esig, 1.0, L->eps);
+    L->has_mask = 1;
+    orange_mask(L->mask_eps);
+    L->dmax = 2.2f;
+    L->gamma = gamma;
+    L->capture_k = k;
+    L->recip_p = p;
+}
+
+/* ColorNeg200 (film/stock/color_neg_200.rs:67-208). */
+static void stock_colorneg200(OStock *S)
+{
+    memset(S, 0, sizeof(*S));
+    S->box_iso = 200.0f;
+    S->nl = 6;
+    absorber(&S->l[0], LK_OVERCOAT, 1.0f, 0, 1, 0);
+    for (int i = 0; i < NB; i++) S->l[0].sens[i] = 0.01;
+    emulsion(&S->l[1], 4.0f, 450.0, 35.0, 0.55, 0.30, 450.0, 40.0, 0.65f, 4.2, 0.88f);
+    absorber(&S->l[2], LK_FILTER, 2.0f, 430.0, 40.0, 1.2);
+    emulsion(&S->l[3], 5.0f, 550.0, 40.0, 0.60, 0.32, 550.0, 40.0, 0.65f, 2.1, 0.90f);
+    emulsion(&S->l[4], 6.0f, 650.0, 45.0, 0.70, 0.35, 650.0, 45.0, 0.65f, 1.35, 0.92f);
+    absorber(&S->l[5], LK_AH, 2.0f, 650.0, 80.0, 0.3);
+    gaussian_curve(680.0, 60.0, 0.08, S->refl);
+    S->psf_local = 3.0f;
+    S->psf_halation = 80.0f;
+    S->dev_diff = 8.0f;
+    S->adj_beta = 0.35f;
+    S->dir_diff = 15.0f;
+    S->dir_n = 3;
+    const float dm[3][3] = {{0.02f, 0.05f, 0.03f}, {0.05f, 0.02f, 0.06f}, {0.03f, 0.06f, 0.02f}};
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) S->dir[i][j] = dm[i][j];
+    for (int i = 0; i < NB; i++) S->scanner[i] = 1.0;
+    finalize(S);
+}
+
+/* BwStub (film/stock/bw_stub.rs:18-82). */
+static void stock_bwstub(OStock *S)
+{
+    memset(S, 0, sizeof(*S));
+    S->box_iso = 100.0f;
+    S->nl = 1;
+    OLayer *L = &S->l[0];
+    L->kind = LK_EMULSION;
+    L->thickness = 10.0f;
+    L->has_sens = 1;
+    for (int i = 0; i < NB; i++) {
+        double t = (grid_nm(i) - 400.0) / 300.0;
+        double env = sin(3.14159265358979323846 * t);
+        if (env < 0.0) env = 0.0;
+        L->sens[i] = 0.3 + 0.7 * env;
+        L->eps[i] = 1.0;
+    }
+    L->mu_ln = log(0.7);
+    L->sigma_ln = 0.35;
+    L->fraction = 0.2f;
+    L->has_mask = 0;
+    L->dmax = 2.5f;
+    L->gamma = 0.65f;
+    L->capture_k = 1.0;
+    L->recip_p = 1.0f;
+    for (int i = 0; i < NB; i++) S->refl[i] = 0.0;
+    S->psf_local = 2.0f;
+    S->psf_halation = 40.0f;
+    S->dev_diff = 5.0f;
+    S->adj_beta = 0.3f;
+    S->dir_diff = 10.0f;
+    S->dir_n = 1;
+    S->dir[0][0] = 0.0f;
+    for (int i = 0; i < NB; i++) S->scanner[i] = 1.0;
+    finalize(S);
+}
+
+static int load_stock(int id, OStock *S)
+{
+    if (id == 0) { stock_bwstub(S); return 1; }
+    if (id == 1) { stock_colorneg200(S); return 1; }
+    return 0;
+}
+
+/* ----------------------------------------------------------------------- */
+/* separable Gaussian blur (film/blur.rs:10-89)                              */
+
+static long reflect_index(long i, long n)
+{
+    if (n == 0) return 0;
+    long x = i;
+    for (;;) {
+        if (x < 0) x = -x;
+        else if (x >= n) x = 2 * n - 2 - x;
+        else return x;
+        if (n == 1) return 0;
+    }
+}
+
+/* Gaussian taps: radius max(ceil(3 sigma), 1), normalised to sum 1. */
+static int blur_kernel(real sigma, real **out)
+{
+    real r3 = RCEIL(K(3.0) * sigma);
+    if (r3 < K(1.0)) r3 = K(1.0);
+    int radius = (int)r3;
+    real *k = (real *)malloc(sizeof(real) * (2 * radius + 1));
+    real inv = K(1.0) / (K(2.0) * sigma * sigma);
+    real sum = K(0.0);
+    for (int i = 0; i < 2 * radius + 1; i++) {
+        real x = (real)i - (real)radius;
+        real v = REXP(-x * x * inv);
+        k[i] = v;
+        sum += v;
+    }
+    for (int i = 0; i < 2 * radius + 1; i++) k[i] /= sum;
+    *out = k;
+    return radius;
+}
+
+/* Horizontal then vertical 1-D passes with mirror reflection.  `radius_override`
+ * >= 0 fixes the tap radius (the baseline preset's halation). */
+static void blur_taps(real *buf, int W, int H, const real *k, int radius)
+{
+    size_t n = (size_t)W * H;
+    real *tmp = (real *)malloc(sizeof(real) * n);
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            real acc = K(0.0);
+            for (int t = 0; t < 2 * radius + 1; t++) {
+                long xx = reflect_index((long)x + t - radius, W);
+                acc += buf[(size_t)y * W + xx] * k[t];
+            }
+            tmp[(size_t)y * W + x] = acc;
+        }
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            real acc = K(0.0);
+            for (int t = 0; t < 2 * radius + 1; t++) {
+                long yy = reflect_index((long)y + t - radius, H);
+                acc += tmp[(size_t)yy * W + x] * k[t];
+            }
+            buf[(size_t)y * W + x] = acc;
+        }
+    free(tmp);
+}
+
+void OSYM(oracle_blur)(real *buf, int W, int H, real sigma)
+{
+    if (sigma < K(1e-3) || W == 0 || H == 0) return;
+    real *k;
+    int radius = blur_kernel(sigma, &k);
+    blur_taps(buf, W, H, k, radius);
+    free(k);
+}
+
+/* Gaussian taps of the baseline preset's halation: fixed radius, so the
+ * output is a smooth function of sigma. */
+static void fixed_radius_taps(real sigma, int radius, real *k)
+{
+    real inv = K(1.0) / (K(2.0) * sigma * sigma);
+    real sum = K(0.0);
+    for (int i = 0; i < 2 * radius + 1; i++) {
+        real x = (real)i - (real)radius;
+        real v = REXP(-x * x * inv);
+        k[i] = v;
+        sum += v;
+    }
+    for (int i = 0; i < 2 * radius + 1; i++) k[i] /= sum;
+}
+
+/* ----------------------------------------------------------------------- */
+/* SplitMix64 + Irwin-Hall noise (film/development/grain.rs:20-45, 71-82)   */
+
+static inline uint64_t splitmix_next(uint64_t *s)
+{
+    *s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = *s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static inline real irwin_hall(uint64_t *s)
+{
+    real acc = K(0.0);
+    for (int i = 0; i < 12; i++) {
+#ifdef ORACLE_F32
+        acc += (float)splitmix_next(s) / (float)UINT64_MAX;
+#else
+        acc += (double)splitmix_next(s) / (double)UINT64_MAX;
+#endif
+    }
+    return acc - K(6.0);
+}
+
+void OSYM(oracle_grain_noise)(real *noise, int W, int H, uint64_t seed, int layer)
+{
+    for (int y = 0; y < H; y++) {
+        uint64_t s = seed * 0xD1B54A32D192ED03ull + (uint64_t)layer * 0x9E3779B97F4A7C15ull + (uint64_t)y;
+        for (int x = 0; x < W; x++) noise[(size_t)y * W + x] = irwin_hall(&s);
+    }
+}
+
+/* blurred unit-variance noise plane (grain.rs:69-90): returns norm */
+static real grain_field(real *noise, int W, int H, uint64_t seed, int layer, real sigma_px)
+{
+    OSYM(oracle_grain_noise)(noise, W, H, seed, layer);
+    OSYM(oracle_blur)(noise, W, H, sigma_px > K(1.0) ? sigma_px : K(1.0));
+    size_t n = (size_t)W * H;
+    double var = 0.0;
+    for (size_t i = 0; i < n; i++) var += (double)noise[i] * (double)noise[i];
+    var /= (double)n;
+    return var > 1e-12 ? (real)(float)(1.0 / sqrt(var)) : K(1.0);
+}
+
+/* ----------------------------------------------------------------------- */
+/* film::process for the reference stocks                                    */
+
+typedef struct {
+    int E;
+    int em_idx[MAXL];
+} EmList;
+
+static EmList emulsions(const OStock *S)
+{
+    EmList e;
+    e.E = 0;
+    for (int i = 0; i < S->nl; i++)
+        if (S->l[i].kind == LK_EMULSION) e.em_idx[e.E++] = i;
+    return e;
+}
+
+static double curve_eval(const double *s, double lam)
+{
+    if (lam <= grid_nm(0)) return s[0];
+    if (lam >= grid_nm(NB - 1)) return s[NB - 1];
+    for (int i = 0; i < NB - 1; i++)
+        if (lam >= grid_nm(i) && lam <= grid_nm(i + 1)) {
+            double t = (lam - grid_nm(i)) / (grid_nm(i + 1) - grid_nm(i));
+            return s[i] * (1.0 - t) + s[i + 1] * t;
+        }
+    return s[NB - 1];
+}
+
+static double curve_integrate(const double *s)
+{
+    double acc = 0.0;
+    for (int i = 0; i < NB - 1; i++) acc += 0.5 * (s[i] + s[i + 1]) * (grid_nm(i + 1) - grid_nm(i));
+    return acc;
+}
+
+static double curve_peak(const double *s)
+{
+    double mv = -INFINITY, pk = 550.0;
+    for (int i = 0; i < NB; i++)
+        if (s[i] > mv) { mv = s[i]; pk = grid_nm(i); }
+    return pk;
+}
+
+/* Emulsion absorbed band-mean fluence per pixel (exposure/mod.rs:45-81,
+ * absorption.rs:24-108) into E planes of `real`. */
+static void expose_absorb(const OStock *S, const Basis *B, const real *rgb, size_t n, real **planes)
+{
+    EmList em = emulsions(S);
+    for (size_t p = 0; p < n; p++) {
+        double phi[NB];
+        fluence_spectrum(B, rgb + 3 * p, phi);
+        int e = 0;
+        for (int li = 0; li < S->nl; li++) {
+            const OLayer *L = &S->l[li];
+            double ab[NB];
+            memset(ab, 0, sizeof ab);
+            if (L->kind == LK_EMULSION) {
+                double rho = (double)L->fraction, th = (double)L->thickness;
+                for (int i = 0; i < NB; i++) {
+                    double sigma = L->sens[i] * 2.0;
+                    double od = sigma * rho * th;
+                    double tr = exp(-od);
+                    double pt = phi[i] * tr;
+                    ab[i] = phi[i] - pt;
+                    phi[i] = pt;
+                }
+            } else if (L->kind != LK_SUPPORT && L->has_sens) {
+                double th = (double)L->thickness;
+                for (int i = 0; i < NB; i++) {
+                    double od = L->sens[i] * th;
+                    double tr = exp(-od);
+                    double pt = phi[i] * tr;
+                    ab[i] = phi[i] - pt;
+                    phi[i] = pt;
+                }
+            }
+            if (L->kind == LK_EMULSION) {
+                double acc = 0.0;
+                for (int i = 0; i < NB - 1; i++) acc += 0.5 * (ab[i] + ab[i + 1]) * 20.0;
+                planes[e][p] = (real)(float)(acc / 300.0);
+#ifndef ORACLE_F32
+                planes[e][p] = acc / 300.0;
+#endif
+                e++;
+            }
+        }
+        (void)em;
+    }
+}
+
+/* Local scatter + wide support bounce (halation.rs:24-93). */
+static void spatial_effects(const OStock *S, real **planes, int E, int W, int H, real pitch)
+{
+    size_t n = (size_t)W * H;
+    real pm = pitch > K(1e-6) ? pitch : K(1e-6);
+    real s_loc = (real)S->psf_local / pm;
+    if (s_loc < 0) s_loc = 0;
+    const real mix = K(0.18);
+    if (s_loc >= K(1e-3)) {
+        real *tmp = (real *)malloc(sizeof(real) * n);
+        for (int e = 0; e < E; e++) {
+            memcpy(tmp, planes[e], sizeof(real) * n);
+            OSYM(oracle_blur)(tmp, W, H, s_loc);
+            real keep = K(1.0) - mix;
+            for (size_t p = 0; p < n; p++) planes[e][p] = keep * planes[e][p] + mix * tmp[p];
+        }
+        free(tmp);
+    }
+    real s_wide = (real)S->psf_halation / pm;
+    if (s_wide < 0) s_wide = 0;
+    if (s_wide < K(1e-3)) return;
+    const double bands[4] = {450.0, 550.0, 650.0, 700.0};
+    real maxr = K(0.0);
+    for (int b = 0; b < 4; b++) {
+        real r = (real)(float)curve_eval(S->refl, bands[b]);
+        maxr = RMAX(maxr, r);
+    }
+    if (maxr <= K(0.0)) return;
+    EmList em = emulsions(S);
+    real *bounce = (real *)malloc(sizeof(real) * n);
+    memcpy(bounce, planes[E - 1], sizeof(real) * n);
+    OSYM(oracle_blur)(bounce, W, H, s_wide);
+    const real bw[3] = {K(0.20), K(0.45), K(1.0)};
+    for (int e = 0; e < E; e++) {
+        const OLayer *L = &S->l[em.em_idx[e]];
+        double pk = curve_peak(L->sens);
+        real w;
+        if (pk <= 450.0) w = bw[0];
+        else if (pk <= 550.0) w = bw[0] + (bw[1] - bw[0]) * (real)(float)((pk - 450.0) / 100.0);
+        else if (pk <= 650.0) w = bw[1] + (bw[2] - bw[1]) * (real)(float)((pk - 550.0) / 100.0);
+        else w = bw[2];
+        double norm = curve_integrate(L->sens);
+        real r_e;
+        if (norm <= 1e-9) {
+            r_e = (real)(float)curve_eval(S->refl, 650.0);
+        } else {
+            double prod[NB];
+            for (int i = 0; i < NB; i++) prod[i] = S->refl[i] * L->sens[i];
+            r_e = (real)(float)(curve_integrate(prod) / norm);
+        }
+        real gain = r_e * w;
+        if (gain <= K(0.0)) continue;
+        for (size_t p = 0; p < n; p++) planes[e][p] += gain * bounce[p];
+    }
+    free(bounce);
+}
+
+static double reciprocity(double t, double p)
+{
+    if (t <= 1.0 || p >= 0.9999) return 1.0;
+    return pow(t > 1.0 ? t : 1.0, p - 1.0);
+}
+
+typedef struct { real *img[MAXL]; real *mask[MAXL]; } Dyes;
+
+/* expose -> develop (reduce, DIR, adjacency, grain): exposure/mod.rs:45-122,
+ * development/mod.rs:18-48. */
+static void expose_develop(const OStock *S, const Basis *B, const real *rgb, int W, int H, real pitch, real shutter,
+                           uint64_t seed, int grain_on, Dyes *D)
+{
+    size_t n = (size_t)W * H;
+    EmList em = emulsions(S);
+    int E = em.E;
+    real *lat[MAXL];
+    for (int e = 0; e < E; e++) lat[e] = (real *)calloc(n, sizeof(real));
+    expose_absorb(S, B, rgb, n, lat);
+    spatial_effects(S, lat, E, W, H, pitch);
+    for (int e = 0; e < E; e++) {
+        const OLayer *L = &S->l[em.em_idx[e]];
+        real eta = (real)(float)reciprocity((double)(float)shutter, (double)L->recip_p);
+        for (size_t p = 0; p < n; p++) {
+            real prod = lat[e][p] * eta;
+            lat[e][p] = (real)(float)lut_sample(L, (double)prod);
+#ifndef ORACLE_F32
+            lat[e][p] = lut_sample(L, (double)prod);
+#endif
+        }
+    }
+    /* reduce (reduction.rs:16-68) */
+    for (int e = 0; e < E; e++) {
+        const OLayer *L = &S->l[em.em_idx[e]];
+        real dmax = (real)L->dmax;
+        real gam = RMAX((real)L->gamma, K(1e-6));
+        real ig = K(1.0) / gam;
+        D->img[e] = (real *)malloc(sizeof(real) * n);
+        D->mask[e] = (real *)malloc(sizeof(real) * n);
+        for (size_t p = 0; p < n; p++) {
+            real f = lat[e][p];
+            if (f < K(0.0)) f = K(0.0);
+            if (f > K(1.0)) f = K(1.0);
+            real ef = L->reversal ? K(1.0) - f : f;
+            D->img[e][p] = dmax * RPOW(ef, ig);
+        }
+        if (L->has_mask) {
+            real ms = dmax * K(0.4);
+            for (size_t p = 0; p < n; p++) {
+                real r = D->img[e][p] / dmax;
+                if (r < K(0.0)) r = K(0.0);
+                if (r > K(1.0)) r = K(1.0);
+                D->mask[e][p] = ms * (K(1.0) - r);
+            }
+        } else {
+            memset(D->mask[e], 0, sizeof(real) * n);
+        }
+        free(lat[e]);
+    }
+    real pm = pitch > K(1e-6) ? pitch : K(1e-6);
+    /* DIR inhibition (diffusion.rs:39-84) */
+    real s_dir = (real)S->dir_diff / pm;
+    if (E > 0 && S->dir_n > 0 && s_dir >= K(1e-3)) {
+        real *inh[MAXL];
+        for (int i = 0; i < E; i++) {
+            inh[i] = (real *)malloc(sizeof(real) * n);
+            memcpy(inh[i], D->img[i], sizeof(real) * n);
+            OSYM(oracle_blur)(inh[i], W, H, s_dir);
+        }
+        real *tot = (real *)malloc(sizeof(real) * n);
+        for (int j = 0; j < E; j++) {
+            memset(tot, 0, sizeof(real) * n);
+            int active = 0;
+            for (int i = 0; i < E; i++) {
+                if (i < S->dir_n && j < S->dir_n) {
+                    real w = (real)S->dir[i][j];
+                    if (RABS(w) > K(1e-6)) {
+                        active = 1;
+                        for (size_t p = 0; p < n; p++) tot[p] += w * inh[i][p];
+                    }
+                }
+            }
+            if (active)
+                for (size_t p = 0; p < n; p++) D->img[j][p] *= REXP(-tot[p]);
+        }
+        free(tot);
+        for (int i = 0; i < E; i++) free(inh[i]);
+    }
+    /* adjacency (diffusion.rs:11-28) */
+    real s_adj = (real)S->dev_diff / pm;
+    real beta = (real)S->adj_beta;
+    if (!(RABS(beta) < K(1e-8) || s_adj < K(1e-3))) {
+        real *bl = (real *)malloc(sizeof(real) * n);
+        for (int e = 0; e < E; e++) {
+            memcpy(bl, D->img[e], sizeof(real) * n);
+            OSYM(oracle_blur)(bl, W, H, s_adj);
+            for (size_t p = 0; p < n; p++) D->img[e][p] += beta * (D->img[e][p] - bl[p]);
+        }
+        free(bl);
+    }
+    /* grain (grain.rs:53-100) */
+    if (grain_on) {
+        real s_g = K(3.0) / pm;
+        real *noise = (real *)malloc(sizeof(real) * n);
+        for (int e = 0; e < E; e++) {
+            const OLayer *L = &S->l[em.em_idx[e]];
+            real dmax = (real)L->dmax;
+            real kappa = ((real)L->kappa / pm) * K(0.15);
+            if (kappa <= K(0.0) || dmax <= K(0.0)) continue;
+            real norm = grain_field(noise, W, H, seed, e, s_g);
+            for (size_t p = 0; p < n; p++) {
+                real d = D->img[e][p];
+                real dens = d < K(0.0) ? K(0.0) : (d > dmax ? dmax : d);
+                real toe = K(0.02) * dmax;
+                real taper = RMIN(dens / (dens + toe), K(1.0));
+                real sd = taper * RSQRT(RMAX(dens * (dmax - dens), K(0.0)));
+                d = dens + kappa * sd * noise[p] * norm;
+                real hi = dmax * K(1.05);
+                if (d < K(0.0)) d = K(0.0);
+                if (d > hi) d = hi;
+                D->img[e][p] = d;
+            }
+        }
+        free(noise);
+    }
+}
+
+/* density -> transmittance -> AP1 for one pixel (densitometry.rs:13-73). */
+static void scan_pixel(const OStock *S, const real *di, const real *dm, double out[3])
+{
+    EmList em = emulsions(S);
+    double d[NB];
+    memset(d, 0, sizeof d);
+    for (int e = 0; e < em.E; e++) {
+        const OLayer *L = &S->l[em.em_idx[e]];
+        double a = (double)di[e], m = (double)dm[e];
+        for (int i = 0; i < NB; i++) {
+            d[i] += a * L->eps[i];
+            if (L->has_mask) d[i] += m * L->mask_eps[i];
+        }
+    }
+    double t[NB];
+    for (int i = 0; i < NB; i++) t[i] = pow(10.0, -d[i]) * S->scanner[i];
+    spectrum_to_ap1(t, out);
+}
+
+static void dmin_rgb(const OStock *S, double out[3])
+{
+    EmList em = emulsions(S);
+    real di[MAXL], dm[MAXL];
+    for (int e = 0; e < em.E; e++) {
+        const OLayer *L = &S->l[em.em_idx[e]];
+        di[e] = K(0.0);
+        dm[e] = L->has_mask ? (real)L->dmax * K(0.4) : K(0.0);
+    }
+    scan_pixel(S, di, dm, out);
+}
+
+static void scan_all(const OStock *S, const Dyes *D, int E, size_t n, real *rgb)
+{
+    double dmn[3];
+    dmin_rgb(S, dmn);
+    double peak = dmn[0] > dmn[1] ? dmn[0] : dmn[1];
+    if (dmn[2] > peak) peak = dmn[2];
+    if (peak < 1e-12) peak = 1e-12;
+    double scale = 1.0 / peak;
+    for (size_t p = 0; p < n; p++) {
+        real di[MAXL], dm[MAXL];
+        for (int e = 0; e < E; e++) { di[e] = D->img[e][p]; dm[e] = D->mask[e][p]; }
+        double o[3];
+        scan_pixel(S, di, dm, o);
+        for (int c = 0; c < 3; c++) {
+            float raw = (float)o[c];
+            rgb[3 * p + c] = (real)(float)((double)raw * scale);
+#ifndef ORACLE_F32
+            rgb[3 * p + c] = o[c] * scale;
+#endif
+        }
+    }
+}
+
+static real soft_inv(real inv, real shoulder)
+{
+    real i = RMAX(inv, K(0.0));
+    real s = RMAX(shoulder, K(1e-6));
+    return i / (K(1.0) + i / s);
+}
+
+/* invert_negative (scan/invert.rs:36-108). */
+void OSYM(oracle_invert)(real *buf, size_t n, const real mid[3], const real dmin_in[3])
+{
+    const real eps = K(1e-6), HEAD = K(8.0), KEEP = K(0.55), FADE = K(0.02);
+    real dmin[3], mt[3], im[3], sh[3], sm[3], g[3];
+    for (int c = 0; c < 3; c++) {
+        dmin[c] = RMAX(dmin_in[c], eps);
+        real v = mid[c] / dmin[c];
+        if (v < eps) v = eps;
+        if (v > K(1.0) - eps) v = K(1.0) - eps;
+        mt[c] = v;
+        im[c] = RMAX(K(1.0) / mt[c] - K(1.0), K(0.0));
+        sh[c] = RMAX(im[c] * HEAD, eps);
+    }
+    for (int c = 0; c < 3; c++) {
+        sm[c] = RMAX(soft_inv(im[c], sh[c]), eps);
+        g[c] = MIDDLE_GRAY / sm[c];
+    }
+    for (size_t p = 0; p < n; p++) {
+        real *px = buf + 3 * p;
+        real raw[3];
+        for (int c = 0; c < 3; c++) {
+            real t = px[c] / dmin[c];
+            if (t < eps) t = eps;
+            if (t > K(1.0)) t = K(1.0);
+            real inv = RMAX(K(1.0) / t - K(1.0), K(0.0));
+            raw[c] = RMAX(g[c] * soft_inv(inv, sh[c]), K(0.0));
+        }
+        real y = RMAX(LUM_R * raw[0] + LUM_G * raw[1] + LUM_B * raw[2], K(0.0));
+        real k;
+        if (y <= K(0.0)) k = K(0.0);
+        else if (y >= FADE) k = KEEP;
+        else k = KEEP * (y / FADE);
+        for (int c = 0; c < 3; c++) px[c] = RMAX(y + k * (raw[c] - y), K(0.0));
+    }
+}
+
+static void free_dyes(Dyes *D, int E)
+{
+    for (int e = 0; e < E; e++) { free(D->img[e]); free(D->mask[e]); }
+}
+
+/* relative -> absolute luminance at sunny-16 for a box ISO (film/mod.rs:155-166). */
+static real rel_to_abs_y(real y, real box_iso)
+{
+    float s = (float)box_iso > 1.0f ? (float)box_iso : 1.0f;
+    float t = 1.0f / s;
+    double l = 12.5 * (double)(float)y * (8.0 * 8.0) / ((double)t * (double)s);
+    return (real)(float)l;
+}
+
+/* film::process.  stock: 0 BwStub, 1 ColorNeg200.  format: 0 35mm, 1 6x6,
+ * 2 4x5.  output: 0 NegativeLinear, 1 PositiveLinear.  shutter < 0 means
+ * "not in metadata" (1 / box ISO).  grain_on = 0 skips grain (parity mode). */
+int OSYM(oracle_film_process)(real *rgb, int W, int H, int stock_id, int format, uint64_t seed, int output,
+                              real shutter, int grain_on)
+{
+    if (W <= 0 || H <= 0 || !rgb) return ORACLE_ERR_ARG;
+    OStock S;
+    if (!load_stock(stock_id, &S)) return ORACLE_ERR_ARG;
+    const float fw[3] = {36.0f, 56.0f, 101.6f};
+    if (format < 0 || format > 2) return ORACLE_ERR_ARG;
+    real pitch = (real)(fw[format] * 1000.0f / (float)W);
+#ifndef ORACLE_F32
+    pitch = (double)fw[format] * 1000.0 / (double)W;
+#endif
+    real sh = shutter >= 0 ? shutter : (real)(1.0f / S.box_iso);
+    Basis B;
+    basis_build(&B);
+    size_t n = (size_t)W * H;
+    EmList em = emulsions(&S);
+    Dyes D;
+    expose_develop(&S, &B, rgb, W, H, pitch, sh, seed, grain_on, &D);
+    scan_all(&S, &D, em.E, n, rgb);
+    free_dyes(&D, em.E);
+    int reversal = 0;
+    for (int i = 0; i < S.nl; i++) reversal |= S.l[i].reversal;
+    if (!reversal && output == 1) {
+        double dmn[3];
+        dmin_rgb(&S, dmn);
+        double pk = dmn[0] > dmn[1] ? dmn[0] : dmn[1];
+        if (dmn[2] > pk) pk = dmn[2];
+        if (pk < 1e-12) pk = 1e-12;
+        real dmin[3] = {(real)(float)(dmn[0] / pk), (real)(float)(dmn[1] / pk), (real)(float)(dmn[2] / pk)};
+        /* mid-gray negative: 32x32 patch through the same path, seed 0 */
+        const int NM = 32;
+        real g = rel_to_abs_y(MIDDLE_GRAY, (real)S.box_iso);
+        real *patch = (real *)malloc(sizeof(real) * NM * NM * 3);
+        for (int i = 0; i < NM * NM * 3; i++) patch[i] = g;
+        Dyes Dm;
+        expose_develop(&S, &B, patch, NM, NM, pitch, sh, 0, grain_on, &Dm);
+        scan_all(&S, &Dm, em.E, (size_t)NM * NM, patch);
+        free_dyes(&Dm, em.E);
+        double acc[3] = {0, 0, 0};
+        for (int i = 0; i < NM * NM; i++)
+            for (int c = 0; c < 3; c++) acc[c] += (double)patch[3 * i + c];
+        real mid[3];
+        for (int c = 0; c < 3; c++) mid[c] = (real)(float)(acc[c] / (double)(NM * NM));
+        free(patch);
+        OSYM(oracle_invert)(rgb, n, mid, dmin);
+    }
+    return ORACLE_OK;
+}
+
+/* Exposed for known-answer tests. */
+double OSYM(oracle_lut_sample)(int stock_id, int layer, double phi)
+{
+    OStock S;
+    if (!load_stock(stock_id, &S)) return NAN;
+    EmList em = emulsions(&S);
+    if (layer < 0 || layer >= em.E) return NAN;
+    return lut_sample(&S.l[em.em_idx[layer]], phi);
+}
+
+float OSYM(oracle_layer_kappa)(int stock_id, int layer)
+{
+    OStock S;
+    if (!load_stock(stock_id, &S)) return NAN;
+    EmList em = emulsions(&S);
+    if (layer < 0 || layer >= em.E) return NAN;
+    return S.l[em.em_idx[layer]].kappa;
+}
+
+/* Normalised film-base RGB (densitometry.rs:109-117). */
+void OSYM(oracle_normalized_dmin)(int stock_id, real out[3])
+{
+    OStock S;
+    load_stock(stock_id, &S);
+    double d[3];
+    dmin_rgb(&S, d);
+    double pk = d[0] > d[1] ? d[0] : d[1];
+    if (d[2] > pk) pk = d[2];
+    if (pk < 1e-12) pk = 1e-12;
+    for (int c = 0; c < 3; c++) out[c] = (real)(float)(d[c] / pk);
+}
+
+/* Upsample one ACEScg pixel and integrate back to ACEScg (round trip used
+ * by upsample.rs:187-224's tests). */
+void OSYM(oracle_upsample_roundtrip)(const real rgb[3], double spectrum[NB], double back[3])
+{
+    Basis B;
+    basis_build(&B);
+    double v[3] = {(double)rgb[0], (double)rgb[1], (double)rgb[2]}, w[3];
+    matvec3(B.minv, v, w);
+    for (int k = 0; k < 3; k++)
+        if (w[k] < 0.0) w[k] = 0.0;
+    for (int i = 0; i < NB; i++) spectrum[i] = w[0] * B.b[0][i] + w[1] * B.b[1][i] + w[2] * B.b[2][i];
+    spectrum_to_ap1(spectrum, back);
+}
+
+/* ======================================================================= */
+/* Part 2: the baseline preset (81 bins, logistic curves, red-highlight     */
+/* halation, seeded grain).                                                  */
+
+#define NB81 81
+
+/* CIE 1931 2-degree observer, multi-lobe Gaussian fit of Wyman, Sloan and
+ * Shirley, "Simple Analytic Approximations to the CIE XYZ Color Matching
+ * Functions", JCGT 2(2), 2013. */
+static double lobe(double x, double mu, double s1, double s2)
+{
+    double t = (x - mu) / (x < mu ? s1 : s2);
+    return exp(-0.5 * t * t);
+}
+
+void OSYM(oracle_cmf81)(double *xb, double *yb, double *zb)
+{
+    for (int i = 0; i < NB81; i++) {
+        double l = 380.0 + 5.0 * i;
+        xb[i] = 1.056 * lobe(l, 599.8, 37.9, 31.0) + 0.362 * lobe(l, 442.0, 16.0, 26.7) -
+                0.065 * lobe(l, 501.1, 20.4, 26.2);
+        yb[i] = 0.821 * lobe(l, 568.8, 46.9, 40.5) + 0.286 * lobe(l, 530.9, 16.3, 31.1);
+        zb[i] = 1.217 * lobe(l, 437.0, 11.8, 36.0) + 0.681 * lobe(l, 459.0, 26.0, 13.8);
+    }
+}
+
+/* Parameters of the baseline preset; the struct layout is shared with the
+ * CUDA library's ImopsBaselineFilm (include/imops_b200.h). */
+typedef struct {
+    float dmax[3], k[3], x0[3];   /* logistic density curve per layer */
+    float hal_strength;           /* 0.15 */
+    float hal_sigma;              /* 20 px */
+    int hal_radius;               /* fixed tap radius (64) */
+    float hal_threshold;          /* 0.8 on ACEScg red */
+    float grain_sigma;            /* 0.02 density */
+    float grain_blur;             /* 1 px */
+    int grain_on;
+    uint64_t seed;
+} OBaseline;
+
+static const double SENS_PEAK[3] = {450.0, 550.0, 650.0}, SENS_SIG[3] = {35.0, 40.0, 45.0};
+static const double DYE_PEAK[3] = {450.0, 550.0, 650.0}, DYE_SIG[3] = {40.0, 40.0, 45.0};
+static const double BLEED[3] = {0.20, 0.45, 1.0};
+
+typedef struct {
+    double lam[NB81], trap[NB81];
+    double xb[NB81], yb[NB81], zb[NB81];
+    double basis[3][NB81], minv[3][3];
+    double sens[3][NB81], sens_norm[3];
+    double dye[3][NB81];
+    double white[3];
+} B81;
+
+static void b81_build(B81 *b)
+{
+    OSYM(oracle_cmf81)(b->xb, b->yb, b->zb);
+    for (int i = 0; i < NB81; i++) {
+        b->lam[i] = 380.0 + 5.0 * i;
+        b->trap[i] = (i == 0 || i == NB81 - 1) ? 2.5 : 5.0;
+    }
+    double cols[3][3];
+    for (int k = 0; k < 3; k++) {
+        double x = 0, y = 0, z = 0;
+        for (int i = 0; i < NB81; i++) {
+            double d = (b->lam[i] - SENS_PEAK[k]) / 40.0;
+            b->basis[k][i] = exp(-0.5 * d * d);
+            x += b->trap[i] * b->basis[k][i] * b->xb[i];
+            y += b->trap[i] * b->basis[k][i] * b->yb[i];
+            z += b->trap[i] * b->basis[k][i] * b->zb[i];
+        }
+        double xyz[3] = {x, y, z};
+        matvec3(XYZ2AP1, xyz, cols[k]);
+    }
+    double m[3][3];
+    for (int r = 0; r < 3; r++)
+        for (int k = 0; k < 3; k++) m[r][k] = cols[k][r];
+    inv3(m, b->minv);
+    /* flat reference exposure: the upsampled spectrum of ACEScg (1,1,1) */
+    double one[3] = {1, 1, 1}, w1[3];
+    matvec3(b->minv, one, w1);
+    for (int e = 0; e < 3; e++) {
+        double nrm = 0;
+        for (int i = 0; i < NB81; i++) {
+            double d = (b->lam[i] - SENS_PEAK[e]) / SENS_SIG[e];
+            b->sens[e][i] = exp(-0.5 * d * d);
+            double s1 = 0;
+            for (int k = 0; k < 3; k++) s1 += (w1[k] > 0 ? w1[k] : 0) * b->basis[k][i];
+            nrm += b->trap[i] * s1 * b->sens[e][i];
+        }
+        b->sens_norm[e] = nrm;
+        for (int i = 0; i < NB81; i++) {
+            double d = (b->lam[i] - DYE_PEAK[e]) / DYE_SIG[e];
+            b->dye[e][i] = exp(-0.5 * d * d);
+        }
+    }
+    double x = 0, y = 0, z = 0;
+    for (int i = 0; i < NB81; i++) {
+        x += b->trap[i] * b->xb[i];
+        y += b->trap[i] * b->yb[i];
+        z += b->trap[i] * b->zb[i];
+    }
+    double xyz[3] = {x, y, z};
+    matvec3(XYZ2AP1, xyz, b->white);
+}
+
+/* Forward of the baseline preset on an ACEScg image (relative scene-linear).
+ * Output: scanned negative ACEScg normalised so that D = 0 maps to a peak
+ * channel of 1.
+ *   w   = max(0, Minv rgb)                        basis weights
+ *   s   = sum_k w_k basis_k(lambda)                81-bin spectrum
+ *   a_e = sum_i trap_i s_i S_e,i / N_e             layer exposure (1 for rgb=1)
+ *   h   = max(0, R - threshold);  B = G_sigma * h  halation (fixed radius)
+ *   E_e = a_e + strength * bleed_e * B
+ *   D_e = Dmax_e / (1 + exp(-k_e (log10 max(E_e,1e-6) - x0_e)))
+ *   D_e += grain_sigma * n_e * norm_e              (seeded SplitMix64 noise)
+ *   T   = 10^(-sum_e D_e dye_e(lambda));  rgb = AP1(sum_i trap_i cmf_i T_i) / peak(white)
+ */
+int OSYM(oracle_film_baseline)(real *rgb, int W, int H, const OBaseline *P)
+{
+    if (!rgb || !P || W <= 0 || H <= 0) return ORACLE_ERR_ARG;
+    B81 b;
+    b81_build(&b);
+    size_t n = (size_t)W * H;
+    real *a[3], *hal = (real *)malloc(sizeof(real) * n);
+    for (int e = 0; e < 3; e++) a[e] = (real *)malloc(sizeof(real) * n);
+    for (size_t p = 0; p < n; p++) {
+        double v[3] = {(double)rgb[3 * p], (double)rgb[3 * p + 1], (double)rgb[3 * p + 2]}, w[3];
+        matvec3(b.minv, v, w);
+        for (int k = 0; k < 3; k++)
+            if (w[k] < 0) w[k] = 0;
+        for (int e = 0; e < 3; e++) {
+            double acc = 0;
+            for (int i = 0; i < NB81; i++) {
+                double s = w[0] * b.basis[0][i] + w[1] * b.basis[1][i] + w[2] * b.basis[2][i];
+                acc += b.trap[i] * s * b.sens[e][i];
+            }
+            a[e][p] = (real)(acc / b.sens_norm[e]);
+        }
+        real h = rgb[3 * p] - (real)P->hal_threshold;
+        hal[p] = h > 0 ? h : 0;
+    }
+    int R = P->hal_radius;
+    real *taps = (real *)malloc(sizeof(real) * (2 * R + 1));
+    fixed_radius_taps((real)P->hal_sigma, R, taps);
+    blur_taps(hal, W, H, taps, R);
+    free(taps);
+    real *noise[3] = {NULL, NULL, NULL};
+    real norm[3] = {0, 0, 0};
+    if (P->grain_on)
+        for (int e = 0; e < 3; e++) {
+            noise[e] = (real *)malloc(sizeof(real) * n);
+            norm[e] = grain_field(noise[e], W, H, P->seed, e, (real)P->grain_blur);
+        }
+    double peak = b.white[0] > b.white[1] ? b.white[0] : b.white[1];
+    if (b.white[2] > peak) peak = b.white[2];
+    for (size_t p = 0; p < n; p++) {
+        double D[3];
+        for (int e = 0; e < 3; e++) {
+            double E = (double)a[e][p] + (double)P->hal_strength * BLEED[e] * (double)hal[p];
+            double le = log10(E > 1e-6 ? E : 1e-6);
+            D[e] = (double)P->dmax[e] / (1.0 + exp(-(double)P->k[e] * (le - (double)P->x0[e])));
+            if (P->grain_on) D[e] += (double)P->grain_sigma * (double)noise[e][p] * (double)norm[e];
+        }
+        double x = 0, y = 0, z = 0;
+        for (int i = 0; i < NB81; i++) {
+            double d = D[0] * b.dye[0][i] + D[1] * b.dye[1][i] + D[2] * b.dye[2][i];
+            double t = pow(10.0, -d);
+            x += b.trap[i] * b.xb[i] * t;
+            y += b.trap[i] * b.yb[i] * t;
+            z += b.trap[i] * b.zb[i] * t;
+        }
+        double xyz[3] = {x, y, z}, o[3];
+        matvec3(XYZ2AP1, xyz, o);
+        for (int c = 0; c < 3; c++) rgb[3 * p + c] = (real)(o[c] / peak);
+    }
+    for (int e = 0; e < 3; e++) { free(a[e]); free(noise[e]); }
+    free(hal);
+    return ORACLE_OK;
+}
