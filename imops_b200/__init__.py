@@ -179,3 +179,55 @@ def camera_cst(rgb, calib, target: int, stream=None):
     f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
     check(f(_ptr(rgb), rgb.numel() // 3, c, target, _stream(stream)))
     return rgb
+
+
+# ---- film -------------------------------------------------------------------
+
+STOCK_BWSTUB, STOCK_COLORNEG200, STOCK_BASELINE81 = 0, 1, 100
+FORMAT_35MM, FORMAT_6X6, FORMAT_4X5 = 0, 1, 2
+FILM_NEGATIVE_LINEAR, FILM_POSITIVE_LINEAR = 0, 1
+
+
+class FilmParams(ctypes.Structure):
+    """ImopsFilmParams (include/imops_b200.h)."""
+
+    _fields_ = [("stock", ctypes.c_int), ("film_format", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("output", ctypes.c_int), ("shutter_seconds", ctypes.c_float), ("grain", ctypes.c_int)]
+
+
+class BaselineFilm(ctypes.Structure):
+    """ImopsBaselineFilm (include/imops_b200.h)."""
+
+    _fields_ = [("dmax", ctypes.c_float * 3), ("k", ctypes.c_float * 3), ("x0", ctypes.c_float * 3),
+                ("hal_strength", ctypes.c_float), ("hal_sigma", ctypes.c_float), ("hal_radius", ctypes.c_int),
+                ("hal_threshold", ctypes.c_float), ("grain_sigma", ctypes.c_float), ("grain_blur", ctypes.c_float),
+                ("grain_on", ctypes.c_int), ("seed", ctypes.c_uint64)]
+
+
+def baseline_film_defaults(**overrides) -> BaselineFilm:
+    p = BaselineFilm()
+    f = lib().imops_baseline_film_defaults
+    f.argtypes = [ctypes.POINTER(BaselineFilm)]
+    f(ctypes.byref(p))
+    for k, v in overrides.items():
+        if k in ("dmax", "k", "x0"):
+            for i in range(3):
+                getattr(p, k)[i] = v[i]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def film_process(rgb, stock: int = STOCK_COLORNEG200, film_format: int = FORMAT_35MM, seed: int = 1,
+                 output: int = FILM_NEGATIVE_LINEAR, shutter: float = -1.0, grain: bool = True,
+                 baseline: BaselineFilm | None = None, color_space: int = CS_ACESCG, stream=None):
+    """film::process (film/mod.rs:77-129) in place on an (H, W, 3) float32 CUDA image."""
+    _require_cuda_f32(rgb, "rgb")
+    H, W = rgb.shape[:2]
+    p = FilmParams(stock, film_format, seed, output, shutter, int(grain))
+    f = lib().imops_film_process
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(FilmParams),
+                  ctypes.c_void_p, ctypes.c_void_p]
+    bptr = ctypes.byref(baseline) if baseline is not None else None
+    check(f(_ptr(rgb), W, H, color_space, ctypes.byref(p), bptr, _stream(stream)))
+    return rgb

@@ -1,0 +1,633 @@
+// film.cu -- spectral film simulation kernels and imops_film_process.
+//
+// Reference model (film::process, pichromatic/src/film/mod.rs:77-129) as a
+// chain of planar kernels:
+//   expose (rank-3 spectral collapse) -> local scatter -> support bounce ->
+//   capture LUT -> reduce -> DIR -> adjacency -> grain -> 16-bin scan ->
+//   [invert].
+// Baseline preset (81 bins): expose + halation source -> halation row pass
+// -> grain noise -> one fused kernel doing the halation column pass, the
+// logistic curves, grain and the 81-bin scan.
+//
+// Layout: per-layer planes (row-major f32), so every pass is a coalesced
+// stream; RGB stays interleaved as in Image.rgb_data.
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "film.cuh"
+
+namespace imops {
+namespace film {
+
+constexpr int MAXR = 64;  // largest blur radius handled (129 taps)
+
+struct Taps {
+    int R;
+    float t[2 * MAXR + 1];
+};
+
+__device__ __forceinline__ int reflect(int i, int n) {
+    // blur.rs:70-89: mirror without repeating the edge sample
+    if (n == 1) return 0;
+    int x = i;
+    for (;;) {
+        if (x < 0) x = -x;
+        else if (x >= n) x = 2 * n - 2 - x;
+        else return x;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// exposure
+
+// rgb (interleaved) -> E planes of absorbed band-mean fluence, optional
+// halation source plane max(0, R - threshold).
+__global__ void expose_kernel(const float* __restrict__ rgb, size_t n, ExposeSpec X, float* __restrict__ planes,
+                              float* __restrict__ hal) {
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        float r = rgb[3 * p], g = rgb[3 * p + 1], b = rgb[3 * p + 2];
+        float w0 = fmaxf(0.0f, X.minv[0] * r + X.minv[1] * g + X.minv[2] * b);
+        float w1 = fmaxf(0.0f, X.minv[3] * r + X.minv[4] * g + X.minv[5] * b);
+        float w2 = fmaxf(0.0f, X.minv[6] * r + X.minv[7] * g + X.minv[8] * b);
+        for (int e = 0; e < X.E; e++) planes[e * n + p] = w0 * X.A[0][e] + w1 * X.A[1][e] + w2 * X.A[2][e];
+        if (X.hal_src) hal[p] = fmaxf(0.0f, r - X.hal_threshold);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// separable Gaussian blur with mirror reflection (blur.rs:10-89)
+
+constexpr int ROW_TILE = 256;
+
+__global__ void blur_rows_kernel(const float* __restrict__ in, float* __restrict__ out, int W, int H, Taps tp) {
+    __shared__ float s[ROW_TILE + 2 * MAXR];
+    int y = blockIdx.y;
+    int x0 = blockIdx.x * ROW_TILE;
+    const float* row = in + (size_t)y * W;
+    int span = ROW_TILE + 2 * tp.R;
+    for (int j = threadIdx.x; j < span; j += blockDim.x) s[j] = __ldg(row + reflect(x0 - tp.R + j, W));
+    __syncthreads();
+    int x = x0 + threadIdx.x;
+    if (x >= W) return;
+    float acc = 0.0f;
+    for (int k = 0; k <= 2 * tp.R; k++) acc = fmaf(s[threadIdx.x + k], tp.t[k], acc);
+    out[(size_t)y * W + x] = acc;
+}
+
+constexpr int COL_TW = 32, COL_TH = 64, COL_RPT = 8;  // 32x8 threads, 8 rows each
+
+// Column pass; epi(index, blurred) writes the result.
+template <class Epi>
+__global__ void blur_cols_kernel(const float* __restrict__ in, int W, int H, Taps tp, Epi epi) {
+    __shared__ float s[(COL_TH + 2 * MAXR) * COL_TW];
+    int x0 = blockIdx.x * COL_TW, y0 = blockIdx.y * COL_TH;
+    int tx = threadIdx.x, ty = threadIdx.y;
+    int x = x0 + tx;
+    int span = COL_TH + 2 * tp.R;
+    if (x < W)
+        for (int j = ty; j < span; j += blockDim.y) s[j * COL_TW + tx] = __ldg(in + (size_t)reflect(y0 - tp.R + j, H) * W + x);
+    __syncthreads();
+    if (x >= W) return;
+    for (int r = 0; r < COL_RPT; r++) {
+        int ly = ty * COL_RPT + r, y = y0 + ly;
+        if (y >= H) break;
+        float acc = 0.0f;
+        for (int k = 0; k <= 2 * tp.R; k++) acc = fmaf(s[(ly + k) * COL_TW + tx], tp.t[k], acc);
+        epi((size_t)y * W + x, acc);
+    }
+}
+
+struct EpiStore {
+    float* out;
+    __device__ __forceinline__ void operator()(size_t i, float v) const { out[i] = v; }
+};
+// local scatter: p = keep*p + mix*blur(p) (halation.rs:164-181)
+struct EpiMix {
+    float* plane;
+    float keep, mix;
+    __device__ __forceinline__ void operator()(size_t i, float v) const { plane[i] = keep * plane[i] + mix * v; }
+};
+// support bounce: plane_e += gain_e * blur(deep) (halation.rs:80-92)
+struct EpiBounce {
+    float* planes;
+    size_t n;
+    int E;
+    float gain[MAXE];
+    __device__ __forceinline__ void operator()(size_t i, float v) const {
+        for (int e = 0; e < E; e++)
+            if (gain[e] > 0.0f) planes[e * n + i] += gain[e] * v;
+    }
+};
+// adjacency: d += beta * (d - blur(d)) (diffusion.rs:11-28)
+struct EpiAdjacency {
+    float* plane;
+    float beta;
+    __device__ __forceinline__ void operator()(size_t i, float v) const {
+        float d = plane[i];
+        plane[i] = d + beta * (d - v);
+    }
+};
+// Sum of squares of a plane into *out (f64), one atomic per block.
+__global__ void sumsq_kernel(const float* __restrict__ v, size_t n, double* __restrict__ out) {
+    __shared__ double sh[256];
+    double a = 0.0;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        double x = (double)v[p];
+        a += x * x;
+    }
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(out, sh[0]);
+}
+
+int taps_for(float sigma, Taps* tp) {
+    int r = gaussian_taps(sigma, tp->t, 2 * MAXR + 1);
+    if (r < 0) return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "film: blur radius above 64 px (pixel pitch too small)");
+    tp->R = r;
+    return IMOPS_OK;
+}
+
+template <class Epi>
+int blur(const float* in, float* tmp, int W, int H, const Taps& tp, Epi epi, cudaStream_t s) {
+    dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
+    blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(in, tmp, W, H, tp);
+    dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
+    blur_cols_kernel<<<cg, cb, 0, s>>>(tmp, W, H, tp, epi);
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film blur launch");
+    return IMOPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// capture LUT + reduce (capture.rs:61-88, reduction.rs:16-68)
+
+__device__ __forceinline__ float lut_sample(const float* logs, const float* fr, float phi) {
+    if (!(phi > 0.0f)) return fr[0];
+    float lp = log10f(phi);
+    if (lp <= logs[0]) return fr[0];
+    if (lp >= logs[LUTN - 1]) return fr[LUTN - 1];
+    int lo = 0, hi = LUTN - 1;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (logs[mid] <= lp) lo = mid; else hi = mid;
+    }
+    float t = (lp - logs[lo]) / (logs[hi] - logs[lo]);
+    return fr[lo] * (1.0f - t) + fr[hi] * t;
+}
+
+__global__ void lut_reduce_kernel(float* __restrict__ planes, float* __restrict__ mask, size_t n, int E,
+                                  const RefSpec* __restrict__ R) {
+    __shared__ float logs[MAXE][LUTN], fr[MAXE][LUTN];
+    for (int k = threadIdx.x; k < E * LUTN; k += blockDim.x) {
+        logs[k / LUTN][k % LUTN] = R->lut_log[k / LUTN][k % LUTN];
+        fr[k / LUTN][k % LUTN] = R->lut_frac[k / LUTN][k % LUTN];
+    }
+    __syncthreads();
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        for (int e = 0; e < E; e++) {
+            float phi = planes[e * n + p] * R->eta[e];
+            float f = lut_sample(logs[e], fr[e], phi);
+            f = fminf(fmaxf(f, 0.0f), 1.0f);
+            float ef = R->reversal[e] ? 1.0f - f : f;
+            float dmax = R->dmax[e];
+            float d = dmax * powf(ef, R->inv_gamma[e]);
+            planes[e * n + p] = d;
+            mask[e * n + p] = R->has_mask[e] ? R->mask_scale[e] * (1.0f - fminf(fmaxf(d / dmax, 0.0f), 1.0f)) : 0.0f;
+        }
+}
+
+// DIR inhibition: D_j *= exp(-sum_i m[i][j] * inh_i) (diffusion.rs:39-84)
+__global__ void dir_apply_kernel(float* __restrict__ planes, const float* __restrict__ inh, size_t n, int E,
+                                 const RefSpec* __restrict__ R) {
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        for (int j = 0; j < E; j++) {
+            float tot = 0.0f;
+            bool active = false;
+            for (int i = 0; i < E; i++) {
+                float w = R->dir[i][j];
+                if (w != 0.0f) {
+                    active = true;
+                    tot += w * inh[i * n + p];
+                }
+            }
+            if (active) planes[j * n + p] *= expf(-tot);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// grain (grain.rs:20-100): SplitMix64 is counter based, so pixel x of row y
+// uses draws 12x+1..12x+12 of the row stream and is generated independently.
+
+__device__ __forceinline__ uint64_t splitmix_at(uint64_t s0, uint64_t k) {
+    uint64_t z = s0 + k * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void grain_noise_kernel(float* __restrict__ noise, int W, int H, uint64_t seed, int layer) {
+    size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        uint64_t y = p / W, x = p % W;
+        uint64_t s0 = seed * 0xD1B54A32D192ED03ull + (uint64_t)layer * 0x9E3779B97F4A7C15ull + y;
+        float acc = 0.0f;
+        for (int k = 1; k <= 12; k++) acc += __ull2float_rn(splitmix_at(s0, 12 * x + k)) / 18446744073709551616.0f;
+        noise[p] = acc - 6.0f;
+    }
+}
+
+// D <- clamp(D + kappa*taper*sqrt(D(Dmax-D))*n*norm, 0, 1.05 Dmax)
+__global__ void grain_apply_kernel(float* __restrict__ plane, const float* __restrict__ noise, size_t n,
+                                   const double* __restrict__ sumsq, float kappa, float dmax) {
+    double var = *sumsq / (double)n;
+    float norm = var > 1e-12 ? (float)(1.0 / sqrt(var)) : 1.0f;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        float d = plane[p];
+        float dens = fminf(fmaxf(d, 0.0f), dmax);
+        float toe = 0.02f * dmax;
+        float taper = fminf(dens / (dens + toe), 1.0f);
+        float sd = taper * sqrtf(fmaxf(dens * (dmax - dens), 0.0f));
+        d = dens + kappa * sd * noise[p] * norm;
+        plane[p] = fminf(fmaxf(d, 0.0f), dmax * 1.05f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// scan (densitometry.rs:13-73) on the 16-bin grid
+
+__global__ void scan16_kernel(const float* __restrict__ img, const float* __restrict__ mask, size_t n,
+                              const ScanSpec16* __restrict__ C, float* __restrict__ rgb) {
+    __shared__ ScanSpec16 sc;
+    for (int k = threadIdx.x; k < (int)(sizeof(ScanSpec16) / 4); k += blockDim.x)
+        reinterpret_cast<float*>(&sc)[k] = reinterpret_cast<const float*>(C)[k];
+    __syncthreads();
+    const int E = sc.E;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        float di[MAXE], dm[MAXE];
+        for (int e = 0; e < E; e++) {
+            di[e] = img[e * n + p];
+            dm[e] = mask[e * n + p];
+        }
+        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+#pragma unroll
+        for (int l = 0; l < NB16; l++) {
+            float d = 0.0f;
+            for (int e = 0; e < E; e++) d = fmaf(di[e], sc.eps[e][l], fmaf(dm[e], sc.meps[e][l], d));
+            float t = exp2f(-d);
+            o0 = fmaf(sc.C[l][0], t, o0);
+            o1 = fmaf(sc.C[l][1], t, o1);
+            o2 = fmaf(sc.C[l][2], t, o2);
+        }
+        rgb[3 * p] = o0;
+        rgb[3 * p + 1] = o1;
+        rgb[3 * p + 2] = o2;
+    }
+}
+
+// invert_negative (invert.rs:36-108); mid/dmin read from device memory.
+__global__ void invert_kernel(float* __restrict__ rgb, size_t n, const float* __restrict__ mid_dmin) {
+    const float eps = 1e-6f, HEAD = 8.0f, KEEP = 0.55f, FADE = 0.02f, MG = 0.185f;
+    const float LR = 0.2722287168f, LG = 0.6740817658f, LB = 0.0536895174f;
+    float dmin[3], sh[3], g[3];
+    for (int c = 0; c < 3; c++) {
+        dmin[c] = fmaxf(mid_dmin[3 + c], eps);
+        float mt = fminf(fmaxf(mid_dmin[c] / dmin[c], eps), 1.0f - eps);
+        float im = fmaxf(1.0f / mt - 1.0f, 0.0f);
+        sh[c] = fmaxf(im * HEAD, eps);
+        float i2 = fmaxf(im, 0.0f), s2 = fmaxf(sh[c], 1e-6f);
+        float sm = fmaxf(i2 / (1.0f + i2 / s2), eps);
+        g[c] = MG / sm;
+    }
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        float raw[3];
+        for (int c = 0; c < 3; c++) {
+            float t = fminf(fmaxf(rgb[3 * p + c] / dmin[c], eps), 1.0f);
+            float inv = fmaxf(1.0f / t - 1.0f, 0.0f);
+            float i2 = fmaxf(inv, 0.0f), s2 = fmaxf(sh[c], 1e-6f);
+            raw[c] = fmaxf(g[c] * (i2 / (1.0f + i2 / s2)), 0.0f);
+        }
+        float y = fmaxf(LR * raw[0] + LG * raw[1] + LB * raw[2], 0.0f);
+        float k = y <= 0.0f ? 0.0f : (y >= FADE ? KEEP : KEEP * (y / FADE));
+        for (int c = 0; c < 3; c++) rgb[3 * p + c] = fmaxf(y + k * (raw[c] - y), 0.0f);
+    }
+}
+
+// mean RGB of a small buffer in f64 (invert.rs:111-125), one block
+__global__ void mean_rgb_kernel(const float* __restrict__ rgb, int n, float* __restrict__ out) {
+    __shared__ double s[3][256];
+    double a[3] = {0, 0, 0};
+    for (int p = threadIdx.x; p < n; p += blockDim.x)
+        for (int c = 0; c < 3; c++) a[c] += (double)rgb[3 * p + c];
+    for (int c = 0; c < 3; c++) s[c][threadIdx.x] = a[c];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int c = 0; c < 3; c++) s[c][threadIdx.x] += s[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; c++) out[c] = (float)(s[c][0] / (double)n);
+}
+
+// ---------------------------------------------------------------------------
+// baseline preset: fused halation column pass + logistic curves + grain +
+// 81-bin scan.  Each block owns a 32x64 pixel tile and stages the rows of
+// the halation row-pass output it needs (64 + 2*64) in shared memory.
+
+struct Base81 {
+    BaselineSpec B;
+    ScanSpec81 S;
+    float taps[2 * HAL_R + 1];
+};
+
+__global__ void __launch_bounds__(256) scan81_fused_kernel(const float* __restrict__ a, const float* __restrict__ hr,
+                                                           const float* __restrict__ noise,
+                                                           const double* __restrict__ sumsq, int W, int H,
+                                                           const Base81* __restrict__ P, float* __restrict__ rgb) {
+    __shared__ float s[(COL_TH + 2 * HAL_R) * COL_TW];
+    __shared__ Base81 c;
+    for (int k = threadIdx.y * blockDim.x + threadIdx.x; k < (int)(sizeof(Base81) / 4); k += blockDim.x * blockDim.y)
+        reinterpret_cast<float*>(&c)[k] = reinterpret_cast<const float*>(P)[k];
+    int x0 = blockIdx.x * COL_TW, y0 = blockIdx.y * COL_TH;
+    int tx = threadIdx.x, ty = threadIdx.y, x = x0 + tx;
+    const int span = COL_TH + 2 * HAL_R;
+    if (x < W)
+        for (int j = ty; j < span; j += blockDim.y) s[j * COL_TW + tx] = __ldg(hr + (size_t)reflect(y0 - HAL_R + j, H) * W + x);
+    __syncthreads();
+    if (x >= W) return;
+    const size_t n = (size_t)W * H;
+    float norm[3] = {1.f, 1.f, 1.f};
+    if (c.B.grain_sigma > 0.0f)
+        for (int e = 0; e < 3; e++) {
+            double var = sumsq[e] / (double)n;
+            norm[e] = var > 1e-12 ? (float)(1.0 / sqrt(var)) : 1.0f;
+        }
+    for (int r = 0; r < COL_RPT; r++) {
+        int ly = ty * COL_RPT + r, y = y0 + ly;
+        if (y >= H) break;
+        size_t p = (size_t)y * W + x;
+        float bsum = 0.0f;
+        for (int k = 0; k <= 2 * HAL_R; k++) bsum = fmaf(s[(ly + k) * COL_TW + tx], c.taps[k], bsum);
+        float D[3];
+        for (int e = 0; e < 3; e++) {
+            float E = a[e * n + p] + c.B.hal_strength * c.B.bleed[e] * bsum;
+            float le = log10f(fmaxf(E, 1e-6f));
+            D[e] = c.B.dmax[e] / (1.0f + expf(-c.B.k[e] * (le - c.B.x0[e])));
+            if (c.B.grain_sigma > 0.0f) D[e] += c.B.grain_sigma * noise[e * n + p] * norm[e];
+        }
+        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+#pragma unroll 9
+        for (int l = 0; l < NB81; l++) {
+            float d = D[0] * c.S.eps[0][l];
+            d = fmaf(D[1], c.S.eps[1][l], d);
+            d = fmaf(D[2], c.S.eps[2][l], d);
+            float t = exp2f(-d);
+            o0 = fmaf(c.S.C[l][0], t, o0);
+            o1 = fmaf(c.S.C[l][1], t, o1);
+            o2 = fmaf(c.S.C[l][2], t, o2);
+        }
+        rgb[3 * p] = o0;
+        rgb[3 * p + 1] = o1;
+        rgb[3 * p + 2] = o2;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// workspace (per device+stream, grows on demand)
+
+struct Workspace {
+    std::mutex mu;
+    struct Entry {
+        int dev;
+        cudaStream_t s;
+        void* p;
+        size_t bytes;
+    };
+    std::vector<Entry> v;
+};
+Workspace g_ws;
+
+int workspace(cudaStream_t s, size_t bytes, void** out) {
+    if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, "injected allocation failure (film workspace)");
+    int dev = 0;
+    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(g_ws.mu);
+    for (auto& e : g_ws.v)
+        if (e.dev == dev && e.s == s) {
+            if (e.bytes < bytes) {
+                IMOPS_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+                IMOPS_CUDA_TRY(cudaFree(e.p), "cudaFree(film workspace)");
+                e.p = nullptr;
+                e.bytes = 0;
+                IMOPS_CUDA_TRY(cudaMalloc(&e.p, bytes), "cudaMalloc(film workspace)");
+                e.bytes = bytes;
+            }
+            *out = e.p;
+            return IMOPS_OK;
+        }
+    void* p = nullptr;
+    IMOPS_CUDA_TRY(cudaMalloc(&p, bytes), "cudaMalloc(film workspace)");
+    g_ws.v.push_back({dev, s, p, bytes});
+    *out = p;
+    return IMOPS_OK;
+}
+
+int grid_for(size_t n) {
+    size_t g = (n + 255) / 256, cap = (size_t)sm_count() * 8;
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+// Bump allocator over the workspace.
+struct Arena {
+    char* base;
+    size_t off;
+    template <class T>
+    T* take(size_t count) {
+        size_t a = (off + 255) & ~(size_t)255;
+        T* p = reinterpret_cast<T*>(base + a);
+        off = a + count * sizeof(T);
+        return p;
+    }
+};
+
+size_t ref_workspace_bytes(size_t n, int E) {
+    // planes(E) + mask(E) + inh(E) + tmp(1) + noise(1) + spec copies + sums
+    return (size_t)(3 * E + 2) * n * 4 + sizeof(RefSpec) + sizeof(ScanSpec16) + 64 * 1024;
+}
+
+// expose -> develop -> scan for the reference model; rgb in, rgb out.
+int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int grain, Arena& A, const RefSpec* dR,
+                  const ScanSpec16* dC, cudaStream_t s) {
+    const RefSpec& R = st.ref;
+    const int E = R.E;
+    const size_t n = (size_t)W * H;
+    float* planes = A.take<float>(E * n);
+    float* mask = A.take<float>(E * n);
+    float* inh = A.take<float>(E * n);
+    float* tmp = A.take<float>(n);
+    float* noise = A.take<float>(n);
+    double* sums = A.take<double>(MAXE);
+    int g = grid_for(n);
+    expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, planes, nullptr);
+    Taps tp;
+    int rc;
+    if (R.sigma_local >= 1e-3f && R.local_mix > 0.0f) {
+        if ((rc = taps_for(R.sigma_local, &tp))) return rc;
+        for (int e = 0; e < E; e++)
+            if ((rc = blur(planes + e * n, tmp, W, H, tp, EpiMix{planes + e * n, 1.0f - R.local_mix, R.local_mix}, s)))
+                return rc;
+    }
+    if (R.sigma_wide >= 1e-3f) {
+        if ((rc = taps_for(R.sigma_wide, &tp))) return rc;
+        EpiBounce eb;
+        eb.planes = planes;
+        eb.n = n;
+        eb.E = E;
+        for (int e = 0; e < MAXE; e++) eb.gain[e] = R.hal_gain[e];
+        // the bounce source is the deepest plane before the bounce is added
+        IMOPS_CUDA_TRY(cudaMemcpyAsync(noise, planes + (E - 1) * n, n * 4, cudaMemcpyDeviceToDevice, s), "copy");
+        if ((rc = blur(noise, tmp, W, H, tp, eb, s))) return rc;
+    }
+    lut_reduce_kernel<<<g, 256, 0, s>>>(planes, mask, n, E, dR);
+    if (R.dir_any && R.sigma_dir >= 1e-3f) {
+        if ((rc = taps_for(R.sigma_dir, &tp))) return rc;
+        for (int i = 0; i < E; i++)
+            if ((rc = blur(planes + i * n, tmp, W, H, tp, EpiStore{inh + i * n}, s))) return rc;
+        dir_apply_kernel<<<g, 256, 0, s>>>(planes, inh, n, E, dR);
+    }
+    if (!(fabsf(R.beta) < 1e-8f || R.sigma_adj < 1e-3f)) {
+        if ((rc = taps_for(R.sigma_adj, &tp))) return rc;
+        for (int e = 0; e < E; e++)
+            if ((rc = blur(planes + e * n, tmp, W, H, tp, EpiAdjacency{planes + e * n, R.beta}, s))) return rc;
+    }
+    if (grain) {
+        if ((rc = taps_for(fmaxf(R.sigma_grain, 1.0f), &tp))) return rc;
+        IMOPS_CUDA_TRY(cudaMemsetAsync(sums, 0, MAXE * sizeof(double), s), "memset");
+        for (int e = 0; e < E; e++) {
+            if (R.kappa[e] <= 0.0f || R.dmax[e] <= 0.0f) continue;
+            grain_noise_kernel<<<g, 256, 0, s>>>(inh, W, H, seed, e);
+            if ((rc = blur(inh, tmp, W, H, tp, EpiStore{noise}, s))) return rc;
+            sumsq_kernel<<<g, 256, 0, s>>>(noise, n, sums + e);
+            grain_apply_kernel<<<g, 256, 0, s>>>(planes + e * n, noise, n, sums + e, R.kappa[e], R.dmax[e]);
+        }
+    }
+    scan16_kernel<<<g, 256, 0, s>>>(planes, mask, n, dC, rgb);
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film kernels");
+    return IMOPS_OK;
+}
+
+int process_reference(float* rgb, int W, int H, const ImopsFilmParams& P, cudaStream_t s) {
+    Stock st;
+    float pitch = 0;
+    int rc = build_stock(P.stock, P.film_format, W, P.shutter_seconds, nullptr, &st, &pitch);
+    if (rc) return rc;
+    const size_t n = (size_t)W * H;
+    const size_t nm = 32 * 32;
+    size_t bytes = ref_workspace_bytes(n, st.ref.E) + ref_workspace_bytes(nm, st.ref.E) + nm * 12 + 4096;
+    void* ws = nullptr;
+    if ((rc = workspace(s, bytes, &ws))) return rc;
+    Arena A{static_cast<char*>(ws), 0};
+    RefSpec* dR = A.take<RefSpec>(1);
+    ScanSpec16* dC = A.take<ScanSpec16>(1);
+    float* mid_dmin = A.take<float>(8);
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(dR, &st.ref, sizeof(RefSpec), cudaMemcpyHostToDevice, s), "copy spec");
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(dC, &st.scan16, sizeof(ScanSpec16), cudaMemcpyHostToDevice, s), "copy spec");
+    bool positive = P.output == IMOPS_FILM_POSITIVE_LINEAR && !st.ref.any_reversal;
+    if (positive) {
+        // mid-gray negative: a 32x32 flat patch through the same path, seed 0
+        // (film/mod.rs:136-151)
+        float g = relative_to_absolute_y(0.185f, st.ref.box_iso);
+        std::vector<float> patch(nm * 3, g);
+        float* dpatch = A.take<float>(nm * 3);
+        IMOPS_CUDA_TRY(cudaMemcpyAsync(dpatch, patch.data(), nm * 12, cudaMemcpyHostToDevice, s), "copy patch");
+        Arena B{A.base, A.off};
+        B.off = A.off + ref_workspace_bytes(n, st.ref.E);
+        if ((rc = run_reference(dpatch, 32, 32, st, 0, P.grain, B, dR, dC, s))) return rc;
+        mean_rgb_kernel<<<1, 256, 0, s>>>(dpatch, (int)nm, mid_dmin);
+        IMOPS_CUDA_TRY(cudaMemcpyAsync(mid_dmin + 3, st.ref.dmin_norm, 12, cudaMemcpyHostToDevice, s), "copy dmin");
+    }
+    if ((rc = run_reference(rgb, W, H, st, P.seed, P.grain, A, dR, dC, s))) return rc;
+    if (positive) invert_kernel<<<grid_for(n), 256, 0, s>>>(rgb, n, mid_dmin);
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film invert");
+    return IMOPS_OK;
+}
+
+}  // namespace film
+}  // namespace imops
+
+namespace imops {
+namespace film {
+
+// Baseline preset forward on an ACEScg image in place.
+int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp, cudaStream_t s) {
+    ImopsBaselineFilm P;
+    if (Pp) P = *Pp;
+    else imops_baseline_film_defaults(&P);
+    Stock st;
+    float pitch;
+    int rc = build_stock(IMOPS_STOCK_BASELINE81, 0, W, -1.0f, &P, &st, &pitch);
+    if (rc) return rc;
+    const size_t n = (size_t)W * H;
+    size_t bytes = (3 + 1 + 1 + 3 + 1) * n * 4 + sizeof(Base81) + 4096;
+    void* ws = nullptr;
+    if ((rc = workspace(s, bytes, &ws))) return rc;
+    Arena A{static_cast<char*>(ws), 0};
+    Base81* dP = A.take<Base81>(1);
+    double* sums = A.take<double>(4);
+    float* a = A.take<float>(3 * n);
+    float* hal = A.take<float>(n);
+    float* hr = A.take<float>(n);
+    float* noise = A.take<float>(3 * n);
+    float* tmp = A.take<float>(n);
+    Base81 hp;
+    hp.B = st.base;
+    hp.S = st.scan81;
+    for (int i = 0; i < 2 * HAL_R + 1; i++) hp.taps[i] = st.hal_taps[i];
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(dP, &hp, sizeof(Base81), cudaMemcpyHostToDevice, s), "copy spec");
+    int g = grid_for(n);
+    expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
+    {
+        Taps tp;
+        tp.R = HAL_R;
+        for (int i = 0; i < 2 * HAL_R + 1; i++) tp.t[i] = st.hal_taps[i];
+        dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
+        blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(hal, hr, W, H, tp);
+    }
+    if (P.grain_on && P.grain_sigma != 0.0f) {
+        Taps tp;
+        if ((rc = taps_for(fmaxf(P.grain_blur, 1.0f), &tp))) return rc;
+        IMOPS_CUDA_TRY(cudaMemsetAsync(sums, 0, 4 * sizeof(double), s), "memset");
+        for (int e = 0; e < 3; e++) {
+            grain_noise_kernel<<<g, 256, 0, s>>>(tmp, W, H, P.seed, e);
+            if ((rc = blur(tmp, hal, W, H, tp, EpiStore{noise + e * n}, s))) return rc;
+            sumsq_kernel<<<g, 256, 0, s>>>(noise + e * n, n, sums + e);
+        }
+    }
+    dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
+    scan81_fused_kernel<<<cg, cb, 0, s>>>(a, hr, noise, sums, W, H, dP, rgb);
+    IMOPS_CUDA_TRY(cudaGetLastError(), "baseline film kernels");
+    return IMOPS_OK;
+}
+
+}  // namespace film
+}  // namespace imops
+
+
+using namespace imops;
+
+extern "C" int imops_film_process(float* rgb, int w, int h, int color_space, const ImopsFilmParams* params,
+                                  const ImopsBaselineFilm* baseline, imops_stream_t stream) {
+    clear_error();
+    if (!params) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film: NULL params");
+    if (color_space != IMOPS_CS_ACESCG)
+        return fail(IMOPS_ERR_WRONG_COLOR_SPACE, "wrong color space: expected ACEScg");
+    if (w <= 0 || h <= 0 || !rgb) return fail(IMOPS_ERR_INVALID_DIMENSIONS, "invalid image dimensions");
+    cudaStream_t s = as_stream(stream);
+    if (params->stock == IMOPS_STOCK_BASELINE81) return film::baseline_forward_impl(rgb, w, h, baseline, s);
+    return film::process_reference(rgb, w, h, *params, s);
+}
+

@@ -124,6 +124,65 @@ int imops_camera_forward_matrix(const float calib_d65[9], float forward[9]);
  * (IMOPS_CS_*).  calib_d65: the 3x3 row-major calibration matrix. */
 int imops_camera_cst(float *rgb, size_t n_pixels, const float calib_d65[9], int target, imops_stream_t stream);
 
+/* ---- spectral film simulation ------------------------------------------- */
+
+/* Stocks: StockId (pichromatic/src/film/stock/mod.rs:126-147), plus the
+ * library's 81-bin "baseline" preset (not in the reference, see
+ * ImopsBaselineFilm). */
+#define IMOPS_STOCK_BWSTUB 0
+#define IMOPS_STOCK_COLORNEG200 1
+#define IMOPS_STOCK_BASELINE81 100
+
+/* FilmFormat (film/types.rs:24-49). */
+#define IMOPS_FORMAT_35MM 0
+#define IMOPS_FORMAT_6X6 1
+#define IMOPS_FORMAT_4X5 2
+
+/* FilmOutput (film/mod.rs:45-51). */
+#define IMOPS_FILM_NEGATIVE_LINEAR 0
+#define IMOPS_FILM_POSITIVE_LINEAR 1
+
+/* FilmParams (film/mod.rs:53-71) plus the image metadata film::process reads. */
+typedef struct {
+    int stock;              /* IMOPS_STOCK_* */
+    int film_format;        /* IMOPS_FORMAT_* */
+    uint64_t seed;          /* grain seed */
+    int output;             /* IMOPS_FILM_* */
+    float shutter_seconds;  /* metadata.shutter_seconds; < 0 when absent (then 1 / box ISO) */
+    int grain;              /* 1: grain as the reference (always on); 0: grain off (parity mode) */
+} ImopsFilmParams;
+
+/* The "baseline" 81-bin preset (380..780 nm, 5 nm): 3 layers with Gaussian
+ * sensitivities (450/550/650 nm), logistic density curves
+ * D = dmax / (1 + exp(-k (log10 E - x0))), halation as a Gaussian blur of
+ * max(0, R - hal_threshold) (fixed tap radius) added with strength * bleed
+ * per layer, and seeded SplitMix64 grain of std grain_sigma.  Operates on
+ * relative scene-linear ACEScg.  Field order is part of the ABI. */
+typedef struct {
+    float dmax[3], k[3], x0[3];
+    float hal_strength;     /* 0.15 */
+    float hal_sigma;        /* 20 px */
+    int hal_radius;         /* 64 (fixed so the output is smooth in sigma) */
+    float hal_threshold;    /* 0.8 */
+    float grain_sigma;      /* 0.02 (density) */
+    float grain_blur;       /* 1 px */
+    int grain_on;
+    uint64_t seed;
+} ImopsBaselineFilm;
+
+/* Defaults of the baseline preset (the benchmark workload's values). */
+void imops_baseline_film_defaults(ImopsBaselineFilm *out);
+
+/* film::process (pichromatic/src/film/mod.rs:77-129) on a device RGB image
+ * in place.  color_space must be IMOPS_CS_ACESCG (else
+ * IMOPS_ERR_WRONG_COLOR_SPACE, FilmError::WrongColorSpace); w, h > 0 (else
+ * IMOPS_ERR_INVALID_DIMENSIONS).  The reference stocks expect absolute
+ * luminance (BaselineExposureCompensation); IMOPS_STOCK_BASELINE81 takes the
+ * preset in `baseline` (NULL = defaults) and relative ACEScg.  Uses a
+ * library-owned per-stream workspace (allocated on first use). */
+int imops_film_process(float *rgb, int w, int h, int color_space, const ImopsFilmParams *params,
+                       const ImopsBaselineFilm *baseline, imops_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
