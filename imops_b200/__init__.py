@@ -231,3 +231,48 @@ def film_process(rgb, stock: int = STOCK_COLORNEG200, film_format: int = FORMAT_
     bptr = ctypes.byref(baseline) if baseline is not None else None
     check(f(_ptr(rgb), W, H, color_space, ctypes.byref(p), bptr, _stream(stream)))
     return rgb
+
+
+class DevelopParams(ctypes.Structure):
+    """ImopsDevelopParams (include/imops_b200.h)."""
+
+    _fields_ = [("demosaic", ctypes.c_int), ("cfa", ctypes.c_char_p), ("clip_pt", ctypes.c_float),
+                ("wb", ctypes.c_float * 4), ("n_gain", ctypes.c_int), ("ev", ctypes.c_float * 2),
+                ("target", ctypes.c_int), ("calib_d65", ctypes.c_float * 9), ("film", ctypes.c_int),
+                ("film_params", FilmParams), ("baseline", BaselineFilm)]
+
+
+def develop_u16(raw, crop, black, white, params: DevelopParams, period=(2, 2), out=None, stream=None):
+    """Fused forward from a u16 frame (imops_develop_u16); returns (h, w, 3)."""
+    import torch
+    x, y, w, h = crop
+    pw, ph = period
+    n = pw * ph
+    bl = (ctypes.c_float * n)(*([float(b) for b in black] if hasattr(black, "__len__") else [float(black)] * n))
+    wh = (ctypes.c_float * n)(*([float(v) for v in white] if hasattr(white, "__len__") else [float(white)] * n))
+    out = out if out is not None else torch.empty((h, w, 3), device=raw.device, dtype=torch.float32)
+    f = lib().imops_develop_u16
+    f.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 6 + [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                           ctypes.c_int, ctypes.POINTER(DevelopParams),
+                                                           ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(raw), raw.shape[1], raw.shape[0], x, y, w, h, bl, wh, pw, ph, ctypes.byref(params), _ptr(out),
+            _stream(stream)))
+    return out
+
+
+def develop_f32(mosaic, params: DevelopParams, shift=(0, 0), out=None, stream=None):
+    import torch
+    _require_cuda_f32(mosaic, "mosaic")
+    h, w = mosaic.shape
+    out = out if out is not None else torch.empty((h, w, 3), device=mosaic.device, dtype=torch.float32)
+    f = lib().imops_develop_f32
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                  ctypes.POINTER(DevelopParams), ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(mosaic), w, h, shift[0], shift[1], ctypes.byref(params), _ptr(out), _stream(stream)))
+    return out
+
+
+def launch_count() -> int:
+    f = lib().imops_launch_count
+    f.restype = ctypes.c_uint64
+    return int(f())

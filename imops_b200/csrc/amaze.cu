@@ -22,7 +22,8 @@
 // hcd, vcd and hvwt (the most re-read) live in shared memory (224 KB), the
 // others in a per-CTA slot of a global scratch buffer that the persistent
 // grid reuses tile after tile, so it stays resident in L2.
-#include "common.cuh"
+#include "amaze.cuh"
+#include "color.cuh"
 
 #include <mutex>
 #include <vector>
@@ -56,8 +57,29 @@ struct Bayer {
     __device__ __forceinline__ int at(int r, int q) const { return c[((r & 1) << 1) | (q & 1)]; }
 };
 
+// Mosaic sources: the reference's f32 mosaic, or a u16 sensor frame scaled
+// on load with the same f32 arithmetic as imops_scale_u16 (so the values,
+// and hence the output bits, are identical).
+struct SrcF32 {
+    const float* p;
+    int W;
+    __device__ __forceinline__ float operator()(int r, int q) const { return __ldg(p + (size_t)r * W + q); }
+};
+struct SrcU16 {
+    const uint16_t* raw;
+    int raw_w, cx, cy, pw, ph;
+    float black[16], white[16];
+    __device__ __forceinline__ float operator()(int r, int q) const {
+        int sy = cy + r, sx = cx + q;
+        int site = (sy % ph) * pw + (sx % pw);
+        float v = (float)__ldg(raw + (size_t)sy * raw_w + sx);
+        return (v - black[site]) / (white[site] - black[site]);
+    }
+};
+
+template <class Src>
 struct Params {
-    const float* in;
+    Src in;
     int W, H;
     Bayer cfa;
     float clip;
@@ -120,10 +142,11 @@ bool size_supported(int W, int H) {
     return true;
 }
 
-__device__ __forceinline__ float get_in(const Params& p, int r, int q) {
+template <class P>
+__device__ __forceinline__ float get_in(const P& p, int r, int q) {
     r = r < 0 ? 0 : (r > p.H - 1 ? p.H - 1 : r);
     q = q < 0 ? 0 : (q > p.W - 1 ? p.W - 1 : q);
-    return __ldg(p.in + (size_t)r * p.W + q);
+    return p.in(r, q);
 }
 
 // One rectangular fill pass: rows [r0,r1) x cols [c0,c1) of the loop space;
@@ -140,7 +163,8 @@ __device__ __forceinline__ void fill_pass(float* mos, int r0, int r1, int c0, in
 
 // Tile fill: demosaic.rs:499-610, passes in the reference's order so later
 // passes overwrite earlier ones exactly as there.
-__device__ void fill(const Params& p, const Geo& g, float* mos) {
+template <class P>
+__device__ void fill(const P& p, const Geo& g, float* mos) {
     const int top = g.top, left = g.left, W = p.W, H = p.H;
     if (g.rrmin == 0 && g.ccmin == 0 && g.rrmax == g.rr1 && g.ccmax == g.cc1) {
         fill_pass(mos, 0, g.rr1, 0, g.cc1, [](int rr, int cc) { return rr * TS + cc; },
@@ -192,8 +216,8 @@ __device__ __forceinline__ void for_rect(int r0, int r1, int c0, int c1, F f) {
     for (int k = threadIdx.x; k < n; k += blockDim.x) f(r0 + k / w, c0 + k % w);
 }
 
-template <class F>
-__device__ __forceinline__ void for_rb(const Params& p, const Geo& g, int r0, int r1, int c0, int c1, F f) {
+template <class F, class P>
+__device__ __forceinline__ void for_rb(const P& p, const Geo& g, int r0, int r1, int c0, int c1, F f) {
     int w = (c1 - c0 + 1) / 2, n = (r1 - r0) * w;
     if (w <= 0 || r1 <= r0) return;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -223,7 +247,8 @@ __device__ void st_gradients(const Geo& g, const Bufs& b) {
 // demosaic.rs:624-698.  Also writes the zeros the reference's freshly
 // allocated arrays hold just outside the computed band (read by the
 // refinement at rows/cols 2,3 and rr1-4, rr1-3).
-__device__ void st_colour_diff(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_colour_diff(const P& p, const Geo& g, const Bufs& b) {
     const float eps = 1e-5f, arth = 0.75f;
     const float clip8 = p.clip * 0.8f;
     for_rect(2, g.rr1 - 2, 2, g.cc1 - 2, [&](int rr, int cc) {
@@ -319,7 +344,8 @@ __device__ __forceinline__ float cd_bound(float cd, float m, float nb0, float nb
 // columns left, vcd on the refined vcd two rows up; the two are independent,
 // so each (row, parity) hcd chain and each (column, parity) vcd chain is one
 // thread walking in the reference's order.
-__device__ void st_cd_refine(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_cd_refine(const P& p, const Geo& g, const Bufs& b) {
     const int nr = g.rr1 - 8, nc = g.cc1 - 8;
     const int nh = nr > 0 ? 2 * nr : 0, nv = nc > 0 ? 2 * nc : 0;
     const float* m = b.mos;
@@ -363,7 +389,8 @@ __device__ void st_cd_refine(const Params& p, const Geo& g, const Bufs& b) {
 }
 
 // demosaic.rs:788-828
-__device__ void st_hv_weight(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_hv_weight(const P& p, const Geo& g, const Bufs& b) {
     const float epssq = 1e-10f;
     for_rb(p, g, 6, g.rr1 - 6, 6, g.cc1 - 6, [&](int rr, int cc) {
         int i = rr * TS + cc;
@@ -401,7 +428,8 @@ struct NyqBox {
 
 // demosaic.rs:830-869: Nyquist test, flags and their bounding box
 // (first/last flagged row, min/max flagged column).
-__device__ NyqBox st_nyquist_flags(const Params& p, const Geo& g, const Bufs& b, int* sh) {
+template <class P>
+__device__ NyqBox st_nyquist_flags(const P& p, const Geo& g, const Bufs& b, int* sh) {
     const float nyqthresh = 0.5f;
     const float go0 = 0.14659727707323927f, go1 = 0.103592713382435f, go2 = 0.0732036125103057f,
                 go3 = 0.0365543548389495f;
@@ -460,7 +488,8 @@ __device__ NyqBox st_nyquist_flags(const Params& p, const Geo& g, const Bufs& b,
 
 // demosaic.rs:873-947: majority vote inside the box, then the area-based
 // weight at voted sites.
-__device__ void st_nyquist_area(const Params& p, const Geo& g, const Bufs& b, const NyqBox& box) {
+template <class P>
+__device__ void st_nyquist_area(const P& p, const Geo& g, const Bufs& b, const NyqBox& box) {
     const float epssq = 1e-10f;
     for_rb(p, g, box.r0, box.r1, box.c0, box.c1, [&](int rr, int cc) {
         int i = rr * TS + cc;
@@ -499,7 +528,8 @@ __device__ void st_nyquist_area(const Params& p, const Geo& g, const Bufs& b, co
 
 // demosaic.rs:949-976: weight smoothing row by row (reads the row above
 // already updated), then green at R/B sites.
-__device__ void st_green_rb(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
     for (int rr = 8; rr < g.rr1 - 8; rr++) {
         int c0 = 8 + (p.cfa.at(g.top + rr, g.left + 2) & 1);
         int n = (g.cc1 - 8 - c0 + 1) / 2;
@@ -530,7 +560,8 @@ __device__ void st_green_rb(const Params& p, const Geo& g, const Bufs& b) {
 }
 
 // demosaic.rs:978-998
-__device__ void st_nyquist_green(const Params& p, const Geo& g, const Bufs& b, const NyqBox& box) {
+template <class P>
+__device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const NyqBox& box) {
     const float epssq = 1e-10f;
     const float q0 = 0.169917f, q1 = 0.108947f, q2 = 0.069855f, q3 = 0.0287182f;
     for_rb(p, g, box.r0, box.r1, box.c0, box.c1, [&](int rr, int cc) {
@@ -555,7 +586,8 @@ __device__ void st_nyquist_green(const Params& p, const Geo& g, const Bufs& b, c
 }
 
 // demosaic.rs:1000-1019
-__device__ void st_diag_setup(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_diag_setup(const P& p, const Geo& g, const Bufs& b) {
     int w = (g.cc1 - 6 - 6 + 1) / 2, n = (g.rr1 - 12) * w;
     if (w <= 0 || g.rr1 - 12 <= 0) return;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -578,7 +610,8 @@ __device__ void st_diag_setup(const Params& p, const Geo& g, const Bufs& b) {
 }
 
 // demosaic.rs:1021-1107
-__device__ void st_diag_interp(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_diag_interp(const P& p, const Geo& g, const Bufs& b) {
     const float eps = 1e-5f, epssq = 1e-10f, arth = 0.75f;
     const float ge0 = 0.13719494435797422f, ge1 = 0.05640252782101291f;
     for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
@@ -629,7 +662,8 @@ __device__ void st_diag_interp(const Params& p, const Geo& g, const Bufs& b) {
 }
 
 // demosaic.rs:1109-1123: pmwt smoothing row by row, then rbint.
-__device__ void st_rb_interp(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_rb_interp(const P& p, const Geo& g, const Bufs& b) {
     for (int rr = 10; rr < g.rr1 - 10; rr++) {
         int c0 = 10 + (p.cfa.at(g.top + rr, g.left + 2) & 1);
         int n = (g.cc1 - 10 - c0 + 1) / 2;
@@ -645,7 +679,8 @@ __device__ void st_rb_interp(const Params& p, const Geo& g, const Bufs& b) {
 }
 
 // demosaic.rs:1125-1194
-__device__ void st_green_refine(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_green_refine(const P& p, const Geo& g, const Bufs& b) {
     const float eps = 1e-5f, arth = 0.75f;
     for_rb(p, g, 12, g.rr1 - 12, 12, g.cc1 - 12, [&](int rr, int cc) {
         int i = rr * TS + cc, h = i >> 1;
@@ -686,7 +721,8 @@ __device__ void st_green_refine(const Params& p, const Geo& g, const Bufs& b) {
 }
 
 // demosaic.rs:1196-1252
-__device__ void st_chroma(const Params& p, const Geo& g, const Bufs& b) {
+template <class P>
+__device__ void st_chroma(const P& p, const Geo& g, const Bufs& b) {
     const float eps = 1e-5f;
     int ex, ey;
     if (p.cfa.at(0, 0) == 1) {
@@ -729,8 +765,8 @@ __device__ void st_chroma(const Params& p, const Geo& g, const Bufs& b) {
 }
 
 // demosaic.rs:1254-1366; the epilogue receives (row, col, r, g, b).
-template <class Epi>
-__device__ void st_output(const Params& p, const Geo& g, const Bufs& b, const Epi& epi) {
+template <class Epi, class P>
+__device__ void st_output(const P& p, const Geo& g, const Bufs& b, const Epi& epi) {
     for_rect(16, g.rr1 - 16, 16, g.cc1 - 16, [&](int rr, int cc) {
         int row = rr + g.top, col = cc + g.left;
         if (!(col >= 0 && col < p.W && row >= 0 && row < p.H)) return;
@@ -768,8 +804,24 @@ struct EpiRGB {
     }
 };
 
-template <class Epi>
-__global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(Params p, Epi epi) {
+// Colour epilogue: WB / exposure / camera CST on the demosaiced pixel before
+// it is stored (the reference runs them as separate passes over the image;
+// the arithmetic per pixel is the same).
+struct EpiColor {
+    float* rgb;
+    int W;
+    color::Epilogue e;
+    __device__ __forceinline__ void operator()(int row, int col, float r, float g, float b) const {
+        e.apply(r, g, b);
+        float* o = rgb + ((size_t)row * W + col) * 3;
+        o[0] = r;
+        o[1] = g;
+        o[2] = b;
+    }
+};
+
+template <class Src, class Epi>
+__global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(Params<Src> p, Epi epi) {
     extern __shared__ __align__(16) float smem[];
     __shared__ int box_sh[4];
     Bufs b;
@@ -896,17 +948,16 @@ int tiles_of(int W, int H, int* ntx) {
     return nty * nx;
 }
 
-template <class Epi>
-int launch(const float* mosaic, int W, int H, const CfaDev& cfa, float clip, const Epi& epi, cudaStream_t stream) {
-    if (!mosaic) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE: NULL input");
+template <class Src, class Epi>
+int launch(const Src& src, int W, int H, const CfaDev& cfa, float clip, const Epi& epi, cudaStream_t stream) {
     if (W <= 0 || H <= 0) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE: empty image");
     if (!cfa_is_bayer(cfa)) return fail(IMOPS_ERR_UNSUPPORTED_CFA, "AMaZE needs a 2x2 Bayer CFA");
     if (!size_supported(W, H))
         return fail(IMOPS_ERR_UNSUPPORTED_SIZE,
                     "AMaZE: for this image size the reference's 128x128 tile border fill indexes past its tile "
                     "buffer (width or height mod 96 in 1..15)");
-    Params p;
-    p.in = mosaic;
+    Params<Src> p;
+    p.in = src;
     p.W = W;
     p.H = H;
     for (int i = 0; i < 4; i++) p.cfa.c[i] = cfa.col[i];
@@ -919,11 +970,40 @@ int launch(const float* mosaic, int W, int H, const CfaDev& cfa, float clip, con
     if (rc) return rc;
     p.scratch = static_cast<uint8_t*>(scratch);
     if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, "injected launch failure (AMaZE)");
-    IMOPS_CUDA_TRY(cudaFuncSetAttribute(amaze_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES),
+    IMOPS_CUDA_TRY(cudaFuncSetAttribute(amaze_kernel<Src, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)SMEM_BYTES),
                    "cudaFuncSetAttribute(AMaZE)");
-    amaze_kernel<Epi><<<grid, NTHREADS, SMEM_BYTES, stream>>>(p, epi);
+    amaze_kernel<Src, Epi><<<grid, NTHREADS, SMEM_BYTES, stream>>>(p, epi);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "AMaZE launch");
     return IMOPS_OK;
+}
+
+int demosaic_color_f32(const float* mosaic, int W, int H, const CfaDev& cfa, float clip,
+                       const color::Epilogue& e, float* rgb, cudaStream_t s) {
+    if (!mosaic || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE: NULL buffer");
+    return launch(SrcF32{mosaic, W}, W, H, cfa, clip, EpiColor{rgb, W, e}, s);
+}
+
+int demosaic_color_u16(const uint16_t* raw, int raw_w, int raw_h, int cx, int cy, int W, int H, const float* black,
+                       const float* white, int pw, int ph, const CfaDev& cfa, float clip, const color::Epilogue& e,
+                       float* rgb, cudaStream_t s) {
+    if (!raw || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE: NULL buffer");
+    if (pw <= 0 || ph <= 0 || pw * ph > 16) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE: level period above 16 cells");
+    if (cx < 0 || cy < 0 || cx + W > raw_w || cy + H > raw_h)
+        return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE: crop rectangle outside the frame");
+    SrcU16 src;
+    src.raw = raw;
+    src.raw_w = raw_w;
+    src.cx = cx;
+    src.cy = cy;
+    src.pw = pw;
+    src.ph = ph;
+    for (int i = 0; i < pw * ph; i++) {
+        src.black[i] = black[i];
+        src.white[i] = white[i];
+    }
+    return launch(src, W, H, cfa, clip, EpiColor{rgb, W, e}, s);
 }
 
 }  // namespace amaze
@@ -938,7 +1018,7 @@ extern "C" int imops_demosaic_amaze(const float* mosaic, int w, int h, const cha
     CfaDev c;
     int rc = parse_cfa(cfa, shift_x, shift_y, &c);
     if (rc) return rc;
-    if (!rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE: NULL output");
+    if (!rgb || !mosaic) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE: NULL buffer");
     amaze::EpiRGB epi{rgb, w};
-    return amaze::launch(mosaic, w, h, c, clip_pt, epi, as_stream(stream));
+    return amaze::launch(amaze::SrcF32{mosaic, w}, w, h, c, clip_pt, epi, as_stream(stream));
 }

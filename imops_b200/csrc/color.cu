@@ -125,6 +125,7 @@ int run_epilogue(float* rgb, size_t n, const Epilogue& e, cudaStream_t s, const 
     if (n == 0) return IMOPS_OK;
     if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, std::string("injected launch failure (") + what + ")");
     epilogue_kernel<<<stream_grid(n, 256), 256, 0, s>>>(rgb, n, e);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), what);
     return IMOPS_OK;
 }
@@ -151,6 +152,7 @@ extern "C" int imops_scale_u16(const uint16_t* raw, int raw_w, int raw_h, int cr
     size_t n = (size_t)crop_w * crop_h;
     color::scale_u16_kernel_p<<<color::stream_grid(n, 256), 256, 0, as_stream(stream)>>>(
         raw, raw_w, crop_x, crop_y, crop_w, crop_h, period_w, period_h, lv, out);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "scale_u16 launch");
     return IMOPS_OK;
 }

@@ -70,5 +70,11 @@ struct Epilogue {
 // Builds an identity epilogue (no-op).
 Epilogue identity_epilogue();
 
+// Applies `e` in place to n interleaved RGB pixels on stream s.
+int run_epilogue(float* rgb, size_t n, const Epilogue& e, cudaStream_t s, const char* what);
+
+// Grid size for a grid-stride loop over n items.
+int stream_grid(size_t n, int block);
+
 }  // namespace color
 }  // namespace imops

@@ -4,6 +4,7 @@
 
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 
 namespace imops {
@@ -91,6 +92,10 @@ int sm_count() {
     return cached[dev];
 }
 
+static std::atomic<uint64_t> g_launches{0};
+
+void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
 bool fault_injected(const char* site) {
     const char* v = std::getenv("IMOPS_FAULT_INJECT");
     if (!v || !*v) return false;
@@ -100,5 +105,7 @@ bool fault_injected(const char* site) {
 }  // namespace imops
 
 extern "C" const char* imops_last_error(void) { return imops::last_error(); }
+
+extern "C" uint64_t imops_launch_count(void) { return imops::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" const char* imops_version(void) { return "imops_b200 0.1.0 (sm_100a)"; }

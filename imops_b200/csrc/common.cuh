@@ -55,6 +55,9 @@ inline cudaStream_t as_stream(imops_stream_t s) { return reinterpret_cast<cudaSt
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Launch evidence counter (imops_launch_count).
+void note_launch(int n = 1);
+
 // Host-side fault injection for failure-path tests: when the environment
 // variable IMOPS_FAULT_INJECT names `site` ("alloc", "launch"), the call
 // reports a failure instead of touching the GPU.

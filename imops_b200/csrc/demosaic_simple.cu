@@ -74,6 +74,7 @@ extern "C" int imops_demosaic_markesteijn(const float* mosaic, int w, int h, con
     if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, "injected launch failure (markesteijn)");
     dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
     simple::mean3x3_kernel<<<grid, block, 0, as_stream(stream)>>>(mosaic, w, h, c, rgb);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "markesteijn launch");
     return IMOPS_OK;
 }
@@ -95,6 +96,7 @@ extern "C" int imops_demosaic_quad(const float* mosaic, int w, int h, const char
     if (nw <= 0 || nh <= 0) return IMOPS_OK;
     dim3 block(32, 8), grid((nw + 31) / 32, (nh + 7) / 8);
     simple::quad_kernel<<<grid, block, 0, as_stream(stream)>>>(mosaic, w, nw, nh, factor, cols, rgb);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "quad demosaic launch");
     return IMOPS_OK;
 }

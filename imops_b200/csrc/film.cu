@@ -156,8 +156,10 @@ template <class Epi>
 int blur(const float* in, float* tmp, int W, int H, const Taps& tp, Epi epi, cudaStream_t s) {
     dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
     blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(in, tmp, W, H, tp);
+    note_launch();
     dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
     blur_cols_kernel<<<cg, cb, 0, s>>>(tmp, W, H, tp, epi);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "film blur launch");
     return IMOPS_OK;
 }
@@ -473,6 +475,7 @@ int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int 
     double* sums = A.take<double>(MAXE);
     int g = grid_for(n);
     expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, planes, nullptr);
+    note_launch();
     Taps tp;
     int rc;
     if (R.sigma_local >= 1e-3f && R.local_mix > 0.0f) {
@@ -493,11 +496,13 @@ int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int 
         if ((rc = blur(noise, tmp, W, H, tp, eb, s))) return rc;
     }
     lut_reduce_kernel<<<g, 256, 0, s>>>(planes, mask, n, E, dR);
+    note_launch();
     if (R.dir_any && R.sigma_dir >= 1e-3f) {
         if ((rc = taps_for(R.sigma_dir, &tp))) return rc;
         for (int i = 0; i < E; i++)
             if ((rc = blur(planes + i * n, tmp, W, H, tp, EpiStore{inh + i * n}, s))) return rc;
         dir_apply_kernel<<<g, 256, 0, s>>>(planes, inh, n, E, dR);
+        note_launch();
     }
     if (!(fabsf(R.beta) < 1e-8f || R.sigma_adj < 1e-3f)) {
         if ((rc = taps_for(R.sigma_adj, &tp))) return rc;
@@ -510,12 +515,16 @@ int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int 
         for (int e = 0; e < E; e++) {
             if (R.kappa[e] <= 0.0f || R.dmax[e] <= 0.0f) continue;
             grain_noise_kernel<<<g, 256, 0, s>>>(inh, W, H, seed, e);
+            note_launch();
             if ((rc = blur(inh, tmp, W, H, tp, EpiStore{noise}, s))) return rc;
             sumsq_kernel<<<g, 256, 0, s>>>(noise, n, sums + e);
+            note_launch();
             grain_apply_kernel<<<g, 256, 0, s>>>(planes + e * n, noise, n, sums + e, R.kappa[e], R.dmax[e]);
+            note_launch();
         }
     }
     scan16_kernel<<<g, 256, 0, s>>>(planes, mask, n, dC, rgb);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "film kernels");
     return IMOPS_OK;
 }
@@ -548,10 +557,12 @@ int process_reference(float* rgb, int W, int H, const ImopsFilmParams& P, cudaSt
         B.off = A.off + ref_workspace_bytes(n, st.ref.E);
         if ((rc = run_reference(dpatch, 32, 32, st, 0, P.grain, B, dR, dC, s))) return rc;
         mean_rgb_kernel<<<1, 256, 0, s>>>(dpatch, (int)nm, mid_dmin);
+        note_launch();
         IMOPS_CUDA_TRY(cudaMemcpyAsync(mid_dmin + 3, st.ref.dmin_norm, 12, cudaMemcpyHostToDevice, s), "copy dmin");
     }
     if ((rc = run_reference(rgb, W, H, st, P.seed, P.grain, A, dR, dC, s))) return rc;
     if (positive) invert_kernel<<<grid_for(n), 256, 0, s>>>(rgb, n, mid_dmin);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "film invert");
     return IMOPS_OK;
 }
@@ -590,12 +601,14 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
     IMOPS_CUDA_TRY(cudaMemcpyAsync(dP, &hp, sizeof(Base81), cudaMemcpyHostToDevice, s), "copy spec");
     int g = grid_for(n);
     expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
+    note_launch();
     {
         Taps tp;
         tp.R = HAL_R;
         for (int i = 0; i < 2 * HAL_R + 1; i++) tp.t[i] = st.hal_taps[i];
         dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
         blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(hal, hr, W, H, tp);
+        note_launch();
     }
     if (P.grain_on && P.grain_sigma != 0.0f) {
         Taps tp;
@@ -603,12 +616,15 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
         IMOPS_CUDA_TRY(cudaMemsetAsync(sums, 0, 4 * sizeof(double), s), "memset");
         for (int e = 0; e < 3; e++) {
             grain_noise_kernel<<<g, 256, 0, s>>>(tmp, W, H, P.seed, e);
+            note_launch();
             if ((rc = blur(tmp, hal, W, H, tp, EpiStore{noise + e * n}, s))) return rc;
             sumsq_kernel<<<g, 256, 0, s>>>(noise + e * n, n, sums + e);
+            note_launch();
         }
     }
     dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
     scan81_fused_kernel<<<cg, cb, 0, s>>>(a, hr, noise, sums, W, H, dP, rgb);
+    note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "baseline film kernels");
     return IMOPS_OK;
 }

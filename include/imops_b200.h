@@ -183,6 +183,44 @@ void imops_baseline_film_defaults(ImopsBaselineFilm *out);
 int imops_film_process(float *rgb, int w, int h, int color_space, const ImopsFilmParams *params,
                        const ImopsBaselineFilm *baseline, imops_stream_t stream);
 
+/* ---- fused forward -------------------------------------------------------
+ * The path Demosaic -> CFACoeffs -> Exp -> CST -> Film (the module chain of
+ * run_pixel_pipeline, pichromatic-pipeline/src/pipeline.rs:4-13, with the
+ * modules of modules.rs:529-668 and 841-876) as one call: demosaic with the
+ * black/white scaling fused into its tile load and WB / exposure / camera CST
+ * fused into its output stage, then the film simulation.  Outputs are the
+ * same as calling the stage entry points one after another. */
+typedef struct {
+    int demosaic;           /* IMOPS_DEMOSAIC_AMAZE or IMOPS_DEMOSAIC_MARKESTEIJN */
+    const char *cfa;        /* CFA pattern of the uncropped frame */
+    float clip_pt;          /* AMaZE clip point (1.0) */
+    float wb[4];            /* metadata.wb_coeffs (CFACoeffs) */
+    int n_gain;             /* exposure steps applied after WB, in order (0..2) */
+    float ev[2];            /* their EV values: rgb *= 2^ev */
+    int target;             /* CST target IMOPS_CS_*, or IMOPS_CS_CAMERA for no CST */
+    float calib_d65[9];     /* metadata.calibration_matrix_d65 */
+    int film;               /* 1: run the film simulation after the CST (target must be ACEScg) */
+    ImopsFilmParams film_params;
+    ImopsBaselineFilm baseline; /* used when film_params.stock == IMOPS_STOCK_BASELINE81 */
+} ImopsDevelopParams;
+
+/* Forward from a u16 sensor frame: crop (crop_x, crop_y, crop_w, crop_h),
+ * per-cell black/white levels over a period_w x period_h CFA period (HOST
+ * arrays), output crop_w*crop_h*3 f32 on the device.  The CFA phase is
+ * shifted by the crop origin (demosaic::get_cfa, demosaic.rs:93-98). */
+int imops_develop_u16(const uint16_t *raw, int raw_w, int raw_h, int crop_x, int crop_y, int crop_w, int crop_h,
+                      const float *black, const float *white, int period_w, int period_h,
+                      const ImopsDevelopParams *params, float *rgb, imops_stream_t stream);
+
+/* Forward from an already scaled and cropped f32 mosaic (Image.raw_data);
+ * shift_x/shift_y: the crop origin used for the CFA phase. */
+int imops_develop_f32(const float *mosaic, int w, int h, int shift_x, int shift_y, const ImopsDevelopParams *params,
+                      float *rgb, imops_stream_t stream);
+
+/* Number of kernels this library has launched in this process (evidence
+ * counter for benchmarks; monotone, thread-safe). */
+uint64_t imops_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -318,12 +318,14 @@ def baseline_params(**kw) -> OracleBaseline:
     return p
 
 
-def film_baseline(rgb: np.ndarray, params: OracleBaseline | None = None, precision: str = "f64"):
+def film_baseline(rgb: np.ndarray, params: OracleBaseline | None = None, precision: str = "f64",
+                  threads: int = 0):
+    """Baseline (81-bin) film preset; the FP64 build is the oracle of record."""
     dt = _dt(precision)
     out = np.ascontiguousarray(rgb, dtype=dt).copy()
     H, W = out.shape[:2]
     p = params if params is not None else baseline_params()
     fn = _f("oracle_film_baseline", precision)
-    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OracleBaseline)]
-    _check(fn(_ptr(out), W, H, ctypes.byref(p)), "film_baseline")
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OracleBaseline), ctypes.c_int]
+    _check(fn(_ptr(out), W, H, ctypes.byref(p), threads or os.cpu_count()), "film_baseline")
     return out

@@ -399,28 +399,54 @@ static int blur_kernel(real sigma, real **out)
 
 /* Horizontal then vertical 1-D passes with mirror reflection.  `radius_override`
  * >= 0 fixes the tap radius (the baseline preset's halation). */
+typedef struct {
+    const real *src;
+    real *dst;
+    int W, H, radius;
+    const real *k;
+} BlurJob;
+
+static void blur_rows_job(void *p, int worker, long b, long e)
+{
+    BlurJob *j = (BlurJob *)p;
+    (void)worker;
+    for (long y = b; y < e; y++)
+        for (int x = 0; x < j->W; x++) {
+            real acc = K(0.0);
+            for (int t = 0; t < 2 * j->radius + 1; t++) {
+                long xx = reflect_index((long)x + t - j->radius, j->W);
+                acc += j->src[(size_t)y * j->W + xx] * j->k[t];
+            }
+            j->dst[(size_t)y * j->W + x] = acc;
+        }
+}
+
+static void blur_cols_job(void *p, int worker, long b, long e)
+{
+    BlurJob *j = (BlurJob *)p;
+    (void)worker;
+    for (long y = b; y < e; y++)
+        for (int x = 0; x < j->W; x++) {
+            real acc = K(0.0);
+            for (int t = 0; t < 2 * j->radius + 1; t++) {
+                long yy = reflect_index(y + t - j->radius, j->H);
+                acc += j->src[(size_t)yy * j->W + x] * j->k[t];
+            }
+            j->dst[(size_t)y * j->W + x] = acc;
+        }
+}
+
+static int g_threads = 1; /* worker threads for the film oracle's loops */
+
+/* Horizontal then vertical 1-D passes with mirror reflection. */
 static void blur_taps(real *buf, int W, int H, const real *k, int radius)
 {
     size_t n = (size_t)W * H;
     real *tmp = (real *)malloc(sizeof(real) * n);
-    for (int y = 0; y < H; y++)
-        for (int x = 0; x < W; x++) {
-            real acc = K(0.0);
-            for (int t = 0; t < 2 * radius + 1; t++) {
-                long xx = reflect_index((long)x + t - radius, W);
-                acc += buf[(size_t)y * W + xx] * k[t];
-            }
-            tmp[(size_t)y * W + x] = acc;
-        }
-    for (int y = 0; y < H; y++)
-        for (int x = 0; x < W; x++) {
-            real acc = K(0.0);
-            for (int t = 0; t < 2 * radius + 1; t++) {
-                long yy = reflect_index((long)y + t - radius, H);
-                acc += tmp[(size_t)yy * W + x] * k[t];
-            }
-            buf[(size_t)y * W + x] = acc;
-        }
+    BlurJob a = {buf, tmp, W, H, radius, k};
+    oracle_parallel_for(H, 8, g_threads, blur_rows_job, &a);
+    BlurJob c = {tmp, buf, W, H, radius, k};
+    oracle_parallel_for(H, 8, g_threads, blur_cols_job, &c);
     free(tmp);
 }
 
@@ -1096,65 +1122,97 @@ static void b81_build(B81 *b)
  *   D_e += grain_sigma * n_e * norm_e              (seeded SplitMix64 noise)
  *   T   = 10^(-sum_e D_e dye_e(lambda));  rgb = AP1(sum_i trap_i cmf_i T_i) / peak(white)
  */
-int OSYM(oracle_film_baseline)(real *rgb, int W, int H, const OBaseline *P)
+typedef struct {
+    const B81 *b;
+    const OBaseline *P;
+    real *rgb, *a[3], *hal, *noise[3];
+    real norm[3];
+    double peak;
+} BJob;
+
+static void base_expose_job(void *p, int worker, long pb, long pe)
 {
-    if (!rgb || !P || W <= 0 || H <= 0) return ORACLE_ERR_ARG;
-    B81 b;
-    b81_build(&b);
-    size_t n = (size_t)W * H;
-    real *a[3], *hal = (real *)malloc(sizeof(real) * n);
-    for (int e = 0; e < 3; e++) a[e] = (real *)malloc(sizeof(real) * n);
-    for (size_t p = 0; p < n; p++) {
-        double v[3] = {(double)rgb[3 * p], (double)rgb[3 * p + 1], (double)rgb[3 * p + 2]}, w[3];
-        matvec3(b.minv, v, w);
+    BJob *j = (BJob *)p;
+    const B81 *b = j->b;
+    (void)worker;
+    for (long q = pb; q < pe; q++) {
+        size_t p3 = 3 * (size_t)q;
+        double v[3] = {(double)j->rgb[p3], (double)j->rgb[p3 + 1], (double)j->rgb[p3 + 2]}, w[3];
+        matvec3(b->minv, v, w);
         for (int k = 0; k < 3; k++)
             if (w[k] < 0) w[k] = 0;
         for (int e = 0; e < 3; e++) {
             double acc = 0;
             for (int i = 0; i < NB81; i++) {
-                double s = w[0] * b.basis[0][i] + w[1] * b.basis[1][i] + w[2] * b.basis[2][i];
-                acc += b.trap[i] * s * b.sens[e][i];
+                double s = w[0] * b->basis[0][i] + w[1] * b->basis[1][i] + w[2] * b->basis[2][i];
+                acc += b->trap[i] * s * b->sens[e][i];
             }
-            a[e][p] = (real)(acc / b.sens_norm[e]);
+            j->a[e][q] = (real)(acc / b->sens_norm[e]);
         }
-        real h = rgb[3 * p] - (real)P->hal_threshold;
-        hal[p] = h > 0 ? h : 0;
+        real h = j->rgb[p3] - (real)j->P->hal_threshold;
+        j->hal[q] = h > 0 ? h : 0;
     }
-    int R = P->hal_radius;
-    real *taps = (real *)malloc(sizeof(real) * (2 * R + 1));
-    fixed_radius_taps((real)P->hal_sigma, R, taps);
-    blur_taps(hal, W, H, taps, R);
-    free(taps);
-    real *noise[3] = {NULL, NULL, NULL};
-    real norm[3] = {0, 0, 0};
-    if (P->grain_on)
-        for (int e = 0; e < 3; e++) {
-            noise[e] = (real *)malloc(sizeof(real) * n);
-            norm[e] = grain_field(noise[e], W, H, P->seed, e, (real)P->grain_blur);
-        }
-    double peak = b.white[0] > b.white[1] ? b.white[0] : b.white[1];
-    if (b.white[2] > peak) peak = b.white[2];
-    for (size_t p = 0; p < n; p++) {
+}
+
+static void base_scan_job(void *p, int worker, long pb, long pe)
+{
+    BJob *j = (BJob *)p;
+    const B81 *b = j->b;
+    const OBaseline *P = j->P;
+    (void)worker;
+    for (long q = pb; q < pe; q++) {
         double D[3];
         for (int e = 0; e < 3; e++) {
-            double E = (double)a[e][p] + (double)P->hal_strength * BLEED[e] * (double)hal[p];
+            double E = (double)j->a[e][q] + (double)P->hal_strength * BLEED[e] * (double)j->hal[q];
             double le = log10(E > 1e-6 ? E : 1e-6);
             D[e] = (double)P->dmax[e] / (1.0 + exp(-(double)P->k[e] * (le - (double)P->x0[e])));
-            if (P->grain_on) D[e] += (double)P->grain_sigma * (double)noise[e][p] * (double)norm[e];
+            if (P->grain_on) D[e] += (double)P->grain_sigma * (double)j->noise[e][q] * (double)j->norm[e];
         }
         double x = 0, y = 0, z = 0;
         for (int i = 0; i < NB81; i++) {
-            double d = D[0] * b.dye[0][i] + D[1] * b.dye[1][i] + D[2] * b.dye[2][i];
+            double d = D[0] * b->dye[0][i] + D[1] * b->dye[1][i] + D[2] * b->dye[2][i];
             double t = pow(10.0, -d);
-            x += b.trap[i] * b.xb[i] * t;
-            y += b.trap[i] * b.yb[i] * t;
-            z += b.trap[i] * b.zb[i] * t;
+            x += b->trap[i] * b->xb[i] * t;
+            y += b->trap[i] * b->yb[i] * t;
+            z += b->trap[i] * b->zb[i] * t;
         }
         double xyz[3] = {x, y, z}, o[3];
         matvec3(XYZ2AP1, xyz, o);
-        for (int c = 0; c < 3; c++) rgb[3 * p + c] = (real)(o[c] / peak);
+        for (int c = 0; c < 3; c++) j->rgb[3 * (size_t)q + c] = (real)(o[c] / j->peak);
     }
-    for (int e = 0; e < 3; e++) { free(a[e]); free(noise[e]); }
-    free(hal);
+}
+
+int OSYM(oracle_film_baseline)(real *rgb, int W, int H, const OBaseline *P, int threads)
+{
+    if (!rgb || !P || W <= 0 || H <= 0) return ORACLE_ERR_ARG;
+    g_threads = threads > 0 ? threads : 1;
+    B81 b;
+    b81_build(&b);
+    size_t n = (size_t)W * H;
+    BJob j;
+    memset(&j, 0, sizeof j);
+    j.b = &b;
+    j.P = P;
+    j.rgb = rgb;
+    j.hal = (real *)malloc(sizeof(real) * n);
+    for (int e = 0; e < 3; e++) j.a[e] = (real *)malloc(sizeof(real) * n);
+    oracle_parallel_for((long)n, 4096, g_threads, base_expose_job, &j);
+    int R = P->hal_radius;
+    real *taps = (real *)malloc(sizeof(real) * (2 * R + 1));
+    fixed_radius_taps((real)P->hal_sigma, R, taps);
+    blur_taps(j.hal, W, H, taps, R);
+    free(taps);
+    if (P->grain_on)
+        for (int e = 0; e < 3; e++) {
+            j.noise[e] = (real *)malloc(sizeof(real) * n);
+            j.norm[e] = grain_field(j.noise[e], W, H, P->seed, e, (real)P->grain_blur);
+        }
+    double peak = b.white[0] > b.white[1] ? b.white[0] : b.white[1];
+    if (b.white[2] > peak) peak = b.white[2];
+    j.peak = peak;
+    oracle_parallel_for((long)n, 1024, g_threads, base_scan_job, &j);
+    for (int e = 0; e < 3; e++) { free(j.a[e]); free(j.noise[e]); }
+    free(j.hal);
+    g_threads = 1;
     return ORACLE_OK;
 }
