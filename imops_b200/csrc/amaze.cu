@@ -1022,3 +1022,94 @@ extern "C" int imops_demosaic_amaze(const float* mosaic, int w, int h, const cha
     amaze::EpiRGB epi{rgb, w};
     return amaze::launch(amaze::SrcF32{mosaic, w}, w, h, c, clip_pt, epi, as_stream(stream));
 }
+
+// ---------------------------------------------------------------------------
+// No-allocation variant.
+//
+// Some callers cannot call cudaMalloc: code recording work into a CUDA graph
+// (allocation is not a stream operation), host applications whose device
+// memory is owned by their own allocator or budget, and latency-critical
+// paths where cudaMalloc's implicit device synchronisation is unacceptable.
+// imops_demosaic_amaze_noalloc serves them: the same AMaZE kernel, with its
+// per-CTA scratch slots taken from the fixed pool below instead of the
+// library's cached cudaMalloc buffer.
+//
+// The pool holds NOALLOC_SLOTS slots of SLOT_BYTES (31,981,568 bytes in all);
+// every GPU that loads this library holds it until the process exits.  A call
+// runs min(tiles, NOALLOC_SLOTS) persistent CTAs, one slot each, so any image
+// size the reference's tiling accepts fits in the pool (large frames are
+// slower than with imops_demosaic_amaze, which uses one CTA per SM).
+namespace imops {
+namespace amaze {
+
+constexpr int NOALLOC_SLOTS = 32;
+constexpr size_t NOALLOC_BYTES = (size_t)NOALLOC_SLOTS * SLOT_BYTES;
+static_assert(SLOT_BYTES % 256 == 0, "scratch slots must stay 256-byte aligned");
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_BYTES];
+
+struct NoallocSetup {
+    std::mutex mu;
+    void* ptr[128] = {};
+};
+NoallocSetup g_noalloc;
+
+// Once per device, with that device current: the device address of the pool
+// (host code must not pass the symbol itself to a kernel) and the kernel's
+// shared-memory opt-in.
+int noalloc_pool(void** out) {
+    int dev = 0;
+    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 128) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE no-alloc: device index above 127");
+    std::lock_guard<std::mutex> lock(g_noalloc.mu);
+    if (!g_noalloc.ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(AMaZE no-alloc pool)");
+        e = cudaFuncSetAttribute(amaze_kernel<SrcF32, EpiRGB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SMEM_BYTES);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(AMaZE no-alloc)");
+        g_noalloc.ptr[dev] = p;
+    }
+    *out = g_noalloc.ptr[dev];
+    return IMOPS_OK;
+}
+
+}  // namespace amaze
+}  // namespace imops
+
+extern "C" int imops_demosaic_amaze_noalloc(const float* mosaic, int w, int h, const char* cfa, int shift_x,
+                                            int shift_y, float clip_pt, float* rgb, imops_stream_t stream) {
+    using namespace imops;
+    using namespace imops::amaze;
+    clear_error();
+    CfaDev c;
+    int rc = parse_cfa(cfa, shift_x, shift_y, &c);
+    if (rc) return rc;
+    if (!mosaic || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE no-alloc: NULL buffer");
+    if (w <= 0 || h <= 0) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE no-alloc: empty image");
+    if (!cfa_is_bayer(c)) return fail(IMOPS_ERR_UNSUPPORTED_CFA, "AMaZE needs a 2x2 Bayer CFA");
+    if (!size_supported(w, h))
+        return fail(IMOPS_ERR_UNSUPPORTED_SIZE,
+                    "AMaZE: for this image size the reference's 128x128 tile border fill indexes past its tile "
+                    "buffer (width or height mod 96 in 1..15)");
+    Params<SrcF32> p;
+    p.in = SrcF32{mosaic, w};
+    p.W = w;
+    p.H = h;
+    for (int i = 0; i < 4; i++) p.cfa.c[i] = c.col[i];
+    p.clip = clip_pt;
+    p.ntiles = tiles_of(w, h, &p.ntx);
+    int grid = p.ntiles < NOALLOC_SLOTS ? p.ntiles : NOALLOC_SLOTS;
+    if ((size_t)grid * SLOT_BYTES > NOALLOC_BYTES)
+        return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "AMaZE no-alloc: request exceeds the 31,981,568-byte scratch pool");
+    void* pool = nullptr;
+    if ((rc = noalloc_pool(&pool))) return rc;
+    p.scratch = static_cast<uint8_t*>(pool);
+    // nothing in the pool has to start at zero: every tile clears the arrays
+    // whose unwritten entries it reads before using them
+    amaze_kernel<SrcF32, EpiRGB><<<grid, NTHREADS, SMEM_BYTES, as_stream(stream)>>>(p, EpiRGB{rgb, w});
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "AMaZE no-alloc launch");
+    return IMOPS_OK;
+}

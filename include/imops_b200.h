@@ -88,6 +88,24 @@ int imops_scale_u16(const uint16_t *raw, int raw_w, int raw_h, int crop_x, int c
 int imops_demosaic_amaze(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y, float clip_pt,
                          float *rgb, imops_stream_t stream);
 
+/* AMaZE without any device allocation (no counterpart in the reference):
+ * for callers that cannot call cudaMalloc -- work being captured into a CUDA
+ * graph, host applications that own all device memory through their own
+ * allocator, or latency-critical paths that cannot afford cudaMalloc's
+ * implicit synchronisation.  Output is identical to imops_demosaic_amaze.
+ * Scratch comes from a fixed 31,981,568-byte pool (32 tile slots) that every
+ * GPU loading this library holds until exit; a call uses at most 32 CTAs, so
+ * any size imops_demosaic_amaze accepts is accepted, and a request that
+ * would need more than the pool is rejected with IMOPS_ERR_UNSUPPORTED_SIZE.
+ * The first call on a device resolves the pool's device address
+ * (cudaGetSymbolAddress) and sets the kernel's shared-memory limit: make
+ * that first call before any stream capture.  All calls share the pool and
+ * it keeps the last call's contents (the kernel clears what must start at
+ * zero per tile); calls that overlap on the GPU, e.g. on two streams, race
+ * on it and must be serialised by the caller. */
+int imops_demosaic_amaze_noalloc(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y,
+                                 float clip_pt, float *rgb, imops_stream_t stream);
+
 /* Whether imops_demosaic_amaze accepts a w x h image (host-only check). */
 int imops_amaze_size_supported(int w, int h);
 
