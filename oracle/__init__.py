@@ -269,6 +269,13 @@ def lut_sample(stock: int, layer: int, phi: float) -> float:
     return fn(stock, layer, phi)
 
 
+def lut_build_sample(mu_ln: float, sigma_ln: float, k: float, phi: float) -> float:
+    fn = lib().oracle_lut_build_sample_f64
+    fn.argtypes = [ctypes.c_double] * 4
+    fn.restype = ctypes.c_double
+    return fn(mu_ln, sigma_ln, k, phi)
+
+
 def layer_kappa(stock: int, layer: int) -> float:
     fn = lib().oracle_layer_kappa_f32
     fn.argtypes = [ctypes.c_int, ctypes.c_int]

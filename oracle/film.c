@@ -1216,3 +1216,17 @@ int OSYM(oracle_film_baseline)(real *rgb, int W, int H, const OBaseline *P, int 
     g_threads = 1;
     return ORACLE_OK;
 }
+
+/* DevelopableFractionLut::build + sample for an explicit crystal
+ * distribution and calibration k (capture.rs:37-88), for the reference's
+ * own LUT tests (capture.rs:113-186). */
+double OSYM(oracle_lut_build_sample)(double mu_ln, double sigma_ln, double k, double phi)
+{
+    OLayer L;
+    memset(&L, 0, sizeof L);
+    L.mu_ln = mu_ln;
+    L.sigma_ln = sigma_ln;
+    L.capture_k = k;
+    lut_build(&L);
+    return lut_sample(&L, phi);
+}

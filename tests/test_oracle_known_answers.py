@@ -1,0 +1,186 @@
+"""The CPU oracle against the reference's own known-answer and property
+tests (the reference cannot be built here, so these pin the restatement).
+Each test names the reference test it ports."""
+import math
+
+import numpy as np
+import pytest
+
+
+def test_cfa_color_at_and_shift(oracle_lib):
+    # cfa.rs:54-62, 189-203, 343-360
+    c = oracle_lib.parse_cfa("RGGB")
+    assert [c.col[i] for i in range(4)] == [0, 1, 1, 2]
+    s = oracle_lib.parse_cfa("RGGB", 1, 1)
+    assert [s.col[i] for i in range(4)] == [2, 1, 1, 0]  # BGGR
+    with pytest.raises(ValueError):
+        oracle_lib.parse_cfa("RGB")
+
+
+@pytest.mark.parametrize("n", [32, 160])
+def test_amaze_flat_field(oracle_lib, n):
+    # demosaic.rs:1410-1443
+    out = oracle_lib.amaze(np.full((n, n), 0.5, np.float32), "RGGB")
+    assert out.shape == (n, n, 3)
+    assert np.abs(out - 0.5).max() < 0.2
+
+
+def test_fast_flat_field(oracle_lib):
+    # demosaic.rs:1388-1408
+    out = oracle_lib.quad(np.full((16, 16), 0.5, np.float32), "RGGB", 2)
+    assert out.shape == (8, 8, 3)
+    assert np.abs(out - 0.5).max() < 1e-4
+
+
+def test_blur_identity_mass_symmetry(oracle_lib):
+    # blur.rs:95-143
+    buf = np.arange(64, dtype=np.float32).reshape(8, 8)
+    assert np.array_equal(oracle_lib.blur(buf, 0.0), buf)
+    ones = np.ones((64, 64), np.float32)
+    out = oracle_lib.blur(ones, 2.0)
+    assert abs(out.astype(np.float64).sum() / ones.sum() - 1) < 1e-3
+    imp = np.zeros((65, 65), np.float32)
+    imp[32, 32] = 1
+    b = oracle_lib.blur(imp, 3.0)
+    for dx, dy in [(5, 0), (0, 5), (4, 3), (3, 4), (-5, 0), (0, -5)]:
+        a = b[32 + dy, 32 + dx]
+        assert abs(a - b[32 - dy, 32 - dx]) < 1e-5
+        assert abs(a - b[32 + dx, 32 + dy]) < 1e-5
+
+
+def test_capture_lut_properties(oracle_lib):
+    # capture.rs:113-186 with the reference tests' distribution: ln s ~ N(ln 0.7, 0.35^2), k = 1
+    mu, sg, k = math.log(0.7), 0.35, 1.0
+    def lut(phi):
+        return oracle_lib.lut_build_sample(mu, sg, k, phi)
+    prev = -1.0
+    for i in range(64):
+        f = lut(10 ** (-4 + i * (12 / 63)))
+        assert f + 1e-12 >= prev
+        prev = f
+    assert lut(1e-6) < 0.05
+    assert lut(1e10) > 0.99
+    n = 40
+    fs = [lut(10 ** (-3 + i * (10 / (n - 1)))) for i in range(n)]
+    slopes = [fs[i] - fs[i - 1] for i in range(1, n)]
+    mi = 1 + int(np.argmax(slopes))
+    ti = max(mi // 3, 2)
+    si = max(min((mi + n) // 2, n - 1), mi + 2)
+    assert (fs[ti] - fs[ti - 1]) - (fs[ti - 1] - fs[ti - 2]) > 0
+    assert (fs[si] - fs[si - 1]) - (fs[si - 1] - fs[si - 2]) < 0
+    assert lut(3.0) == lut(3.0)  # deterministic
+
+
+def test_stock_lut_monotone(oracle_lib):
+    # the same LUT machinery on ColorNeg200's three emulsions
+    for layer in range(3):
+        fs = [oracle_lib.lut_sample(1, layer, 10 ** (-4 + i * 12 / 63)) for i in range(64)]
+        assert all(b + 1e-12 >= a for a, b in zip(fs, fs[1:]))
+
+
+def test_upsample_roundtrip_gray_and_red(oracle_lib):
+    # upsample.rs:187-224
+    spec, back = oracle_lib.upsample_roundtrip([0.185, 0.185, 0.185])
+    assert (spec >= 0).all()
+    assert np.abs(back - 0.185).max() < 0.02
+    spec, _ = oracle_lib.upsample_roundtrip([0.8, 0.05, 0.02])
+    assert spec[12:16].sum() > spec[0:4].sum()
+
+
+def test_invert_dmin_black_mid_gray(oracle_lib):
+    # invert.rs:131-148
+    dmin = [1.0, 0.45, 0.13]
+    mid = [0.23, 0.15, 0.10]
+    out = oracle_lib.invert(np.array([dmin, mid], np.float32), mid, dmin)
+    assert np.abs(out[0]).max() < 1e-5
+    assert np.abs(out[1] - 0.185).max() < 1e-3
+
+
+def test_invert_pathological_blue_bounded(oracle_lib):
+    # invert.rs:150-175
+    dmin, mid = [1.0, 0.45, 0.127], [0.65, 0.315, 0.122]
+    p = oracle_lib.invert(np.array([[0.16, 0.087, 0.058]], np.float32), mid, dmin)[0]
+    y = 0.2722287168 * p[0] + 0.6740817658 * p[1] + 0.0536895174 * p[2]
+    assert math.isfinite(y) and y > 0
+    assert (p < 2.5).all()
+    assert p.max() / max(p.min(), 1e-6) < 4.0
+
+
+def test_baseline_exposure_ratios(oracle_lib):
+    # radiance.rs:76-128: L = K v N^2 / (t S); doubling t halves L, N x2 -> x4, ISO x2 -> /2
+    x = np.full((1, 3), 0.185, np.float32)
+    def L(t, n, s):
+        return float(oracle_lib.baseline_exposure(x, 0.0, t, n, s, precision="f64")[0][0, 0])
+    l1 = L(1 / 200, 8.0, 200.0)
+    assert abs(l1 - 12.5 * 0.185 * 64) < 1e-5 * l1
+    assert abs(L(2 / 200, 8.0, 200.0) / l1 - 0.5) < 1e-10
+    assert abs(L(1 / 200, 16.0, 200.0) / l1 - 4.0) < 1e-10
+    assert abs(L(1 / 200, 8.0, 400.0) / l1 - 0.5) < 1e-10
+    _, applied = oracle_lib.baseline_exposure(x, 0.0, 0.0, 8.0, 200.0)
+    assert not applied
+
+
+def test_film_bwstub_hd_monotone_and_dmin(oracle_lib):
+    # film/mod.rs:234-273 (BwStub, box ISO 100)
+    g = 12.5 * 64.0
+    ys = []
+    for y in [0.02, 0.05, 0.1, 0.185, 0.3, 0.5, 0.8, 1.2]:
+        img = np.full((8, 8, 3), y * g, np.float32)
+        out = oracle_lib.film_process(img, stock=0, seed=1)
+        ys.append(float((0.2722287168 * out[..., 0] + 0.6740817658 * out[..., 1] +
+                         0.0536895174 * out[..., 2]).mean()))
+    assert all(b <= a + 1e-4 for a, b in zip(ys, ys[1:]))
+    z = oracle_lib.film_process(np.zeros((8, 8, 3), np.float32), stock=0, seed=1)
+    assert abs(z.max(axis=2).mean() - 1.0) < 0.05
+    mg = oracle_lib.film_process(np.full((8, 8, 3), 0.185 * g, np.float32), stock=0, seed=1)
+    assert np.isfinite(mg).all() and (mg > 0).all() and (mg < 1.5).all()
+
+
+def test_film_determinism_and_dmin_norm(oracle_lib):
+    # film/mod.rs:325-334 and 516-535
+    img = np.tile(np.array([0.185, 0.1, 0.05], np.float32) * 1600, (8, 8, 1))
+    a = oracle_lib.film_process(img, stock=1, seed=1)
+    b = oracle_lib.film_process(img, stock=1, seed=1)
+    assert np.array_equal(a, b)
+    d = oracle_lib.normalized_dmin(1)
+    assert abs(d.max() - 1.0) < 1e-5
+    assert d[0] > d[1] > d[2]
+
+
+def test_film_neutral_positive_near_neutral(oracle_lib):
+    # film/mod.rs:285-300: mid gray through ColorNeg200 PositiveLinear has |a|,|b| < 5
+    g = 0.185 * 12.5 * 64.0
+    out = oracle_lib.film_process(np.full((16, 16, 3), g, np.float32), stock=1, seed=1, output=1)
+    m = out.reshape(-1, 3).astype(np.float64).mean(0)
+    M = np.array([[0.6624541811, 0.1340042065, 0.1561876870], [0.2722287168, 0.6740817658, 0.0536895174],
+                  [-0.0055746495, 0.0040607335, 1.0103391003]])
+    xyz = M @ m
+    def f(t):
+        return np.cbrt(t) if t > (6 / 29) ** 3 else t / (3 * (6 / 29) ** 2) + 4 / 29
+    fx, fy, fz = f(xyz[0] / 0.95047), f(xyz[1] / 1.0), f(xyz[2] / 1.08883)
+    a, b = 500 * (fx - fy), 200 * (fy - fz)
+    assert abs(a) < 5 and abs(b) < 5
+
+
+def test_grain_noise_counter_based(oracle_lib):
+    # grain.rs:20-45: the noise of row y does not depend on other rows
+    full = oracle_lib.grain_noise(17, 9, seed=123, layer=1)
+    assert full.shape == (9, 17)
+    assert abs(full.mean()) < 0.5
+    again = oracle_lib.grain_noise(17, 9, seed=123, layer=1)
+    assert np.array_equal(full, again)
+    other = oracle_lib.grain_noise(17, 9, seed=124, layer=1)
+    assert not np.array_equal(full, other)
+
+
+def test_baseline_preset_oracle_sane(oracle_lib):
+    # the library's own 81-bin preset: D=0 (zero exposure) scans to peak 1,
+    # more exposure gives a denser (darker) negative
+    p = oracle_lib.baseline_params(grain_on=0)
+    out0 = oracle_lib.film_baseline(np.zeros((4, 4, 3), np.float32), p)
+    assert out0.max() <= 1.0 + 1e-9
+    lo = oracle_lib.film_baseline(np.full((4, 4, 3), 0.05, np.float32), p)
+    hi = oracle_lib.film_baseline(np.full((4, 4, 3), 0.5, np.float32), p)
+    assert (hi < lo).all()
+    x, y, z = oracle_lib.cmf81()
+    assert abs(y.max() - 1.0) < 0.02 and 550 <= 380 + 5 * int(np.argmax(y)) <= 560
