@@ -31,12 +31,28 @@ H, W = 4024, 6048
 SEED = 1002
 METRIC = "MP/s fwd, 24MP AMaZE+colour+film on 1xB200"
 L2_FLUSH_BYTES = 256 << 20
+PIPELINE_CONFIG = """
+[[pipeline_modules]]
+name = "Demosaic"
+algorithm = "amaze"
+[[pipeline_modules]]
+name = "CFACoeffs"
+[[pipeline_modules]]
+name = "CST"
+target_color_space = "AcesCg"
+[[pipeline_modules]]
+name = "Film"
+stock = "Baseline81"
+film_format = "Film35mm"
+seed = 1002
+output = "NegativeLinear"
+"""
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="imops_b200", choices=["imops_b200", "reference"])
     return ap.parse_args()
@@ -79,7 +95,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -247,23 +263,32 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_total = float(t.item())
 
-    # end to end through the C-ABI: pinned host raw in, pinned host RGB out
+    # end to end through the reference-facing C-ABI (extern_pipeline.rs names):
+    # host u16 frame in, pipeline run, host f32 RGB out, image freed -- every
+    # step.  Each call synchronises, so the host clock brackets the work.
+    from imops_b200.pipeline import Image, make_meta, parse_config, run_pixel_pipeline
     raw_h = torch.from_numpy(raw_np.view(np.int16)).pin_memory()
     rgb_h = torch.empty((H, W, 3), dtype=torch.float32).pin_memory()
+    cfg = parse_config(PIPELINE_CONFIG)
+    meta = make_meta(cfa="RGGB", wb=synthetic.WB, calibration=synthetic.CALIB_D65, black=synthetic.BLACK,
+                     white=synthetic.WHITE)
+    Lp = im.lib()
+
+    def step_e2e():
+        img = Image(Lp.new_raw_image_u16_c(ctypes.c_void_p(raw_h.data_ptr()), W, H, ctypes.byref(meta)))
+        run_pixel_pipeline(img, cfg)
+        im.check(Lp.get_image_rgb_f32_c(img._h, ctypes.c_void_p(rgb_h.data_ptr()), H * W * 3))
+        del img
+
     for _ in range(2):
-        raw.copy_(raw_h, non_blocking=True)
-        step_device()
-        rgb_h.copy_(rgb, non_blocking=True)
+        step_e2e()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
     for _ in range(args.steps):
-        raw.copy_(raw_h, non_blocking=True)
-        step_device()
-        rgb_h.copy_(rgb, non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_e2e = e0.elapsed_time(e1)
+        step_e2e()
+    t_e2e = (time.perf_counter() - t0) * 1e3
     if dist:
         t = torch.tensor([t_e2e], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -294,7 +319,8 @@ def main():
             "cpu_baseline": {"value": round(cpu_v, 3), "unit": "MP/s", "cores": os.cpu_count(), "kind": "port",
                              "sample": cpu_sample_desc},
             "e2e": {"value": round(e2e, 2), "unit": "MP/s", "h2d_bytes_per_step": H * W * 2,
-                    "d2h_bytes_per_step": H * W * 12},
+                    "d2h_bytes_per_step": H * W * 12, "api": "new_raw_image_u16_c + run_pixel_pipeline_c + "
+                    "get_image_rgb_f32_c (pinned host buffers, host clock)"},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }

@@ -66,6 +66,24 @@ bool xyz_to_target(int target, float m[9]) {
     return true;
 }
 
+bool to_xyz(int space, float m[9]) {
+    static const double lsrgb[9] = {506752.0 / 1228815.0, 87881.0 / 245763.0,  12673.0 / 70218.0,
+                                    87098.0 / 409605.0,   175762.0 / 245763.0, 12673.0 / 175545.0,
+                                    7918.0 / 409605.0,    87881.0 / 737289.0,  1001167.0 / 1053270.0};
+    static const double ap1[9] = {0.6624541811,  0.1340042065, 0.1561876870, 0.2722287168, 0.6740817658,
+                                  0.0536895174, -0.0055746495, 0.0040607335, 1.0103391003};
+    const double* src = nullptr;
+    if (space == IMOPS_CS_XYZD65) {
+        for (int i = 0; i < 9; i++) m[i] = (i % 4 == 0) ? 1.0f : 0.0f;
+        return true;
+    }
+    if (space == IMOPS_CS_LINEAR_SRGB || space == IMOPS_CS_SRGB) src = lsrgb;
+    if (space == IMOPS_CS_ACESCG) src = ap1;
+    if (!src) return false;
+    for (int i = 0; i < 9; i++) m[i] = (float)src[i];
+    return true;
+}
+
 float exp_value(float ev) { return powf(2.0f, ev); }
 
 float luminance_gain(float shutter, float f_number, float iso) {
@@ -77,10 +95,11 @@ Epilogue identity_epilogue() {
     Epilogue e;
     e.wb[0] = e.wb[1] = e.wb[2] = 1.0f;
     e.n_gain = 0;
-    e.gain[0] = e.gain[1] = 1.0f;
+    e.gain[0] = e.gain[1] = e.gain[2] = e.gain[3] = 1.0f;
     e.do_cst = 0;
     for (int i = 0; i < 9; i++) e.fwd[i] = e.tgt[i] = (i % 4 == 0) ? 1.0f : 0.0f;
     e.srgb = 0;
+    e.src_srgb = 0;
     return e;
 }
 

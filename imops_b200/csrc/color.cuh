@@ -28,12 +28,13 @@ float luminance_gain(float shutter, float f_number, float iso);
 // rounding matches the separate module passes.
 struct Epilogue {
     float wb[3];
-    int n_gain;       // 0..2 scalar gains applied one after another
-    float gain[2];
+    int n_gain;       // 0..4 scalar gains applied one after another
+    float gain[4];
     int do_cst;
     float fwd[9];
     float tgt[9];
     int srgb;         // apply the sRGB transfer after the target matrix
+    int src_srgb;     // decode an sRGB-encoded input before the first matrix
 
     __device__ __forceinline__ void apply(float& r, float& g, float& b) const {
         r = r * wb[0];
@@ -45,6 +46,11 @@ struct Epilogue {
             b = b * gain[k];
         }
         if (do_cst) {
+            if (src_srgb) {
+                r = srgb_decode(r);
+                g = srgb_decode(g);
+                b = srgb_decode(b);
+            }
             float x = fwd[0] * r + fwd[1] * g + fwd[2] * b;
             float y = fwd[3] * r + fwd[4] * g + fwd[5] * b;
             float z = fwd[6] * r + fwd[7] * g + fwd[8] * b;
@@ -59,6 +65,12 @@ struct Epilogue {
         }
     }
 
+    __device__ __forceinline__ static float srgb_decode(float v) {
+        float a = fabsf(v);
+        float l = a <= 0.04045f ? a / 12.92f : powf((a + 0.055f) / 1.055f, 2.4f);
+        return v < 0.0f ? -l : l;
+    }
+
     // sRGB transfer with odd symmetry (IEC 61966-2-1).
     __device__ __forceinline__ static float srgb_encode(float v) {
         float a = fabsf(v);
@@ -66,6 +78,10 @@ struct Epilogue {
         return v < 0.0f ? -e : e;
     }
 };
+
+// Colour space -> XYZ(D65) 3x3 for IMOPS_CS_{XYZD65,LINEAR_SRGB,SRGB (after
+// decoding),ACESCG}; false otherwise.
+bool to_xyz(int space, float m[9]);
 
 // Builds an identity epilogue (no-op).
 Epilogue identity_epilogue();

@@ -643,7 +643,17 @@ extern "C" int imops_film_process(float* rgb, int w, int h, int color_space, con
         return fail(IMOPS_ERR_WRONG_COLOR_SPACE, "wrong color space: expected ACEScg");
     if (w <= 0 || h <= 0 || !rgb) return fail(IMOPS_ERR_INVALID_DIMENSIONS, "invalid image dimensions");
     cudaStream_t s = as_stream(stream);
-    if (params->stock == IMOPS_STOCK_BASELINE81) return film::baseline_forward_impl(rgb, w, h, baseline, s);
+    if (params->stock == IMOPS_STOCK_BASELINE81) {
+        // without an explicit preset, the defaults with the module's grain seed
+        ImopsBaselineFilm d;
+        if (!baseline) {
+            imops_baseline_film_defaults(&d);
+            d.seed = params->seed;
+            d.grain_on = params->grain;
+            baseline = &d;
+        }
+        return film::baseline_forward_impl(rgb, w, h, baseline, s);
+    }
     return film::process_reference(rgb, w, h, *params, s);
 }
 

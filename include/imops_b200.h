@@ -196,7 +196,8 @@ void imops_baseline_film_defaults(ImopsBaselineFilm *out);
  * IMOPS_ERR_WRONG_COLOR_SPACE, FilmError::WrongColorSpace); w, h > 0 (else
  * IMOPS_ERR_INVALID_DIMENSIONS).  The reference stocks expect absolute
  * luminance (BaselineExposureCompensation); IMOPS_STOCK_BASELINE81 takes the
- * preset in `baseline` (NULL = defaults) and relative ACEScg.  Uses a
+ * preset in `baseline` and relative ACEScg (baseline == NULL: the defaults,
+ * with params->seed as grain seed and params->grain as grain switch).  Uses a
  * library-owned per-stream workspace (allocated on first use). */
 int imops_film_process(float *rgb, int w, int h, int color_space, const ImopsFilmParams *params,
                        const ImopsBaselineFilm *baseline, imops_stream_t stream);
@@ -238,6 +239,84 @@ int imops_develop_f32(const float *mosaic, int w, int h, int shift_x, int shift_
 /* Number of kernels this library has launched in this process (evidence
  * counter for benchmarks; monotone, thread-safe). */
 uint64_t imops_launch_count(void);
+
+/* ---- pipeline-level C-ABI -------------------------------------------------
+ * The embedding interface of pichromatic-pipeline/src/extern_pipeline.rs
+ * (get_pixel_pipeline_c :326-341, run_pixel_pipeline_c :343-359,
+ * get_image_rgb_data_c :361-397, free_* :399-455, get_last_error_c :27-38)
+ * with the same names, ownership and NULL-on-error convention, running the
+ * module chain of run_pixel_pipeline (pipeline.rs:4-13) on the GPU.  HOST
+ * buffers in and out; images live on the device between modules.
+ * Decoding raw files (get_raw_img, rawler) stays on the reference: images
+ * are created from the decoded sensor frame or an already scaled mosaic. */
+typedef struct ImopsImage ImopsImage;        /* Image (pichromatic/src/pixel.rs:23-27) */
+typedef struct ImopsPipeline ImopsPipeline;  /* PipelineConfig (pichromatic-pipeline/src/config.rs:9-11) */
+
+/* The ImageMetadata fields the path reads (pichromatic/src/image.rs:7-50). */
+typedef struct {
+    const char *cfa;            /* metadata.cfa pattern of the uncropped frame */
+    int crop_x, crop_y;         /* metadata.crop_area origin */
+    int crop_w, crop_h;         /* crop size (u16 frames; 0 = whole frame) */
+    int has_wb;
+    float wb_coeffs[4];
+    int has_calibration;
+    float calibration_matrix_d65[9];
+    float black_level, white_level;   /* scaling levels of u16 frames (same for every CFA cell) */
+    int has_baseline_exposure;
+    float baseline_exposure;
+    int has_shutter;
+    float shutter_seconds;
+    int has_f_number;
+    float f_number;
+    int has_iso;
+    float iso;
+} ImopsImageMeta;
+
+/* Image from a decoded u16 sensor frame (what rawler returns before
+ * apply_scaling): the Demosaic module scales, crops and demosaics it. */
+ImopsImage *new_raw_image_u16_c(const uint16_t *raw, size_t width, size_t height, const ImopsImageMeta *meta);
+
+/* Image from an already scaled and cropped f32 mosaic (Image.raw_data after
+ * parse_raw_image, extern_pipeline.rs:239-324); width/height are the cropped
+ * size and crop_x/crop_y give the CFA phase. */
+ImopsImage *new_raw_image_f32_c(const float *raw_data, size_t width, size_t height, const ImopsImageMeta *meta);
+
+/* Image from interleaved f32 RGB in a colour space (IMOPS_CS_*, or
+ * IMOPS_CS_CAMERA for demosaiced camera RGB). */
+ImopsImage *new_rgb_image_c(const float *rgb, size_t width, size_t height, int color_space,
+                            const ImopsImageMeta *meta);
+
+/* parse_config (config.rs:13-34): TOML, else JSON, list of
+ * [[pipeline_modules]] tables matched by case-insensitive name.  NULL on
+ * error (get_last_error_c). */
+ImopsPipeline *get_pixel_pipeline_c(const uint8_t *config, size_t config_len);
+
+/* Runs every module in order on the image; returns `image`, or NULL on error. */
+ImopsImage *run_pixel_pipeline_c(ImopsImage *image, ImopsPipeline *pipeline);
+
+/* RGB as u8 (clamp(0,1)*255 truncated), width*height*3 bytes; free with
+ * free_rgb_buffer_c(ptr, len). */
+const uint8_t *get_image_rgb_data_c(ImopsImage *image, size_t *out_width, size_t *out_height, size_t *out_len);
+
+/* Copies the f32 RGB (width*height*3 floats) into a host buffer. */
+int get_image_rgb_f32_c(ImopsImage *image, float *out, size_t n_floats);
+
+/* Current width, height and colour space (IMOPS_CS_*). */
+int get_image_info_c(const ImopsImage *image, size_t *width, size_t *height, int *color_space);
+
+/* Metadata as JSON (free with free_string_c). */
+char *get_image_metadata_c(const ImopsImage *image);
+
+/* get_pipeline_schema (modules.rs:917-923) as JSON (free with free_string_c). */
+char *get_pipeline_schema_c(void);
+
+/* Last error message of this thread as a new string (free_string_c), or NULL. */
+char *get_last_error_c(void);
+
+void free_image_c(ImopsImage *image);
+void free_pipeline_c(ImopsPipeline *pipeline);
+void free_rgb_buffer_c(uint8_t *ptr, size_t len);
+void free_string_c(char *ptr);
 
 #ifdef __cplusplus
 }
