@@ -1,0 +1,49 @@
+"""Single-launch cases for profiling one kernel of the path under ncu.
+
+  python -m imops_b200.profile_cases amaze --width 4096 --height 3072
+  python -m imops_b200.profile_cases film81 --width 4096 --height 3072
+
+Each case builds a seeded synthetic input, runs the stage once and
+synchronises, so `ncu -k regex:<kernel> -c 1` captures exactly one launch.
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["amaze", "film81", "develop"])
+    ap.add_argument("--width", type=int, default=4096)
+    ap.add_argument("--height", type=int, default=3072)
+    a = ap.parse_args()
+
+    import torch
+
+    import imops_b200 as im
+    from imops_b200 import synthetic
+
+    W, H = a.width, a.height
+    raw = torch.from_numpy(synthetic.mosaic_u16(H, W, seed=5).view(np.int16)).cuda()
+    p = im.DevelopParams()
+    p.demosaic, p.cfa, p.clip_pt = im.DEMOSAIC_AMAZE, b"RGGB", 1.0
+    for i in range(4):
+        p.wb[i] = synthetic.WB[i]
+    p.target = im.CS_ACESCG
+    for i in range(9):
+        p.calib_d65[i] = synthetic.CALIB_D65[i]
+    p.film = 1 if a.case == "develop" else 0
+    p.film_params = im.FilmParams(im.STOCK_BASELINE81, 0, 1, 0, -1.0, 1)
+    p.baseline = im.baseline_film_defaults()
+    out = im.develop_u16(raw, (0, 0, W, H), synthetic.BLACK, synthetic.WHITE, p)
+    if a.case == "film81":
+        torch.cuda.synchronize()
+        im.film_process(out, stock=im.STOCK_BASELINE81)
+    torch.cuda.synchronize()
+    print(f"{a.case} {W}x{H} ok, mean {float(out.mean()):.6f}")
+
+
+if __name__ == "__main__":
+    main()
