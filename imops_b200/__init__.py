@@ -276,3 +276,59 @@ def launch_count() -> int:
     f = lib().imops_launch_count
     f.restype = ctypes.c_uint64
     return int(f())
+
+
+class FilmGradParams(ctypes.Structure):
+    """ImopsFilmGradParams: the 24 parameters of the differentiable model."""
+
+    _fields_ = [("wb", ctypes.c_float * 3), ("matrix", ctypes.c_float * 9), ("ev", ctypes.c_float),
+                ("dmax", ctypes.c_float * 3), ("k", ctypes.c_float * 3), ("x0", ctypes.c_float * 3),
+                ("hal_strength", ctypes.c_float), ("hal_sigma", ctypes.c_float)]
+
+    NAMES = (["wb_r", "wb_g", "wb_b"] + [f"m{i}{j}" for i in range(3) for j in range(3)] + ["ev"] +
+             [f"dmax{l}" for l in range(3)] + [f"k{l}" for l in range(3)] + [f"x0_{l}" for l in range(3)] +
+             ["hal_strength", "hal_sigma"])
+
+    def to_vector(self):
+        return [*self.wb, *self.matrix, self.ev, *self.dmax, *self.k, *self.x0, self.hal_strength, self.hal_sigma]
+
+    @classmethod
+    def from_vector(cls, v):
+        g = cls()
+        v = [float(a) for a in v]
+        for i in range(3):
+            g.wb[i] = v[i]
+        for i in range(9):
+            g.matrix[i] = v[3 + i]
+        g.ev = v[12]
+        for i in range(3):
+            g.dmax[i], g.k[i], g.x0[i] = v[13 + i], v[16 + i], v[19 + i]
+        g.hal_strength, g.hal_sigma = v[22], v[23]
+        return g
+
+
+def param_forward(cam_rgb, params: FilmGradParams, fixed: BaselineFilm | None = None, out=None, stream=None):
+    import torch
+    _require_cuda_f32(cam_rgb, "cam_rgb")
+    H, W = cam_rgb.shape[:2]
+    out = out if out is not None else torch.empty_like(cam_rgb)
+    f = lib().imops_param_forward
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(FilmGradParams), ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(cam_rgb), W, H, ctypes.byref(params), ctypes.byref(fixed) if fixed is not None else None,
+            _ptr(out), _stream(stream)))
+    return out
+
+
+def param_backward(cam_rgb, params: FilmGradParams, grad, g_out=None, target=None, loss_scale: float = 1.0,
+                   fixed: BaselineFilm | None = None, stream=None):
+    """Adds d(loss)/d(params) into `grad` (a (25,) float64 CUDA tensor; [24] is the loss)."""
+    _require_cuda_f32(cam_rgb, "cam_rgb")
+    H, W = cam_rgb.shape[:2]
+    f = lib().imops_param_backward
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                  ctypes.POINTER(FilmGradParams), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(cam_rgb), _ptr(g_out) if g_out is not None else None, _ptr(target) if target is not None else None,
+            loss_scale, W, H, ctypes.byref(params), ctypes.byref(fixed) if fixed is not None else None, _ptr(grad),
+            _stream(stream)))
+    return grad

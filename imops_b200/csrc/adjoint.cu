@@ -1,0 +1,494 @@
+// adjoint.cu -- hand-written adjoints of the colour + film stages for
+// parameter fitting (the reference has no gradients; this is new).
+//
+// Differentiable forward per pixel, from demosaiced camera RGB x (demosaic is
+// upstream of every parameter, so its decisions are simply held fixed):
+//   y   = 2^ev * (wb (.) x)                     WB + exposure
+//   a   = C y                                   camera -> ACEScg matrix (9)
+//   w   = max(0, Minv a);  e_l = sum_k w_k A[k][l]     spectral exposure
+//   h   = max(0, a_R - thr);  B = G_sigma * h   halation (fixed tap radius)
+//   E_l = e_l + s bleed_l B
+//   D_l = Dmax_l / (1 + exp(-k_l (log10 max(E_l,1e-6) - x0_l)))
+//   T(l)= 2^(-sum_l D_l eps'_l(lambda));  out_c = sum_lambda Cscan[lambda][c] T
+// with the baseline preset's tables (film_host.cpp), grain off.
+//
+// Backward: a per-pixel kernel recomputes the forward, takes the upstream
+// gradient (or 2/N (out - target) for an MSE loss), and produces the curve /
+// halation-strength / sigma partials, the gradient w.r.t. B (a plane) and
+// w.r.t. a (3 planes).  The halation blur is recomputed instead of stored; its
+// sigma-derivative uses derivative taps, and the gradient w.r.t. h is the
+// exact transpose of the mirror-reflect blur.  Parameter partials are summed
+// per block in f64 and reduced by one block in a fixed order (deterministic).
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "film.cuh"
+
+namespace imops {
+namespace adj {
+
+using film::HAL_R;
+using film::NB81;
+
+constexpr int NPAR = 24;  // wb3 C9 ev1 dmax3 k3 x03 s1 sigma1
+constexpr int BLK = 256;
+
+struct Const {
+    float wb[3], C[9], ev2, ev;
+    float dmax[3], k[3], x0[3], s, thr;
+    float minv[9];
+    float A[3][3];
+    float bleed[3];
+    float eps[3][NB81];
+    float Cs[NB81][3];
+};
+
+__device__ __forceinline__ void color_fwd(const Const& c, const float* x, float y[3], float a[3]) {
+    for (int i = 0; i < 3; i++) y[i] = c.ev2 * (c.wb[i] * x[i]);
+    for (int i = 0; i < 3; i++) a[i] = c.C[3 * i] * y[0] + c.C[3 * i + 1] * y[1] + c.C[3 * i + 2] * y[2];
+}
+
+__global__ void prep_kernel(const float* __restrict__ x, size_t n, const Const* __restrict__ cp, float* __restrict__ h) {
+    const Const& c = *cp;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        float y[3], a[3];
+        color_fwd(c, x + 3 * p, y, a);
+        h[p] = fmaxf(0.0f, a[0] - c.thr);
+    }
+}
+
+// Per-pixel forward (and optionally backward).  MODE 0: write out.  MODE 1:
+// backward with g_out or target; writes gB (plane) and ga (3 planes) and the
+// block partials of dmax, k, x0, s, sigma and the loss.
+template <int MODE>
+__global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x, const float* __restrict__ B,
+                                                    const float* __restrict__ Bs, const float* __restrict__ g_out,
+                                                    const float* __restrict__ target, float loss_scale, size_t n,
+                                                    const Const* __restrict__ cp, float* __restrict__ out,
+                                                    float* __restrict__ gB, float* __restrict__ ga,
+                                                    double* __restrict__ partial) {
+    __shared__ Const c;
+    for (int k = threadIdx.x; k < (int)(sizeof(Const) / 4); k += blockDim.x)
+        reinterpret_cast<float*>(&c)[k] = reinterpret_cast<const float*>(cp)[k];
+    __syncthreads();
+    // partials: dmax0-2 (0..2), k0-2 (3..5), x00-2 (6..8), s (9), sigma (10), loss (11)
+    float acc[12];
+    for (int i = 0; i < 12; i++) acc[i] = 0.0f;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        float y[3], a[3];
+        color_fwd(c, x + 3 * p, y, a);
+        float w[3];
+        for (int k = 0; k < 3; k++) w[k] = c.minv[3 * k] * a[0] + c.minv[3 * k + 1] * a[1] + c.minv[3 * k + 2] * a[2];
+        float b = B[p];
+        float E[3], le[3], sg[3], D[3];
+        for (int l = 0; l < 3; l++) {
+            float e = fmaxf(w[0], 0.0f) * c.A[0][l] + fmaxf(w[1], 0.0f) * c.A[1][l] + fmaxf(w[2], 0.0f) * c.A[2][l];
+            E[l] = e + c.s * c.bleed[l] * b;
+            le[l] = log10f(fmaxf(E[l], 1e-6f));
+            sg[l] = 1.0f / (1.0f + expf(-c.k[l] * (le[l] - c.x0[l])));
+            D[l] = c.dmax[l] * sg[l];
+        }
+        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+#pragma unroll 9
+        for (int l = 0; l < NB81; l++) {
+            float d = D[0] * c.eps[0][l];
+            d = fmaf(D[1], c.eps[1][l], d);
+            d = fmaf(D[2], c.eps[2][l], d);
+            float t = exp2f(-d);
+            o0 = fmaf(c.Cs[l][0], t, o0);
+            o1 = fmaf(c.Cs[l][1], t, o1);
+            o2 = fmaf(c.Cs[l][2], t, o2);
+        }
+        if (MODE == 0) {
+            out[3 * p] = o0;
+            out[3 * p + 1] = o1;
+            out[3 * p + 2] = o2;
+            continue;
+        }
+        float go[3];
+        if (g_out) {
+            go[0] = g_out[3 * p];
+            go[1] = g_out[3 * p + 1];
+            go[2] = g_out[3 * p + 2];
+        } else {
+            float r0 = o0 - target[3 * p], r1 = o1 - target[3 * p + 1], r2 = o2 - target[3 * p + 2];
+            acc[11] += loss_scale * (r0 * r0 + r1 * r1 + r2 * r2);
+            go[0] = 2.0f * loss_scale * r0;
+            go[1] = 2.0f * loss_scale * r1;
+            go[2] = 2.0f * loss_scale * r2;
+        }
+        // scan backward: gD_l = sum_lambda eps'_l (-ln2 T gT); T is recomputed
+        // (same arithmetic as above) instead of kept per bin
+        float gD0 = 0.f, gD1 = 0.f, gD2 = 0.f;
+#pragma unroll 9
+        for (int l = 0; l < NB81; l++) {
+            float d = D[0] * c.eps[0][l];
+            d = fmaf(D[1], c.eps[1][l], d);
+            d = fmaf(D[2], c.eps[2][l], d);
+            float t = exp2f(-d);
+            float gT = c.Cs[l][0] * go[0] + c.Cs[l][1] * go[1] + c.Cs[l][2] * go[2];
+            float gd = -0.69314718055994531f * t * gT;
+            gD0 = fmaf(c.eps[0][l], gd, gD0);
+            gD1 = fmaf(c.eps[1][l], gd, gD1);
+            gD2 = fmaf(c.eps[2][l], gd, gD2);
+        }
+        float gD[3] = {gD0, gD1, gD2};
+        float gE[3];
+        for (int l = 0; l < 3; l++) {
+            float ds = sg[l] * (1.0f - sg[l]);
+            acc[l] += gD[l] * sg[l];
+            acc[3 + l] += gD[l] * c.dmax[l] * ds * (le[l] - c.x0[l]);
+            acc[6 + l] += -gD[l] * c.dmax[l] * ds * c.k[l];
+            gE[l] = E[l] > 1e-6f ? gD[l] * c.dmax[l] * ds * c.k[l] / (E[l] * 2.302585092994046f) : 0.0f;
+        }
+        float gb = c.s * (c.bleed[0] * gE[0] + c.bleed[1] * gE[1] + c.bleed[2] * gE[2]);
+        acc[9] += (c.bleed[0] * gE[0] + c.bleed[1] * gE[1] + c.bleed[2] * gE[2]) * b;
+        acc[10] += gb * Bs[p];
+        gB[p] = gb;
+        float gw[3];
+        for (int k = 0; k < 3; k++)
+            gw[k] = w[k] > 0.0f ? c.A[k][0] * gE[0] + c.A[k][1] * gE[1] + c.A[k][2] * gE[2] : 0.0f;
+        for (int j = 0; j < 3; j++) ga[j * n + p] = c.minv[j] * gw[0] + c.minv[3 + j] * gw[1] + c.minv[6 + j] * gw[2];
+    }
+    if (MODE == 0) return;
+    // block reduction in f64
+    __shared__ double red[12][BLK / 32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = 0; i < 12; i++) {
+        double v = (double)acc[i];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[i][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        double v = 0.0;
+        for (int k = 0; k < (int)(blockDim.x / 32); k++) v += red[threadIdx.x][k];
+        partial[(size_t)blockIdx.x * 12 + threadIdx.x] = v;
+    }
+}
+
+// Colour backward: ga (+ the halation path through h) -> C, ev, wb partials.
+__global__ void __launch_bounds__(BLK) color_back_kernel(const float* __restrict__ x, const float* __restrict__ ga,
+                                                         const float* __restrict__ gh, size_t n,
+                                                         const Const* __restrict__ cp,
+                                                         double* __restrict__ partial) {
+    __shared__ Const c;
+    for (int k = threadIdx.x; k < (int)(sizeof(Const) / 4); k += blockDim.x)
+        reinterpret_cast<float*>(&c)[k] = reinterpret_cast<const float*>(cp)[k];
+    __syncthreads();
+    // wb0-2 (0..2), C00..C22 (3..11), ev (12)
+    float acc[13];
+    for (int i = 0; i < 13; i++) acc[i] = 0.0f;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        float y[3], a[3];
+        const float* xp = x + 3 * p;
+        color_fwd(c, xp, y, a);
+        float g[3] = {ga[p], ga[n + p], ga[2 * n + p]};
+        if (a[0] - c.thr > 0.0f) g[0] += gh[p];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) acc[3 + 3 * i + j] += g[i] * y[j];
+        float gy[3];
+        for (int j = 0; j < 3; j++) gy[j] = c.C[j] * g[0] + c.C[3 + j] * g[1] + c.C[6 + j] * g[2];
+        acc[12] += 0.69314718055994531f * (gy[0] * y[0] + gy[1] * y[1] + gy[2] * y[2]);
+        for (int j = 0; j < 3; j++) acc[j] += gy[j] * c.ev2 * xp[j];
+    }
+    __shared__ double red[13][BLK / 32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = 0; i < 13; i++) {
+        double v = (double)acc[i];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[i][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 13) {
+        double v = 0.0;
+        for (int k = 0; k < (int)(blockDim.x / 32); k++) v += red[threadIdx.x][k];
+        partial[(size_t)blockIdx.x * 13 + threadIdx.x] = v;
+    }
+}
+
+// One block: sum the partials in block order and add into grad[25]
+// (24 parameters + loss), in the parameter order of ImopsFilmGradParams.
+__global__ void finish_kernel(const double* __restrict__ p1, int nb1, const double* __restrict__ p2, int nb2,
+                              double* __restrict__ grad) {
+    int t = threadIdx.x;
+    if (t < 12) {
+        double v = 0.0;
+        for (int b = 0; b < nb1; b++) v += p1[(size_t)b * 12 + t];
+        // p1 order: dmax(0..2) k(3..5) x0(6..8) s(9) sigma(10) loss(11)
+        int dst = t < 9 ? 13 + t : (t == 9 ? 22 : (t == 10 ? 23 : 24));
+        grad[dst] += v;
+    } else if (t >= 32 && t < 32 + 13) {
+        int i = t - 32;
+        double v = 0.0;
+        for (int b = 0; b < nb2; b++) v += p2[(size_t)b * 13 + i];
+        // p2 order: wb(0..2) C(3..11) ev(12) -> grad wb(0..2) C(3..11) ev(12)
+        grad[i] += v;
+    }
+}
+
+// Transposed mirror-reflect 1-D convolution (adjoint of blur.rs's pass):
+// out[y] = sum_k w_k * sum_{x: refl(x+k-R) = y} in[x].  Requires n > R + 1
+// (then only single reflections occur).
+__global__ void blurT_rows_kernel(const float* __restrict__ in, float* __restrict__ out, int W, int H, const float* __restrict__ taps, int R) {
+    size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        int y = (int)(p % W);
+        const float* row = in + (p - y);
+        float acc = 0.0f;
+        for (int k = 0; k <= 2 * R; k++) {
+            float wk = taps[k];
+            int x0 = y - k + R;
+            if (x0 >= 0 && x0 < W) acc = fmaf(wk, row[x0], acc);
+            if (y >= 1) {
+                int x1 = -y - k + R;
+                if (x1 >= 0 && x1 < W) acc = fmaf(wk, row[x1], acc);
+            }
+            if (y <= W - 2) {
+                int x2 = 2 * W - 2 - y - k + R;
+                if (x2 >= 0 && x2 < W) acc = fmaf(wk, row[x2], acc);
+            }
+        }
+        out[p] = acc;
+    }
+}
+
+__global__ void blurT_cols_kernel(const float* __restrict__ in, float* __restrict__ out, int W, int H, const float* __restrict__ taps, int R) {
+    size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        int xcol = (int)(p % W), y = (int)(p / W);
+        float acc = 0.0f;
+        for (int k = 0; k <= 2 * R; k++) {
+            float wk = taps[k];
+            int y0 = y - k + R;
+            if (y0 >= 0 && y0 < H) acc = fmaf(wk, in[(size_t)y0 * W + xcol], acc);
+            if (y >= 1) {
+                int y1 = -y - k + R;
+                if (y1 >= 0 && y1 < H) acc = fmaf(wk, in[(size_t)y1 * W + xcol], acc);
+            }
+            if (y <= H - 2) {
+                int y2 = 2 * H - 2 - y - k + R;
+                if (y2 >= 0 && y2 < H) acc = fmaf(wk, in[(size_t)y2 * W + xcol], acc);
+            }
+        }
+        out[p] = acc;
+    }
+}
+
+// ---- host ---------------------------------------------------------------------
+
+struct Workspace {
+    std::mutex mu;
+    struct E {
+        int dev;
+        cudaStream_t s;
+        void* p;
+        size_t bytes;
+    };
+    std::vector<E> v;
+};
+Workspace g_ws;
+
+int workspace(cudaStream_t s, size_t bytes, void** out) {
+    if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, "injected allocation failure (adjoint workspace)");
+    int dev = 0;
+    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(g_ws.mu);
+    for (auto& e : g_ws.v)
+        if (e.dev == dev && e.s == s) {
+            if (e.bytes < bytes) {
+                IMOPS_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+                IMOPS_CUDA_TRY(cudaFree(e.p), "cudaFree");
+                e.p = nullptr;
+                e.bytes = 0;
+                IMOPS_CUDA_TRY(cudaMalloc(&e.p, bytes), "cudaMalloc(adjoint workspace)");
+                e.bytes = bytes;
+            }
+            *out = e.p;
+            return IMOPS_OK;
+        }
+    void* p = nullptr;
+    IMOPS_CUDA_TRY(cudaMalloc(&p, bytes), "cudaMalloc(adjoint workspace)");
+    g_ws.v.push_back({dev, s, p, bytes});
+    *out = p;
+    return IMOPS_OK;
+}
+
+struct Arena {
+    char* base;
+    size_t off;
+    template <class T>
+    T* take(size_t count) {
+        size_t a = (off + 255) & ~(size_t)255;
+        T* p = reinterpret_cast<T*>(base + a);
+        off = a + count * sizeof(T);
+        return p;
+    }
+};
+
+// Halation taps and their sigma-derivative for the fixed radius R:
+// w_i = g_i / S, g_i = exp(-x_i^2 / (2 s^2)); dw_i/ds = w_i (x_i^2 - sum_j w_j x_j^2) / s^3.
+void halation_taps(float sigma, int R, float* t, float* dt) {
+    double sum = 0.0, m2 = 0.0;
+    std::vector<double> g(2 * R + 1);
+    for (int i = 0; i <= 2 * R; i++) {
+        double x = i - R;
+        g[i] = std::exp(-x * x / (2.0 * sigma * sigma));
+        sum += g[i];
+    }
+    for (int i = 0; i <= 2 * R; i++) {
+        double x = i - R;
+        m2 += g[i] / sum * x * x;
+    }
+    double s3 = (double)sigma * sigma * sigma;
+    for (int i = 0; i <= 2 * R; i++) {
+        double x = i - R, w = g[i] / sum;
+        t[i] = (float)w;
+        dt[i] = (float)(w * (x * x - m2) / s3);
+    }
+}
+
+int build_const(const ImopsFilmGradParams& P, const ImopsBaselineFilm& F, Const* c, float* taps, float* dtaps) {
+    film::Stock st;
+    float pitch;
+    ImopsBaselineFilm f2 = F;
+    f2.grain_on = 0;
+    int rc = film::build_stock(IMOPS_STOCK_BASELINE81, 0, 1, -1.0f, &f2, &st, &pitch);
+    if (rc) return rc;
+    for (int i = 0; i < 3; i++) c->wb[i] = P.wb[i];
+    for (int i = 0; i < 9; i++) c->C[i] = P.matrix[i];
+    c->ev = P.ev;
+    c->ev2 = std::exp2(P.ev);
+    for (int l = 0; l < 3; l++) {
+        c->dmax[l] = P.dmax[l];
+        c->k[l] = P.k[l];
+        c->x0[l] = P.x0[l];
+        c->bleed[l] = st.base.bleed[l];
+    }
+    c->s = P.hal_strength;
+    c->thr = F.hal_threshold;
+    for (int i = 0; i < 9; i++) c->minv[i] = st.expose.minv[i];
+    for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) c->A[k][l] = st.expose.A[k][l];
+    for (int l = 0; l < 3; l++)
+        for (int i = 0; i < NB81; i++) c->eps[l][i] = st.scan81.eps[l][i];
+    for (int i = 0; i < NB81; i++)
+        for (int j = 0; j < 3; j++) c->Cs[i][j] = st.scan81.C[i][j];
+    if (F.hal_radius < 1 || F.hal_radius > HAL_R) return fail(IMOPS_ERR_INVALID_ARGUMENT, "hal_radius must be 1..64");
+    if (!(P.hal_sigma > 0.0f)) return fail(IMOPS_ERR_INVALID_ARGUMENT, "hal_sigma must be > 0");
+    halation_taps(P.hal_sigma, F.hal_radius, taps, dtaps);
+    return IMOPS_OK;
+}
+
+struct Bufs {
+    Const* c;
+    float *taps, *dtaps;
+    float *h, *t1, *B, *t2, *Bs, *gB, *t3, *gh, *ga;
+    double *p1, *p2;
+    int nb;
+};
+
+int prepare(const float* x, int W, int H, const ImopsFilmGradParams* P, const ImopsBaselineFilm* F, bool backward,
+            cudaStream_t s, Bufs* b) {
+    if (!x || !P) return fail(IMOPS_ERR_INVALID_ARGUMENT, "param film: NULL argument");
+    if (W <= 0 || H <= 0) return fail(IMOPS_ERR_INVALID_DIMENSIONS, "invalid image dimensions");
+    ImopsBaselineFilm Fd;
+    if (F) Fd = *F;
+    else imops_baseline_film_defaults(&Fd);
+    if (backward && (W <= Fd.hal_radius + 1 || H <= Fd.hal_radius + 1))
+        return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "param film backward: image sides must exceed the halation radius + 1");
+    const size_t n = (size_t)W * H;
+    b->nb = film::grid_for_n(n);
+    size_t bytes = sizeof(Const) + 2 * (2 * HAL_R + 1) * 4 + (backward ? 12 : 3) * n * 4 +
+                   (size_t)b->nb * 25 * 8 + 8192;
+    void* ws = nullptr;
+    int rc = workspace(s, bytes, &ws);
+    if (rc) return rc;
+    Arena A{static_cast<char*>(ws), 0};
+    b->c = A.take<Const>(1);
+    b->taps = A.take<float>(2 * HAL_R + 1);
+    b->dtaps = A.take<float>(2 * HAL_R + 1);
+    b->h = A.take<float>(n);
+    b->t1 = A.take<float>(n);
+    b->B = A.take<float>(n);
+    if (backward) {
+        b->t2 = A.take<float>(n);
+        b->Bs = A.take<float>(n);
+        b->gB = A.take<float>(n);
+        b->t3 = A.take<float>(n);
+        b->gh = A.take<float>(n);
+        b->ga = A.take<float>(3 * n);
+        b->p1 = A.take<double>((size_t)b->nb * 12);
+        b->p2 = A.take<double>((size_t)b->nb * 13);
+    }
+    Const hc;
+    std::vector<float> taps(2 * HAL_R + 1), dtaps(2 * HAL_R + 1);
+    if ((rc = build_const(*P, Fd, &hc, taps.data(), dtaps.data()))) return rc;
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(b->c, &hc, sizeof(Const), cudaMemcpyHostToDevice, s), "copy constants");
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(b->taps, taps.data(), taps.size() * 4, cudaMemcpyHostToDevice, s), "copy taps");
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(b->dtaps, dtaps.data(), dtaps.size() * 4, cudaMemcpyHostToDevice, s), "copy taps");
+    const int R = Fd.hal_radius;
+    prep_kernel<<<b->nb, BLK, 0, s>>>(x, n, b->c, b->h);
+    note_launch();
+    if ((rc = film::blur_rows(b->h, b->t1, W, H, taps.data(), R, s))) return rc;
+    if ((rc = film::blur_cols(b->t1, b->B, W, H, taps.data(), R, 0, s))) return rc;
+    if (backward) {
+        // dB/dsigma = cols_G(rows_dG(h)) + cols_dG(rows_G(h))
+        if ((rc = film::blur_rows(b->h, b->t2, W, H, dtaps.data(), R, s))) return rc;
+        if ((rc = film::blur_cols(b->t2, b->Bs, W, H, taps.data(), R, 0, s))) return rc;
+        if ((rc = film::blur_cols(b->t1, b->Bs, W, H, dtaps.data(), R, 1, s))) return rc;
+    }
+    return IMOPS_OK;
+}
+
+}  // namespace adj
+}  // namespace imops
+
+using namespace imops;
+
+extern "C" int imops_param_forward(const float* cam_rgb, int w, int h, const ImopsFilmGradParams* params,
+                                   const ImopsBaselineFilm* fixed, float* out, imops_stream_t stream) {
+    clear_error();
+    if (!out) return fail(IMOPS_ERR_INVALID_ARGUMENT, "param forward: NULL output");
+    cudaStream_t s = as_stream(stream);
+    adj::Bufs b;
+    int rc = adj::prepare(cam_rgb, w, h, params, fixed, false, s, &b);
+    if (rc) return rc;
+    adj::pixel_kernel<0><<<b.nb, adj::BLK, 0, s>>>(cam_rgb, b.B, nullptr, nullptr, nullptr, 0.0f, (size_t)w * h, b.c,
+                                                   out, nullptr, nullptr, nullptr);
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "param forward");
+    return IMOPS_OK;
+}
+
+extern "C" int imops_param_backward(const float* cam_rgb, const float* g_out, const float* target, float loss_scale,
+                                    int w, int h, const ImopsFilmGradParams* params, const ImopsBaselineFilm* fixed,
+                                    double* grad, imops_stream_t stream) {
+    clear_error();
+    if (!grad) return fail(IMOPS_ERR_INVALID_ARGUMENT, "param backward: NULL gradient buffer");
+    if (!g_out && !target) return fail(IMOPS_ERR_INVALID_ARGUMENT, "param backward: need g_out or target");
+    cudaStream_t s = as_stream(stream);
+    adj::Bufs b;
+    int rc = adj::prepare(cam_rgb, w, h, params, fixed, true, s, &b);
+    if (rc) return rc;
+    const size_t n = (size_t)w * h;
+    ImopsBaselineFilm Fd;
+    if (fixed) Fd = *fixed;
+    else imops_baseline_film_defaults(&Fd);
+    const int R = Fd.hal_radius;
+    adj::pixel_kernel<1><<<b.nb, adj::BLK, 0, s>>>(cam_rgb, b.B, b.Bs, g_out, target, loss_scale, n, b.c, nullptr,
+                                                   b.gB, b.ga, b.p1);
+    note_launch();
+    // gh = rows^T(cols^T(gB)) with the same taps (the blur is rows then cols)
+    adj::blurT_cols_kernel<<<b.nb, adj::BLK, 0, s>>>(b.gB, b.t3, w, h, b.taps, R);
+    note_launch();
+    adj::blurT_rows_kernel<<<b.nb, adj::BLK, 0, s>>>(b.t3, b.gh, w, h, b.taps, R);
+    note_launch();
+    adj::color_back_kernel<<<b.nb, adj::BLK, 0, s>>>(cam_rgb, b.ga, b.gh, n, b.c, b.p2);
+    note_launch();
+    adj::finish_kernel<<<1, 64, 0, s>>>(b.p1, b.nb, b.p2, b.nb, grad);
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "param backward");
+    return IMOPS_OK;
+}

@@ -145,6 +145,36 @@ __global__ void sumsq_kernel(const float* __restrict__ v, size_t n, double* __re
     if (threadIdx.x == 0) atomicAdd(out, sh[0]);
 }
 
+struct EpiAdd {
+    float* out;
+    __device__ __forceinline__ void operator()(size_t i, float v) const { out[i] += v; }
+};
+
+int blur_rows(const float* in, float* out, int W, int H, const float* taps, int R, cudaStream_t s) {
+    if (R < 0 || R > MAXR) return fail(IMOPS_ERR_INVALID_ARGUMENT, "blur radius above 64");
+    Taps tp;
+    tp.R = R;
+    for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
+    dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
+    blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(in, out, W, H, tp);
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "blur rows");
+    return IMOPS_OK;
+}
+
+int blur_cols(const float* in, float* out, int W, int H, const float* taps, int R, int add, cudaStream_t s) {
+    if (R < 0 || R > MAXR) return fail(IMOPS_ERR_INVALID_ARGUMENT, "blur radius above 64");
+    Taps tp;
+    tp.R = R;
+    for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
+    dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
+    if (add) blur_cols_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiAdd{out});
+    else blur_cols_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiStore{out});
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "blur cols");
+    return IMOPS_OK;
+}
+
 int taps_for(float sigma, Taps* tp) {
     int r = gaussian_taps(sigma, tp->t, 2 * MAXR + 1);
     if (r < 0) return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "film: blur radius above 64 px (pixel pitch too small)");
@@ -442,6 +472,8 @@ int grid_for(size_t n) {
     size_t g = (n + 255) / 256, cap = (size_t)sm_count() * 8;
     return (int)(g < 1 ? 1 : (g > cap ? cap : g));
 }
+
+int grid_for_n(size_t n) { return grid_for(n); }
 
 // Bump allocator over the workspace.
 struct Arena {

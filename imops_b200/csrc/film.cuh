@@ -101,6 +101,13 @@ int build_stock(int stock_id, int film_format, int W, float shutter_seconds, con
 // exp(-x^2/(2 sigma^2)) in f32, normalised by their f32 sum.  Returns the radius.
 int gaussian_taps(float sigma, float* taps, int max_taps);
 
+// Separable-blur launchers shared with the adjoint (film.cu).  taps: 2R+1
+// weights (R <= 64), mirror reflection at the edges (blur.rs:70-89).
+int blur_rows(const float* in, float* out, int W, int H, const float* taps, int R, cudaStream_t s);
+// out = blur_cols(in) (add == 0) or out += blur_cols(in) (add == 1)
+int blur_cols(const float* in, float* out, int W, int H, const float* taps, int R, int add, cudaStream_t s);
+int grid_for_n(size_t n);
+
 // Relative -> absolute luminance of a value at sunny-16 for a box ISO
 // (film/mod.rs:155-166).
 float relative_to_absolute_y(float y, float box_iso);

@@ -240,6 +240,37 @@ int imops_develop_f32(const float *mosaic, int w, int h, int shift_x, int shift_
  * counter for benchmarks; monotone, thread-safe). */
 uint64_t imops_launch_count(void);
 
+/* ---- adjoints (no counterpart in the reference, which has no gradients) ----
+ * Parameters of the differentiable colour + film model, from demosaiced
+ * camera RGB x (demosaic decisions held fixed):
+ *   y = 2^ev (wb * x);  a = matrix y (ACEScg);  exposure a -> 3 layers;
+ *   halation G_sigma * max(0, a_R - threshold) added with hal_strength * bleed;
+ *   logistic curves (dmax, k, x0); 81-bin scan -> out (ACEScg negative).
+ * Fixed settings (threshold, tap radius) come from an ImopsBaselineFilm;
+ * grain is off.  24 parameters, gradient order as the fields below. */
+typedef struct {
+    float wb[3];
+    float matrix[9];        /* camera RGB -> ACEScg, row-major */
+    float ev;
+    float dmax[3], k[3], x0[3];
+    float hal_strength;
+    float hal_sigma;
+} ImopsFilmGradParams;
+
+/* out (w*h*3) = model(cam_rgb); fixed may be NULL (defaults). */
+int imops_param_forward(const float *cam_rgb, int w, int h, const ImopsFilmGradParams *params,
+                        const ImopsBaselineFilm *fixed, float *out, imops_stream_t stream);
+
+/* Adds the gradient of a scalar loss w.r.t. the 24 parameters to grad[0..23]
+ * and the loss to grad[24] (DEVICE doubles, not cleared: accumulate over a
+ * batch).  Either g_out (dL/dout, w*h*3) is given, or target is and the loss
+ * is loss_scale * sum((out - target)^2) (e.g. loss_scale = 1/(3 N) for an
+ * MSE over N pixels).  Halation is recomputed, not stored.  Requires
+ * w, h > hal_radius + 1. */
+int imops_param_backward(const float *cam_rgb, const float *g_out, const float *target, float loss_scale, int w,
+                         int h, const ImopsFilmGradParams *params, const ImopsBaselineFilm *fixed, double *grad,
+                         imops_stream_t stream);
+
 /* ---- pipeline-level C-ABI -------------------------------------------------
  * The embedding interface of pichromatic-pipeline/src/extern_pipeline.rs
  * (get_pixel_pipeline_c :326-341, run_pixel_pipeline_c :343-359,

@@ -336,3 +336,59 @@ def film_baseline(rgb: np.ndarray, params: OracleBaseline | None = None, precisi
     fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OracleBaseline), ctypes.c_int]
     _check(fn(_ptr(out), W, H, ctypes.byref(p), threads or os.cpu_count()), "film_baseline")
     return out
+
+
+class OracleGrad(ctypes.Structure):
+    """Parameters of the differentiable colour + film model (mirrors OGrad /
+    ImopsFilmGradParams): wb3, matrix9, ev, dmax3, k3, x03, hal_strength, hal_sigma."""
+
+    _fields_ = [("wb", ctypes.c_float * 3), ("matrix", ctypes.c_float * 9), ("ev", ctypes.c_float),
+                ("dmax", ctypes.c_float * 3), ("k", ctypes.c_float * 3), ("x0", ctypes.c_float * 3),
+                ("hal_strength", ctypes.c_float), ("hal_sigma", ctypes.c_float)]
+
+    def to_vector(self) -> np.ndarray:
+        return np.array(list(self.wb) + list(self.matrix) + [self.ev] + list(self.dmax) + list(self.k) +
+                        list(self.x0) + [self.hal_strength, self.hal_sigma], dtype=np.float64)
+
+    @classmethod
+    def from_vector(cls, v) -> "OracleGrad":
+        g = cls()
+        v = list(map(float, v))
+        for i in range(3):
+            g.wb[i] = v[i]
+        for i in range(9):
+            g.matrix[i] = v[3 + i]
+        g.ev = v[12]
+        for i in range(3):
+            g.dmax[i], g.k[i], g.x0[i] = v[13 + i], v[16 + i], v[19 + i]
+        g.hal_strength, g.hal_sigma = v[22], v[23]
+        return g
+
+
+def param_forward(x: np.ndarray, params: OracleGrad, fixed: OracleBaseline | None = None) -> np.ndarray:
+    """FP64 forward of the differentiable model from camera RGB (H, W, 3)."""
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    H, W = xx.shape[:2]
+    out = np.zeros_like(xx)
+    f = fixed if fixed is not None else baseline_params(grain_on=0)
+    fn = lib().oracle_param_forward_f64
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OracleGrad),
+                   ctypes.POINTER(OracleBaseline), ctypes.c_void_p]
+    _check(fn(_ptr(xx), W, H, ctypes.byref(params), ctypes.byref(f), _ptr(out)), "param_forward")
+    return out
+
+
+def param_grad(x: np.ndarray, target: np.ndarray, params: OracleGrad, scale: float,
+               fixed: OracleBaseline | None = None) -> np.ndarray:
+    """Analytic FP64 gradient of scale * sum((out - target)^2); returns 25
+    values (24 parameter gradients, then the loss)."""
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    tt = np.ascontiguousarray(target, dtype=np.float64)
+    H, W = xx.shape[:2]
+    g = np.zeros(25)
+    f = fixed if fixed is not None else baseline_params(grain_on=0)
+    fn = lib().oracle_param_grad_f64
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OracleGrad),
+                   ctypes.POINTER(OracleBaseline), ctypes.c_double, ctypes.c_void_p]
+    _check(fn(_ptr(xx), _ptr(tt), W, H, ctypes.byref(params), ctypes.byref(f), scale, _ptr(g)), "param_grad")
+    return g

@@ -1230,3 +1230,256 @@ double OSYM(oracle_lut_build_sample)(double mu_ln, double sigma_ln, double k, do
     lut_build(&L);
     return lut_sample(&L, phi);
 }
+
+#ifndef ORACLE_F32
+/* ======================================================================= */
+/* Part 3: FP64 oracle of the library's differentiable colour + film model  */
+/* (the reference has no gradients).  Same model as the GPU adjoint:        */
+/*   y = 2^ev (wb*x); a = C y; w = max(0, Minv a); e = A^T w;               */
+/*   h = max(0, a_R - thr); B = G_sigma * h (fixed radius, mirror);         */
+/*   E = e + s bleed B; D = dmax / (1 + exp(-k (log10 max(E,1e-6) - x0)));  */
+/*   T = 10^(-sum D dye); out = AP1(sum trap cmf T) / peak.                 */
+/* The backward is analytic; the transposed blur is an explicit scatter.    */
+
+typedef struct {
+    float wb[3], matrix[9], ev;
+    float dmax[3], k[3], x0[3];
+    float hal_strength, hal_sigma;
+} OGrad;
+
+static void g_taps(double sigma, int R, double *t, double *dt)
+{
+    double sum = 0, m2 = 0;
+    for (int i = 0; i <= 2 * R; i++) {
+        double x = i - R;
+        t[i] = exp(-x * x / (2 * sigma * sigma));
+        sum += t[i];
+    }
+    for (int i = 0; i <= 2 * R; i++) {
+        t[i] /= sum;
+        double x = i - R;
+        m2 += t[i] * x * x;
+    }
+    for (int i = 0; i <= 2 * R; i++) {
+        double x = i - R;
+        dt[i] = t[i] * (x * x - m2) / (sigma * sigma * sigma);
+    }
+}
+
+/* out = cols(rows(in)) with taps tr (rows) and tc (cols), mirror reflection */
+static void conv2(const double *in, double *out, int W, int H, const double *tr, const double *tc, int R)
+{
+    double *tmp = (double *)malloc(sizeof(double) * (size_t)W * H);
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            double acc = 0;
+            for (int k = 0; k <= 2 * R; k++) acc += in[(size_t)y * W + reflect_index((long)x + k - R, W)] * tr[k];
+            tmp[(size_t)y * W + x] = acc;
+        }
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            double acc = 0;
+            for (int k = 0; k <= 2 * R; k++) acc += tmp[(size_t)reflect_index((long)y + k - R, H) * W + x] * tc[k];
+            out[(size_t)y * W + x] = acc;
+        }
+    free(tmp);
+}
+
+/* transpose of conv2 (scatter form): out = rows^T(cols^T(in)) */
+static void conv2_T(const double *in, double *out, int W, int H, const double *t, int R)
+{
+    size_t n = (size_t)W * H;
+    double *tmp = (double *)calloc(n, sizeof(double));
+    memset(out, 0, n * sizeof(double));
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++)
+            for (int k = 0; k <= 2 * R; k++)
+                tmp[(size_t)reflect_index((long)y + k - R, H) * W + x] += t[k] * in[(size_t)y * W + x];
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++)
+            for (int k = 0; k <= 2 * R; k++)
+                out[(size_t)y * W + reflect_index((long)x + k - R, W)] += t[k] * tmp[(size_t)y * W + x];
+    free(tmp);
+}
+
+typedef struct { B81 b; double peak; double ev2; } GCtx;
+
+static void g_color(const OGrad *P, double ev2, const double *x, double y[3], double a[3])
+{
+    for (int i = 0; i < 3; i++) y[i] = ev2 * ((double)P->wb[i] * x[i]);
+    for (int i = 0; i < 3; i++)
+        a[i] = (double)P->matrix[3 * i] * y[0] + (double)P->matrix[3 * i + 1] * y[1] + (double)P->matrix[3 * i + 2] * y[2];
+}
+
+/* forward for every pixel; optionally returns B (per pixel) */
+int oracle_param_forward_f64(const double *x, int W, int H, const OGrad *P, const OBaseline *F, double *out)
+{
+    size_t n = (size_t)W * H;
+    GCtx g;
+    b81_build(&g.b);
+    double pk = g.b.white[0] > g.b.white[1] ? g.b.white[0] : g.b.white[1];
+    if (g.b.white[2] > pk) pk = g.b.white[2];
+    double ev2 = exp2((double)P->ev);
+    int R = F->hal_radius;
+    double *t = malloc(sizeof(double) * (2 * R + 1)), *dt = malloc(sizeof(double) * (2 * R + 1));
+    g_taps(P->hal_sigma, R, t, dt);
+    double *h = calloc(n + 1, sizeof(double)), *B = calloc(n + 1, sizeof(double));
+    for (size_t p = 0; p < n; p++) {
+        double y[3], a[3];
+        g_color(P, ev2, x + 3 * p, y, a);
+        double v = a[0] - (double)F->hal_threshold;
+        h[p] = v > 0 ? v : 0;
+    }
+    conv2(h, B, W, H, t, t, R);
+    for (size_t p = 0; p < n; p++) {
+        double y[3], a[3], w[3];
+        g_color(P, ev2, x + 3 * p, y, a);
+        matvec3(g.b.minv, a, w);
+        double D[3];
+        for (int l = 0; l < 3; l++) {
+            double e = 0;
+            for (int k = 0; k < 3; k++) {
+                double ak = 0;
+                for (int i = 0; i < NB81; i++) ak += g.b.trap[i] * g.b.basis[k][i] * g.b.sens[l][i];
+                e += (w[k] > 0 ? w[k] : 0) * (ak / g.b.sens_norm[l]);
+            }
+            double E = e + (double)P->hal_strength * BLEED[l] * B[p];
+            double le = log10(E > 1e-6 ? E : 1e-6);
+            D[l] = (double)P->dmax[l] / (1.0 + exp(-(double)P->k[l] * (le - (double)P->x0[l])));
+        }
+        double X = 0, Y = 0, Z = 0;
+        for (int i = 0; i < NB81; i++) {
+            double d = D[0] * g.b.dye[0][i] + D[1] * g.b.dye[1][i] + D[2] * g.b.dye[2][i];
+            double tt = pow(10.0, -d);
+            X += g.b.trap[i] * g.b.xb[i] * tt;
+            Y += g.b.trap[i] * g.b.yb[i] * tt;
+            Z += g.b.trap[i] * g.b.zb[i] * tt;
+        }
+        double xyz[3] = {X, Y, Z}, o[3];
+        matvec3(XYZ2AP1, xyz, o);
+        for (int c = 0; c < 3; c++) out[3 * p + c] = o[c] / pk;
+    }
+    free(t); free(dt); free(h); free(B);
+    return ORACLE_OK;
+}
+
+/* loss = scale * sum (out - target)^2; grad[0..23] += dloss/dparam, grad[24] += loss */
+int oracle_param_grad_f64(const double *x, const double *target, int W, int H, const OGrad *P, const OBaseline *F,
+                          double scale, double *grad)
+{
+    size_t n = (size_t)W * H;
+    GCtx g;
+    b81_build(&g.b);
+    double pk = g.b.white[0] > g.b.white[1] ? g.b.white[0] : g.b.white[1];
+    if (g.b.white[2] > pk) pk = g.b.white[2];
+    double A[3][3];
+    for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) {
+            double ak = 0;
+            for (int i = 0; i < NB81; i++) ak += g.b.trap[i] * g.b.basis[k][i] * g.b.sens[l][i];
+            A[k][l] = ak / g.b.sens_norm[l];
+        }
+    double ev2 = exp2((double)P->ev);
+    int R = F->hal_radius;
+    double *t = malloc(sizeof(double) * (2 * R + 1)), *dt = malloc(sizeof(double) * (2 * R + 1));
+    g_taps(P->hal_sigma, R, t, dt);
+    double *h = calloc(n + 1, sizeof(double)), *B = calloc(n + 1, sizeof(double)), *Bs = calloc(n + 1, sizeof(double));
+    double *Bs2 = malloc(sizeof(double) * n), *gB = malloc(sizeof(double) * n), *gh = malloc(sizeof(double) * n);
+    double *ga = malloc(sizeof(double) * 3 * n);
+    for (size_t p = 0; p < n; p++) {
+        double y[3], a[3];
+        g_color(P, ev2, x + 3 * p, y, a);
+        double v = a[0] - (double)F->hal_threshold;
+        h[p] = v > 0 ? v : 0;
+    }
+    conv2(h, B, W, H, t, t, R);
+    conv2(h, Bs, W, H, dt, t, R);
+    conv2(h, Bs2, W, H, t, dt, R);
+    for (size_t p = 0; p < n; p++) Bs[p] += Bs2[p];
+    double gdmax[3] = {0}, gk[3] = {0}, gx0[3] = {0}, gs = 0, gsig = 0, loss = 0;
+    const double LN10 = 2.302585092994045684;
+    for (size_t p = 0; p < n; p++) {
+        double y[3], a[3], w[3];
+        g_color(P, ev2, x + 3 * p, y, a);
+        matvec3(g.b.minv, a, w);
+        double E[3], le[3], sg[3], D[3];
+        for (int l = 0; l < 3; l++) {
+            double e = 0;
+            for (int k = 0; k < 3; k++) e += (w[k] > 0 ? w[k] : 0) * A[k][l];
+            E[l] = e + (double)P->hal_strength * BLEED[l] * B[p];
+            le[l] = log10(E[l] > 1e-6 ? E[l] : 1e-6);
+            sg[l] = 1.0 / (1.0 + exp(-(double)P->k[l] * (le[l] - (double)P->x0[l])));
+            D[l] = (double)P->dmax[l] * sg[l];
+        }
+        double T[NB81], X = 0, Y = 0, Z = 0;
+        for (int i = 0; i < NB81; i++) {
+            double d = D[0] * g.b.dye[0][i] + D[1] * g.b.dye[1][i] + D[2] * g.b.dye[2][i];
+            T[i] = pow(10.0, -d);
+            X += g.b.trap[i] * g.b.xb[i] * T[i];
+            Y += g.b.trap[i] * g.b.yb[i] * T[i];
+            Z += g.b.trap[i] * g.b.zb[i] * T[i];
+        }
+        double xyz[3] = {X, Y, Z}, o[3];
+        matvec3(XYZ2AP1, xyz, o);
+        double go[3];
+        for (int c = 0; c < 3; c++) {
+            double r = o[c] / pk - target[3 * p + c];
+            loss += scale * r * r;
+            go[c] = 2 * scale * r / pk;  /* through the /peak */
+        }
+        /* o = XYZ2AP1 * xyz -> g_xyz = XYZ2AP1^T go */
+        double gx = 0, gy = 0, gz = 0;
+        for (int c = 0; c < 3; c++) {
+            gx += XYZ2AP1[c][0] * go[c];
+            gy += XYZ2AP1[c][1] * go[c];
+            gz += XYZ2AP1[c][2] * go[c];
+        }
+        double gD[3] = {0, 0, 0};
+        for (int i = 0; i < NB81; i++) {
+            double gT = g.b.trap[i] * (g.b.xb[i] * gx + g.b.yb[i] * gy + g.b.zb[i] * gz);
+            double gd = -LN10 * T[i] * gT;
+            for (int l = 0; l < 3; l++) gD[l] += g.b.dye[l][i] * gd;
+        }
+        double gE[3];
+        for (int l = 0; l < 3; l++) {
+            double ds = sg[l] * (1 - sg[l]);
+            gdmax[l] += gD[l] * sg[l];
+            gk[l] += gD[l] * (double)P->dmax[l] * ds * (le[l] - (double)P->x0[l]);
+            gx0[l] += -gD[l] * (double)P->dmax[l] * ds * (double)P->k[l];
+            gE[l] = E[l] > 1e-6 ? gD[l] * (double)P->dmax[l] * ds * (double)P->k[l] / (E[l] * LN10) : 0.0;
+        }
+        double sb = BLEED[0] * gE[0] + BLEED[1] * gE[1] + BLEED[2] * gE[2];
+        gs += sb * B[p];
+        gB[p] = (double)P->hal_strength * sb;
+        gsig += gB[p] * Bs[p];
+        double gw[3];
+        for (int k = 0; k < 3; k++) gw[k] = w[k] > 0 ? A[k][0] * gE[0] + A[k][1] * gE[1] + A[k][2] * gE[2] : 0;
+        for (int j = 0; j < 3; j++)
+            ga[3 * p + j] = g.b.minv[0][j] * gw[0] + g.b.minv[1][j] * gw[1] + g.b.minv[2][j] * gw[2];
+    }
+    conv2_T(gB, gh, W, H, t, R);
+    for (size_t p = 0; p < n; p++) {
+        double y[3], a[3];
+        g_color(P, ev2, x + 3 * p, y, a);
+        double gg[3] = {ga[3 * p], ga[3 * p + 1], ga[3 * p + 2]};
+        if (a[0] - (double)F->hal_threshold > 0) gg[0] += gh[p];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) grad[3 + 3 * i + j] += gg[i] * y[j];
+        double gy3[3];
+        for (int j = 0; j < 3; j++)
+            gy3[j] = (double)P->matrix[j] * gg[0] + (double)P->matrix[3 + j] * gg[1] + (double)P->matrix[6 + j] * gg[2];
+        grad[12] += 0.69314718055994530942 * (gy3[0] * y[0] + gy3[1] * y[1] + gy3[2] * y[2]);
+        for (int j = 0; j < 3; j++) grad[j] += gy3[j] * ev2 * x[3 * p + j];
+    }
+    for (int l = 0; l < 3; l++) {
+        grad[13 + l] += gdmax[l];
+        grad[16 + l] += gk[l];
+        grad[19 + l] += gx0[l];
+    }
+    grad[22] += gs;
+    grad[23] += gsig;
+    grad[24] += loss;
+    free(t); free(dt); free(h); free(B); free(Bs); free(Bs2); free(gB); free(gh); free(ga);
+    return ORACLE_OK;
+}
+#endif
