@@ -99,3 +99,19 @@ def test_param_backward_with_upstream_gradient(gpu):
     im.param_backward(xd, p, g1, g_out=g_out)
     im.param_backward(xd, p, g2, target=td, loss_scale=scale)
     assert torch.allclose(g1[:24], g2[:24], rtol=1e-5, atol=1e-12)
+
+
+def test_autograd_function_matches_adjoint(gpu):
+    import sys
+    import torch
+    import imops_b200 as im
+    sys.path.insert(0, __import__("os").path.dirname(__import__("os").path.dirname(__file__)))
+    from experiments.film_autograd import film_model
+    _, _, xd, td = _setup(gpu, seed=66)
+    theta = torch.tensor(base_vector(), dtype=torch.float64, requires_grad=True)
+    out = film_model(xd, theta)
+    loss = ((out.double() - td.double()) ** 2).mean()
+    loss.backward()
+    ref = torch.zeros(25, dtype=torch.float64, device=gpu)
+    im.param_backward(xd, im.FilmGradParams.from_vector(base_vector()), ref, target=td, loss_scale=1.0 / xd.numel())
+    assert torch.allclose(theta.grad, ref[:24].cpu(), rtol=1e-4, atol=1e-12)
