@@ -263,6 +263,56 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_total = float(t.item())
 
+    # forward + backward of the differentiable colour + film model (24
+    # parameters: WB, camera->ACEScg matrix, EV, curves, halation) on the same
+    # frame: AMaZE to camera RGB, the model's forward, and its adjoint
+    # against a target rendered once with perturbed parameters.
+    p_cam = develop_params(im, film=False)
+    p_cam.target = im.CS_CAMERA
+    for i in range(4):
+        p_cam.wb[i] = 1.0
+    theta = im.FilmGradParams.from_vector(synthetic.film_grad_base())
+    cam = torch.empty((H, W, 3), device=dev)
+    fwd_out = torch.empty((H, W, 3), device=dev)
+    grad = torch.zeros(25, dtype=torch.float64, device=dev)
+    im.check(L.imops_develop_u16(ctypes.c_void_p(raw.data_ptr()), W, H, 0, 0, W, H, black, white, 2, 2,
+                                 ctypes.byref(p_cam), ctypes.c_void_p(cam.data_ptr()), sp))
+    target = im.param_forward(cam, im.FilmGradParams.from_vector(synthetic.film_grad_perturbed(2)), stream=stream)
+    loss_scale = 1.0 / (H * W * 3)
+
+    def step_fwd_bwd(events=None):
+        if events:
+            events[0].record(stream)
+        im.check(L.imops_develop_u16(ctypes.c_void_p(raw.data_ptr()), W, H, 0, 0, W, H, black, white, 2, 2,
+                                     ctypes.byref(p_cam), ctypes.c_void_p(cam.data_ptr()), sp))
+        im.param_forward(cam, theta, out=fwd_out, stream=stream)
+        if events:
+            events[1].record(stream)
+        grad.zero_()
+        im.param_backward(cam, theta, grad, target=target, loss_scale=loss_scale, stream=stream)
+        if events:
+            events[2].record(stream)
+
+    for _ in range(args.warmup):
+        step_fwd_bwd()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    evb = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        step_fwd_bwd(evb[k])
+    torch.cuda.synchronize()
+    t_fb = sum(e[0].elapsed_time(e[2]) for e in evb)
+    t_fb_fwd = sum(e[0].elapsed_time(e[1]) for e in evb) / args.steps
+    t_fb_bwd = sum(e[1].elapsed_time(e[2]) for e in evb) / args.steps
+    assert np.isfinite(grad.cpu().numpy()).all()
+    if dist:
+        t = torch.tensor([t_fb], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_fb = float(t.item())
+
     # end to end through the reference-facing C-ABI (extern_pipeline.rs names):
     # host u16 frame in, pipeline run, host f32 RGB out, image freed -- every
     # step.  Each call synchronises, so the host clock brackets the work.
@@ -297,6 +347,7 @@ def main():
     mp = H * W / 1e6
     value = world * mp * args.steps / (t_total / 1e3)
     e2e = world * mp * args.steps / (t_e2e / 1e3)
+    fwd_bwd = world * mp * args.steps / (t_fb / 1e3)
     bw, peak_kind = peaks()
     dom_bytes = H * W * 14  # u16 mosaic in (2 B) + f32 RGB out (12 B) per pixel
     achieved = dom_bytes / (t_dem / 1e3) / 1e9
@@ -310,6 +361,11 @@ def main():
                                    "81-bin film (halation, grain)", "global_batch": world, "frames_per_gpu": 1,
                        "parallelism": f"replicas x{world}", "l2": "256 MB buffer written between timed steps"},
             "stages_ms": {"amaze_colour": round(t_dem, 4), "film": round(t_film, 4)},
+            "fwd_bwd": {"value": round(fwd_bwd, 2), "unit": "MP/s", "ms_per_step": round(t_fb / args.steps, 4),
+                        "stages_ms": {"amaze_cam_plus_model_fwd": round(t_fb_fwd, 4),
+                                      "model_bwd": round(t_fb_bwd, 4)},
+                        "model": "24 params: WB 3, camera->ACEScg 9, EV, dmax/k/x0 per layer, halation strength/sigma; "
+                                 "81-bin scan, grain off; MSE to a perturbed-parameter target"},
             "roofline": {"bound": "hbm", "kernel": "amaze (fused u16 load + colour epilogue)",
                          "achieved": round(achieved, 2), "peak": bw, "unit": "GB/s",
                          "frac": round(achieved / bw, 5), "traffic": ncu_traffic(), "peak_kind": peak_kind,

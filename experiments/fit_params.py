@@ -1,4 +1,4 @@
-"""Parameter-fit workload: a batch of Bayer mosaics, loss
+"""Parameter-fit workload (8 x 2048x1365 Bayer frames): a batch of mosaics, loss
 = MSE to targets rendered with perturbed parameters, gradients w.r.t. the 24
 parameters (WB 3, colour matrix 9, exposure 1, curves 3x3, halation
 strength/sigma 2), plain gradient descent.
@@ -66,19 +66,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     H, W = a.height, a.width
-    XYZ2AP1 = np.array([[1.6410233797, -0.3248032942, -0.2364246952],
-                        [-0.6636628587, 1.6153315917, 0.0167563477],
-                        [0.0117218943, -0.0082844165, 0.9883948585]])
-    F = np.array(im.camera_forward_matrix(synthetic.CALIB_D65), dtype=np.float64).reshape(3, 3)
-    base = np.array([2.0, 1.0, 1.5, *(XYZ2AP1 @ F).reshape(9), 0.0, 2.0, 2.1, 2.2, 2.3, 2.5, 2.7, -0.70, -0.73,
-                     -0.76, 0.15, 20.0])
-    rng = np.random.default_rng(7)
-    truth = base.copy()
-    truth[0:3] *= 1 + rng.uniform(-0.05, 0.05, 3)
-    truth[3:12] += rng.uniform(-0.02, 0.02, 9)
-    truth[12] += rng.uniform(-0.1, 0.1)
-    truth[13:22] *= 1 + rng.uniform(-0.05, 0.05, 9)
-    truth[22:24] *= 1 + rng.uniform(-0.1, 0.1, 2)
+    base = synthetic.film_grad_base()
+    truth = synthetic.film_grad_perturbed(7)
 
     mine = shard(a.images, rank, world)
     cams, targets = [], []

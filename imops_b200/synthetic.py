@@ -69,3 +69,31 @@ CALIB_D65 = (0.6722, -0.0635, -0.0963,
              -0.4287, 1.2460, 0.2028,
              -0.0908, 0.2162, 0.5668)
 WB = (2.0, 1.0, 1.5, 0.0)
+
+# XYZ (D65) -> ACES AP1, the matrix the film model uses for ACEScg.
+XYZ2AP1 = np.array([[1.6410233797, -0.3248032942, -0.2364246952], [-0.6636628587, 1.6153315917, 0.0167563477],
+                    [0.0117218943, -0.0082844165, 0.9883948585]])
+
+
+def film_grad_base() -> np.ndarray:
+    """The 24 parameters of the differentiable colour + film model at the
+    workload's settings: WB, camera->ACEScg matrix (rows of the D65
+    calibration scaled to map D65 white to 1, inverted, then XYZ->AP1),
+    EV 0 and the baseline preset's curves and halation."""
+    M = np.array(CALIB_D65, np.float64).reshape(3, 3)
+    d65 = M @ np.array([0.95042, 1.0, 1.08890])
+    C = XYZ2AP1 @ np.linalg.inv(M / d65[:, None])
+    return np.array([*WB[:3], *C.reshape(9), 0.0, 2.0, 2.1, 2.2, 2.3, 2.5, 2.7, -0.70, -0.73, -0.76, 0.15, 20.0])
+
+
+def film_grad_perturbed(seed: int = 0) -> np.ndarray:
+    """film_grad_base() perturbed as the fitting workload does: +-5% WB,
+    +-0.02 matrix, +-0.1 EV, +-5% curve parameters, +-10% halation."""
+    rng = np.random.default_rng(seed)
+    v = film_grad_base()
+    v[0:3] *= 1 + rng.uniform(-0.05, 0.05, 3)
+    v[3:12] += rng.uniform(-0.02, 0.02, 9)
+    v[12] += rng.uniform(-0.1, 0.1)
+    v[13:22] *= 1 + rng.uniform(-0.05, 0.05, 9)
+    v[22:24] *= 1 + rng.uniform(-0.1, 0.1, 2)
+    return v

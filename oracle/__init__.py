@@ -310,7 +310,7 @@ def cmf81():
 
 
 def baseline_params(**kw) -> OracleBaseline:
-    """The baseline preset's defaults, overridable."""
+    """The baseline preset's defaults (the 24 MP film workload), overridable."""
     p = OracleBaseline()
     d = dict(dmax=(2.0, 2.1, 2.2), k=(2.3, 2.5, 2.7), x0=(-0.70, -0.73, -0.76), hal_strength=0.15,
              hal_sigma=20.0, hal_radius=64, hal_threshold=0.8, grain_sigma=0.02, grain_blur=1.0, grain_on=1,
