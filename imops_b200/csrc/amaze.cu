@@ -34,6 +34,7 @@ namespace amaze {
 constexpr int TS = 128, TSH = 64, NF = TS * TS, NH = TS * TSH;
 constexpr int V1 = 128, V2 = 256, V3 = 384, P1 = 127, P2 = 254, P3 = 381, M1 = 129, M2 = 258, M3 = 387;
 constexpr int NTHREADS = 512;
+static_assert(NTHREADS % TS == 0 && NTHREADS % TSH == 0, "row mapping of the stage loops");
 
 // global scratch per CTA slot: 8 full arrays, 14 half arrays, 2 byte maps
 constexpr size_t SLOT_FLOATS = 8 * (size_t)NF + 14 * (size_t)NH;
@@ -153,12 +154,9 @@ __device__ __forceinline__ float get_in(const P& p, int r, int q) {
 // dst(rr,cc) / src(rr,cc) give the flat index and the value.
 template <class Dst, class Src>
 __device__ __forceinline__ void fill_pass(float* mos, int r0, int r1, int c0, int c1, Dst dst, Src src) {
-    int w = c1 - c0, n = (r1 - r0) * w;
-    if (w <= 0 || n <= 0) return;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        int rr = r0 + k / w, cc = c0 + k % w;
-        mos[dst(rr, cc)] = src(rr, cc);
-    }
+    const int cc = c0 + (int)(threadIdx.x & (TS - 1));
+    if (cc >= c1) return;
+    for (int rr = r0 + (int)(threadIdx.x / TS); rr < r1; rr += NTHREADS / TS) mos[dst(rr, cc)] = src(rr, cc);
 }
 
 // Tile fill: demosaic.rs:499-610, passes in the reference's order so later
@@ -208,23 +206,127 @@ __device__ void fill(const P& p, const Geo& g, float* mos) {
 }
 
 // Loop helpers: every site of rows [r0,r1) x cols [c0,c1), and the R/B
-// sites of those rows (first R/B column = c0 + parity of the row).
+// sites of those rows (first R/B column = c0 + parity of the row; c0 even).
+// Threads map to (row group, column) directly: a tile row has at most 128
+// sites and 64 R/B sites, so no integer division is needed.
 template <class F>
 __device__ __forceinline__ void for_rect(int r0, int r1, int c0, int c1, F f) {
-    int w = c1 - c0, n = (r1 - r0) * w;
-    if (w <= 0 || r1 <= r0) return;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) f(r0 + k / w, c0 + k % w);
+    const int cc = c0 + (int)(threadIdx.x & (TS - 1));
+    if (cc >= c1) return;
+    for (int rr = r0 + (int)(threadIdx.x / TS); rr < r1; rr += NTHREADS / TS) f(rr, cc);
 }
 
 template <class F, class P>
 __device__ __forceinline__ void for_rb(const P& p, const Geo& g, int r0, int r1, int c0, int c1, F f) {
-    int w = (c1 - c0 + 1) / 2, n = (r1 - r0) * w;
-    if (w <= 0 || r1 <= r0) return;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        int rr = r0 + k / w;
-        int cc = c0 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k % w);
+    const int k = (int)(threadIdx.x & (TSH - 1));
+    for (int rr = r0 + (int)(threadIdx.x / TSH); rr < r1; rr += NTHREADS / TSH) {
+        int cc = c0 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * k;
         if (cc < c1) f(rr, cc);
     }
+}
+
+// A subset of the block's threads working one stage: thread t of n.
+struct Team {
+    int t, n;
+};
+__device__ __forceinline__ Team whole_block() { return Team{(int)threadIdx.x, NTHREADS}; }
+// warps 1.. of the block, while warp 0 runs a wavefront
+constexpr int WORKERS = NTHREADS - 32;
+__device__ __forceinline__ Team workers() { return Team{(int)threadIdx.x - 32, WORKERS}; }
+__device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, %0;" ::"r"(WORKERS) : "memory"); }
+
+// R/B sites of rows [r0,r1) x cols [c0,c1) split over a team (c0 even).
+template <class F, class P>
+__device__ __forceinline__ void for_rb_team(const P& p, const Geo& g, Team tm, int r0, int r1, int c0, int c1,
+                                            F f) {
+    const int n = (r1 - r0) * TSH;
+    for (int k = tm.t; k < n; k += tm.n) {
+        int rr = r0 + (k >> 6);
+        int cc = c0 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k & (TSH - 1));
+        if (cc < c1) f(rr, cc);
+    }
+}
+
+// The kernel's dynamic shared memory, named at namespace scope so that the
+// wavefronts index it directly (shared-memory loads, not generic ones).
+extern __shared__ __align__(16) float amaze_smem[];
+
+// Row wavefront of the weight smoothing (demosaic.rs:949-958 for hvwt,
+// :1109-1118 for pmwt), run by ONE warp.  At R/B site (r, c) of rows
+// [lo, rr1-lo) x cols [lo, cc1-lo):
+//     alt = (w(r-1,c-1) + w(r-1,c+1) + w(r+1,c-1) + w(r+1,c+1)) / 4
+//     if |0.5 - w(r,c)| < |0.5 - alt|: w(r,c) = alt
+// where row r-1 holds already-updated values.  Lane L owns sites k = L and
+// L+32 of every row and keeps the updated row in registers; the neighbours
+// (r-1, c-+1) are sites k-1/k/k+1 of the previous row, fetched by shuffle.
+// Sites outside the updated range keep their stored values.  Division by 4
+// is exact, so * 0.25f gives the same bits.  post(r, c, w_new) runs after
+// each update.  The array is amaze_smem[woff ...].
+template <class P, class Post>
+__device__ void wavefront(const P& p, const Geo& g, int woff, int lo, Post post) {
+    float* const w = amaze_smem + woff;
+    const int lane = threadIdx.x & 31;
+    const int rhi = g.rr1 - lo, chi = g.cc1 - lo;
+    // Bayer rows alternate the column parity of their R/B sites
+    int par = p.cfa.at(g.top + lo, g.left + 2) & 1;
+    const int n0 = (chi - lo + 1) >> 1, n1 = (chi - lo) >> 1;
+    // row being updated: own value, stored upper neighbours (used where the
+    // previous row was not updated) and the lower neighbours (not updated yet)
+    float own[2], upl[2], upr[2], lwl[2], lwr[2];
+    auto load = [&](int rr, int pr, float* o, float* ul, float* ur, float* dl, float* dr) {
+        const int c0 = lo + pr, n = pr ? n1 : n0;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int i = rr * TS + c0 + 2 * min(lane + 32 * j, n - 1);
+            o[j] = w[i >> 1];
+            ul[j] = w[(i - M1) >> 1];
+            ur[j] = w[(i - P1) >> 1];
+            dl[j] = w[(i + P1) >> 1];
+            dr[j] = w[(i + M1) >> 1];
+        }
+    };
+    load(lo, par, own, upl, upr, lwl, lwr);
+    float prevA = 0.f, prevB = 0.f;  // updated previous row, sites lane / lane+32
+    int nprev = 0;
+    for (int rr = lo; rr < rhi; rr++) {
+        const int n = par ? n1 : n0, c0 = lo + par;
+        float nown[2], nul[2], nur[2], ndl[2], ndr[2];
+        if (rr + 1 < rhi) load(rr + 1, par ^ 1, nown, nul, nur, ndl, ndr);
+        const float aM = __shfl_up_sync(0xffffffffu, prevA, 1), aP = __shfl_down_sync(0xffffffffu, prevA, 1);
+        const float bM = __shfl_up_sync(0xffffffffu, prevB, 1), bP = __shfl_down_sync(0xffffffffu, prevB, 1);
+        const float a31 = __shfl_sync(0xffffffffu, prevA, 31), b0 = __shfl_sync(0xffffffffu, prevB, 0);
+        float nv[2];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int k = lane + 32 * j;
+            const float vm1 = j == 0 ? aM : (lane == 0 ? a31 : bM);  // previous-row site k-1
+            const float v0 = j == 0 ? prevA : prevB;                 // site k
+            const float vp1 = j == 0 ? (lane == 31 ? b0 : aP) : bP;  // site k+1
+            const int kl = par == 0 ? k - 1 : k, kr = par == 0 ? k : k + 1;
+            const float ul = (kl >= 0 && kl < nprev) ? (par == 0 ? vm1 : v0) : upl[j];
+            const float ur = (kr >= 0 && kr < nprev) ? (par == 0 ? v0 : vp1) : upr[j];
+            const float alt = (ul + ur + lwl[j] + lwr[j]) * 0.25f;
+            const float v = fabsf(0.5f - own[j]) < fabsf(0.5f - alt) ? alt : own[j];
+            nv[j] = v;
+            if (k < n) {
+                w[(rr * TS + c0 + 2 * k) >> 1] = v;
+                post(rr, c0 + 2 * k, rr * TS + c0 + 2 * k, v);
+            }
+        }
+        prevA = nv[0];
+        prevB = nv[1];
+        nprev = n;
+        par ^= 1;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            own[j] = nown[j];
+            upl[j] = nul[j];
+            upr[j] = nur[j];
+            lwl[j] = ndl[j];
+            lwr[j] = ndr[j];
+        }
+    }
+    __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
@@ -526,22 +628,16 @@ __device__ void st_nyquist_area(const P& p, const Geo& g, const Bufs& b, const N
     });
 }
 
-// demosaic.rs:949-976: weight smoothing row by row (reads the row above
-// already updated), then green at R/B sites.
+// demosaic.rs:949-958: hvwt smoothing (one warp).
 template <class P>
-__device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
-    for (int rr = 8; rr < g.rr1 - 8; rr++) {
-        int c0 = 8 + (p.cfa.at(g.top + rr, g.left + 2) & 1);
-        int n = (g.cc1 - 8 - c0 + 1) / 2;
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            int i = rr * TS + c0 + 2 * k;
-            float* w = b.hvwt;
-            float alt = (w[(i - M1) >> 1] + w[(i - P1) >> 1] + w[(i + P1) >> 1] + w[(i + M1) >> 1]) / 4.0f;
-            if (fabsf(0.5f - w[i >> 1]) < fabsf(0.5f - alt)) w[i >> 1] = alt;
-        }
-        __syncthreads();
-    }
-    for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
+__device__ void wave_hvwt(const P& p, const Geo& g, const Bufs& b) {
+    wavefront(p, g, 3 * NF, 8, [](int, int, int, float) {});
+}
+
+// demosaic.rs:959-976: green at R/B sites from the smoothed weights.
+template <class P>
+__device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b, Team tm) {
+    for_rb_team(p, g, tm, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
         int i = rr * TS + cc;
         float wt = b.hvwt[i >> 1];
         float d0 = wt * b.vcd[i] + (1.0f - wt) * b.hcd[i];
@@ -561,10 +657,10 @@ __device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
 
 // demosaic.rs:978-998
 template <class P>
-__device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const NyqBox& box) {
+__device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const NyqBox& box, Team tm) {
     const float epssq = 1e-10f;
     const float q0 = 0.169917f, q1 = 0.108947f, q2 = 0.069855f, q3 = 0.0287182f;
-    for_rb(p, g, box.r0, box.r1, box.c0, box.c1, [&](int rr, int cc) {
+    for_rb_team(p, g, tm, box.r0, box.r1, box.c0, box.c1, [&](int rr, int cc) {
         int i = rr * TS + cc;
         if (!b.nyq2[i >> 1]) return;
         // dgrb2_h/v are zero wherever the vote map is zero (the reference
@@ -585,38 +681,58 @@ __device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const 
     });
 }
 
-// demosaic.rs:1000-1019
+// demosaic.rs:1000-1019, the dgrbsq1m/p half: squared diagonal differences
+// at the green site of each column pair.  (The delm/delp half is a single
+// absolute difference at the R/B site of the pair; st_diag_rb recomputes it.)
 template <class P>
-__device__ void st_diag_setup(const P& p, const Geo& g, const Bufs& b) {
-    int w = (g.cc1 - 6 - 6 + 1) / 2, n = (g.rr1 - 12) * w;
-    if (w <= 0 || g.rr1 - 12 <= 0) return;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        int rr = 6 + k / w, cc = 6 + 2 * (k % w);
+__device__ void st_diag_setup(const P& p, const Geo& g, const Bufs& b, Team tm) {
+    const int n = (g.rr1 - 12) * TSH;
+    for (int k = tm.t; k < n; k += tm.n) {
+        int rr = 6 + (k >> 6), cc = 6 + 2 * (k & (TSH - 1));
+        if (cc >= g.cc1 - 6) continue;
         int i = rr * TS + cc, h = i >> 1;
         const float* m = b.mos;
         bool rb_even = (p.cfa.at(g.top + rr, g.left + 2) & 1) == 0;
         if (rb_even) {
-            b.delp[h] = fabsf(m[i - P1] - m[i + P1]);
-            b.delm[h] = fabsf(m[i + M1] - m[i - M1]);
             b.q1p[h] = sqr(m[i + 1] - m[i + 1 - P1]) + sqr(m[i + 1] - m[i + 1 + P1]);
             b.q1m[h] = sqr(m[i + 1] - m[i + 1 + M1]) + sqr(m[i + 1] - m[i + 1 - M1]);
         } else {
             b.q1p[h] = sqr(m[i] - m[i - P1]) + sqr(m[i] - m[i + P1]);
             b.q1m[h] = sqr(m[i] - m[i - M1]) + sqr(m[i] - m[i + M1]);
-            b.delp[h] = fabsf(m[i + 1 - P1] - m[i + 1 + P1]);
-            b.delm[h] = fabsf(m[i + 1 - M1] - m[i + 1 + M1]);
         }
     }
 }
 
-// demosaic.rs:1021-1107
+// demosaic.rs:1021-1107, the diagonal weight pmwt (from dgrbsq1m/p).
 template <class P>
-__device__ void st_diag_interp(const P& p, const Geo& g, const Bufs& b) {
-    const float eps = 1e-5f, epssq = 1e-10f, arth = 0.75f;
+__device__ void st_diag_weight(const P& p, const Geo& g, const Bufs& b, Team tm) {
+    const float epssq = 1e-10f;
     const float ge0 = 0.13719494435797422f, ge1 = 0.05640252782101291f;
-    for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
+    for_rb_team(p, g, tm, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
         int i = rr * TS + cc, h = i >> 1;
-        const float *m = b.mos, *dm = b.delm, *dp = b.delp, *qm = b.q1m, *qp = b.q1p;
+        const float *qm = b.q1m, *qp = b.q1p;
+        float varm = epssq + ge0 * (qm[(i - V1) >> 1] + qm[(i - 1) >> 1] + qm[(i + 1) >> 1] + qm[(i + V1) >> 1]) +
+                     ge1 * (qm[(i - V2 - 1) >> 1] + qm[(i - V2 + 1) >> 1] + qm[(i - 2 - V1) >> 1] + qm[(i + 2 - V1) >> 1] +
+                            qm[(i - 2 + V1) >> 1] + qm[(i + 2 + V1) >> 1] + qm[(i + V2 - 1) >> 1] + qm[(i + V2 + 1) >> 1]);
+        float varp = epssq + ge0 * (qp[(i - V1) >> 1] + qp[(i - 1) >> 1] + qp[(i + 1) >> 1] + qp[(i + V1) >> 1]) +
+                     ge1 * (qp[(i - V2 - 1) >> 1] + qp[(i - V2 + 1) >> 1] + qp[(i - 2 - V1) >> 1] + qp[(i + 2 - V1) >> 1] +
+                            qp[(i - 2 + V1) >> 1] + qp[(i + 2 + V1) >> 1] + qp[(i + V2 - 1) >> 1] + qp[(i + V2 + 1) >> 1]);
+        b.pmwt[h] = varm / (varp + varm);
+    });
+}
+
+// demosaic.rs:1021-1107, the diagonal R+B estimates rbm/rbp.  delm/delp of
+// the R/B site j are |m[j+M1] - m[j-M1]| and |m[j-P1] - m[j+P1]| (the
+// reference stores them per column pair; the sign inside fabs does not
+// change the value).
+template <class P>
+__device__ void st_diag_rb(const P& p, const Geo& g, const Bufs& b, Team tm) {
+    const float eps = 1e-5f, arth = 0.75f;
+    for_rb_team(p, g, tm, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
+        int i = rr * TS + cc, h = i >> 1;
+        const float* m = b.mos;
+        auto dm = [&](int j) { return fabsf(m[j + M1] - m[j - M1]); };
+        auto dp = [&](int j) { return fabsf(m[j - P1] - m[j + P1]); };
         float crse = (m[i + M1] * 2.0f) / (eps + m[i] + m[i + M2]);
         float crnw = (m[i - M1] * 2.0f) / (eps + m[i] + m[i - M2]);
         float crne = (m[i - P1] * 2.0f) / (eps + m[i] + m[i - P2]);
@@ -625,19 +741,13 @@ __device__ void st_diag_interp(const P& p, const Geo& g, const Bufs& b) {
         float rbnw = fabsf(1.0f - crnw) < arth ? m[i] * crnw : m[i - M1] + (m[i] - m[i - M2]) * 0.5f;
         float rbne = fabsf(1.0f - crne) < arth ? m[i] * crne : m[i - P1] + (m[i] - m[i - P2]) * 0.5f;
         float rbsw = fabsf(1.0f - crsw) < arth ? m[i] * crsw : m[i + P1] + (m[i] - m[i + P2]) * 0.5f;
-        float wtse = eps + dm[h] + dm[(i + M1) >> 1] + dm[(i + M2) >> 1];
-        float wtnw = eps + dm[h] + dm[(i - M1) >> 1] + dm[(i - M2) >> 1];
-        float wtne = eps + dp[h] + dp[(i - P1) >> 1] + dp[(i - P2) >> 1];
-        float wtsw = eps + dp[h] + dp[(i + P1) >> 1] + dp[(i + P2) >> 1];
+        const float dm0 = dm(i), dp0 = dp(i);
+        float wtse = eps + dm0 + dm(i + M1) + dm(i + M2);
+        float wtnw = eps + dm0 + dm(i - M1) + dm(i - M2);
+        float wtne = eps + dp0 + dp(i - P1) + dp(i - P2);
+        float wtsw = eps + dp0 + dp(i + P1) + dp(i + P2);
         float rbm = (wtse * rbnw + wtnw * rbse) / (wtse + wtnw);
         float rbp = (wtne * rbsw + wtsw * rbne) / (wtne + wtsw);
-        float varm = epssq + ge0 * (qm[(i - V1) >> 1] + qm[(i - 1) >> 1] + qm[(i + 1) >> 1] + qm[(i + V1) >> 1]) +
-                     ge1 * (qm[(i - V2 - 1) >> 1] + qm[(i - V2 + 1) >> 1] + qm[(i - 2 - V1) >> 1] + qm[(i + 2 - V1) >> 1] +
-                            qm[(i - 2 + V1) >> 1] + qm[(i + 2 + V1) >> 1] + qm[(i + V2 - 1) >> 1] + qm[(i + V2 + 1) >> 1]);
-        float varp = epssq + ge0 * (qp[(i - V1) >> 1] + qp[(i - 1) >> 1] + qp[(i + 1) >> 1] + qp[(i + V1) >> 1]) +
-                     ge1 * (qp[(i - V2 - 1) >> 1] + qp[(i - V2 + 1) >> 1] + qp[(i - 2 - V1) >> 1] + qp[(i + 2 - V1) >> 1] +
-                            qp[(i - 2 + V1) >> 1] + qp[(i + 2 + V1) >> 1] + qp[(i + V2 - 1) >> 1] + qp[(i + V2 + 1) >> 1]);
-        b.pmwt[h] = varm / (varp + varm);
         if (rbp < m[i]) {
             if (rbp * 2.0f < m[i]) {
                 rbp = ulim(rbp, m[i - P1], m[i + P1]);
@@ -661,21 +771,21 @@ __device__ void st_diag_interp(const P& p, const Geo& g, const Bufs& b) {
     });
 }
 
-// demosaic.rs:1109-1123: pmwt smoothing row by row, then rbint.
+// demosaic.rs:1109-1118: pmwt smoothing (one warp); pmwt lives at the vcd
+// region of shared memory (amaze_smem + 2 NF) while it runs.
 template <class P>
-__device__ void st_rb_interp(const P& p, const Geo& g, const Bufs& b) {
-    for (int rr = 10; rr < g.rr1 - 10; rr++) {
-        int c0 = 10 + (p.cfa.at(g.top + rr, g.left + 2) & 1);
-        int n = (g.cc1 - 10 - c0 + 1) / 2;
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            int i = rr * TS + c0 + 2 * k, h = i >> 1;
-            float* pm = b.pmwt;
-            float alt = (pm[(i - M1) >> 1] + pm[(i - P1) >> 1] + pm[(i + P1) >> 1] + pm[(i + M1) >> 1]) / 4.0f;
-            if (fabsf(0.5f - pm[h]) < fabsf(0.5f - alt)) pm[h] = alt;
-            b.rbint[h] = (b.mos[i] + b.rbm[h] * (1.0f - pm[h]) + b.rbp[h] * pm[h]) * 0.5f;
-        }
-        __syncthreads();
-    }
+__device__ void wave_pmwt(const P& p, const Geo& g) {
+    wavefront(p, g, 2 * NF, 10, [](int, int, int, float) {});
+}
+
+// demosaic.rs:1119-1122: rbint from the final diagonal weight.
+template <class P>
+__device__ void st_rbint(const P& p, const Geo& g, const Bufs& b) {
+    for_rb(p, g, 10, g.rr1 - 10, 10, g.cc1 - 10, [&](int rr, int cc) {
+        const int i = rr * TS + cc, h = i >> 1;
+        const float pm = b.pmwt[h];
+        b.rbint[h] = (b.mos[i] + b.rbm[h] * (1.0f - pm) + b.rbp[h] * pm) * 0.5f;
+    });
 }
 
 // demosaic.rs:1125-1194
@@ -821,8 +931,8 @@ struct EpiColor {
 };
 
 template <class Src, class Epi>
-__global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(Params<Src> p, Epi epi) {
-    extern __shared__ __align__(16) float smem[];
+__global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constant__ Params<Src> p, const __grid_constant__ Epi epi) {
+    float* smem = amaze_smem;
     __shared__ int box_sh[4];
     Bufs b;
     b.mos = smem;
@@ -879,22 +989,37 @@ __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(Params<Src> p, Epi e
             st_nyquist_area(p, g, b, box);
             __syncthreads();
         }
-        st_green_rb(p, g, b);
+        // hvwt smoothing: one warp walks the rows (the others wait)
+        if ((threadIdx.x >> 5) == 0) wave_hvwt(p, g, b);
         __syncthreads();
-        if (box.on) {
-            st_nyquist_green(p, g, b, box);
-        }
-        st_diag_setup(p, g, b);
+        st_green_rb(p, g, b, whole_block());
         __syncthreads();
-        st_diag_interp(p, g, b);
+        if (box.on) st_nyquist_green(p, g, b, box, whole_block());
         __syncthreads();
-        st_rb_interp(p, g, b);
+        // hcd / vcd are dead from here: the diagonal stage keeps its arrays
+        // in their shared memory
+        Bufs d = b;
+        d.q1m = b.hcd;
+        d.q1p = b.hcd + NH;
+        d.pmwt = b.vcd;
+        d.rbint = b.vcd + NH;
+        st_diag_setup(p, g, d, whole_block());
         __syncthreads();
-        st_green_refine(p, g, b);
+        st_diag_weight(p, g, d, whole_block());
         __syncthreads();
-        st_chroma(p, g, b);
+        d.rbm = b.hcd;  // over dgrbsq1m/p, no longer read
+        d.rbp = b.hcd + NH;
+        st_diag_rb(p, g, d, whole_block());
         __syncthreads();
-        st_output(p, g, b, epi);
+        if ((threadIdx.x >> 5) == 0) wave_pmwt(p, g);
+        __syncthreads();
+        st_rbint(p, g, d);
+        __syncthreads();
+        st_green_refine(p, g, d);
+        __syncthreads();
+        st_chroma(p, g, d);
+        __syncthreads();
+        st_output(p, g, d, epi);
         __syncthreads();
     }
 }
