@@ -36,18 +36,30 @@ constexpr int V1 = 128, V2 = 256, V3 = 384, P1 = 127, P2 = 254, P3 = 381, M1 = 1
 constexpr int NTHREADS = 512;
 static_assert(NTHREADS % TS == 0 && NTHREADS % TSH == 0, "row mapping of the stage loops");
 
-// global scratch per CTA slot: 8 full arrays, 14 half arrays, 2 byte maps
-constexpr size_t SLOT_FLOATS = 8 * (size_t)NF + 14 * (size_t)NH;
-constexpr size_t SLOT_BYTES = SLOT_FLOATS * 4 + 2 * (size_t)NH;
+// global scratch per CTA slot: 5 half arrays
+constexpr size_t SLOT_FLOATS = 5 * (size_t)NH;
+constexpr size_t SLOT_BYTES = SLOT_FLOATS * 4;
 constexpr size_t SMEM_BYTES = (3 * (size_t)NF + (size_t)NH) * 4 + 64;
 
 struct Bufs {
-    float *mos, *hcd, *vcd, *hvwt;                                  // shared
-    float *wv, *wh, *gsq, *vcda, *hcda, *cdd, *dgv, *dgh;           // global, full
-    float *dgrb0, *dgrb1, *delp, *delm, *rbint, *q1m, *q1p, *pmwt;  // global, half
-    float *rbm, *rbp, *nyqt, *rg, *d2h, *d2v;
-    uint8_t *nyq, *nyq2;
+    // shared memory: the mosaic; hcd / vcd regions (candidates and refined
+    // colour differences, later the diagonal stage's arrays); hvwt
+    float *mos, *hcd, *vcd, *hvwt;
+    // per-CTA global scratch (half arrays, flat index >> 1)
+    float *dgrb0, *dgrb1, *rg, *d2h, *d2v;
+    // shared-memory half arrays of the diagonal stage (set per tile)
+    float *q1m, *q1p, *pmwt, *rbm, *rbp, *rbint;
+    unsigned long long *nyqw, *nyq2w;  // shared: per-row bit masks of the R/B sites
 };
+
+// Nyquist flags are kept as one 64-bit mask per tile row, bit k for the R/B
+// site of column pair k (a Bayer row has one R/B site per pair).
+__device__ __forceinline__ bool rbflag(const unsigned long long* w, int i) {
+    return (w[i >> 7] >> ((i & (TS - 1)) >> 1)) & 1ull;
+}
+__device__ __forceinline__ void rbflag_set(unsigned long long* w, int i) {
+    atomicOr(&w[i >> 7], 1ull << ((i & (TS - 1)) >> 1));
+}
 
 struct Geo {
     int top, left, rr1, cc1, rrmin, ccmin, rrmax, ccmax;
@@ -332,86 +344,6 @@ __device__ void wavefront(const P& p, const Geo& g, int woff, int lo, Post post)
 // ---------------------------------------------------------------------------
 // stages
 
-// demosaic.rs:612-622
-__device__ void st_gradients(const Geo& g, const Bufs& b) {
-    const float eps = 1e-5f;
-    for_rect(2, g.rr1 - 2, 2, g.cc1 - 2, [&](int rr, int cc) {
-        int i = rr * TS + cc;
-        const float* m = b.mos;
-        float dh = fabsf(m[i + 1] - m[i - 1]);
-        float dv = fabsf(m[i + V1] - m[i - V1]);
-        b.wv[i] = eps + fabsf(m[i + V2] - m[i]) + fabsf(m[i] - m[i - V2]) + dv;
-        b.wh[i] = eps + fabsf(m[i + 2] - m[i]) + fabsf(m[i] - m[i - 2]) + dh;
-        b.gsq[i] = sqr(dh) + sqr(dv);
-    });
-}
-
-// demosaic.rs:624-698.  Also writes the zeros the reference's freshly
-// allocated arrays hold just outside the computed band (read by the
-// refinement at rows/cols 2,3 and rr1-4, rr1-3).
-template <class P>
-__device__ void st_colour_diff(const P& p, const Geo& g, const Bufs& b) {
-    const float eps = 1e-5f, arth = 0.75f;
-    const float clip8 = p.clip * 0.8f;
-    for_rect(2, g.rr1 - 2, 2, g.cc1 - 2, [&](int rr, int cc) {
-        int i = rr * TS + cc;
-        bool in_r = rr >= 4 && rr < g.rr1 - 4, in_c = cc >= 4 && cc < g.cc1 - 4;
-        if (!(in_r && in_c)) {
-            if (in_c) { b.vcd[i] = 0.f; b.vcda[i] = 0.f; }
-            if (in_r) { b.hcd[i] = 0.f; b.hcda[i] = 0.f; }
-            return;
-        }
-        const float *m = b.mos, *wv = b.wv, *wh = b.wh;
-        float cru = m[i - V1] * (wv[i - V2] + wv[i]) /
-                    fmaxf(wv[i - V2] * (eps + m[i]) + wv[i] * (eps + m[i - V2]), 1e-10f);
-        float crd = m[i + V1] * (wv[i + V2] + wv[i]) /
-                    fmaxf(wv[i + V2] * (eps + m[i]) + wv[i] * (eps + m[i + V2]), 1e-10f);
-        float crl = m[i - 1] * (wh[i - 2] + wh[i]) /
-                    fmaxf(wh[i - 2] * (eps + m[i]) + wh[i] * (eps + m[i - 2]), 1e-10f);
-        float crr = m[i + 1] * (wh[i + 2] + wh[i]) /
-                    fmaxf(wh[i + 2] * (eps + m[i]) + wh[i] * (eps + m[i + 2]), 1e-10f);
-        float guha = m[i - V1] + (m[i] - m[i - V2]) * 0.5f;
-        float gdha = m[i + V1] + (m[i] - m[i + V2]) * 0.5f;
-        float glha = m[i - 1] + (m[i] - m[i - 2]) * 0.5f;
-        float grha = m[i + 1] + (m[i] - m[i + 2]) * 0.5f;
-        float guar = fabsf(1.0f - cru) < arth ? m[i] * cru : guha;
-        float gdar = fabsf(1.0f - crd) < arth ? m[i] * crd : gdha;
-        float glar = fabsf(1.0f - crl) < arth ? m[i] * crl : glha;
-        float grar = fabsf(1.0f - crr) < arth ? m[i] * crr : grha;
-        float hwt = wh[i - 1] / fmaxf(wh[i - 1] + wh[i + 1], 1e-10f);
-        float vwt = wv[i - V1] / fmaxf(wv[i + V1] + wv[i - V1], 1e-10f);
-        float gintvha = vwt * gdha + (1.0f - vwt) * guha;
-        float ginthha = hwt * grha + (1.0f - hwt) * glha;
-        // the reference toggles a G/non-G switch per column; for a Bayer
-        // row that equals the site's own colour test
-        bool gsite = (p.cfa.at(g.top + rr, g.left + cc) & 1) != 0;
-        float vcdv, hcdv, vcdalt, hcdalt;
-        if (gsite) {
-            vcdv = m[i] - (vwt * gdar + (1.0f - vwt) * guar);
-            hcdv = m[i] - (hwt * grar + (1.0f - hwt) * glar);
-            vcdalt = m[i] - gintvha;
-            hcdalt = m[i] - ginthha;
-        } else {
-            vcdv = (vwt * gdar + (1.0f - vwt) * guar) - m[i];
-            hcdv = (hwt * grar + (1.0f - hwt) * glar) - m[i];
-            vcdalt = gintvha - m[i];
-            hcdalt = ginthha - m[i];
-        }
-        float gu = guar, gd = gdar, gl = glar, gr = grar;
-        if (m[i] > clip8 || gintvha > clip8 || ginthha > clip8) {
-            vcdv = vcdalt;
-            hcdv = hcdalt;
-            gu = guha; gd = gdha; gl = glha; gr = grha;
-        }
-        b.vcd[i] = vcdv;
-        b.hcd[i] = hcdv;
-        b.vcda[i] = vcdalt;
-        b.hcda[i] = hcdalt;
-        b.dgv[i] = fminf(sqr(guha - gdha), sqr(gu - gd));
-        b.dgh[i] = fminf(sqr(glha - grha), sqr(gl - gr));
-    });
-}
-
 // Bound a colour difference by the two neighbours along its direction
 // (the clamp half of demosaic.rs:724-784).  nb0/nb1: neighbours.
 __device__ __forceinline__ float cd_bound(float cd, float m, float nb0, float nb1, bool gsite, float clip) {
@@ -442,96 +374,331 @@ __device__ __forceinline__ float cd_bound(float cd, float m, float nb0, float nb
     return cd;
 }
 
-// demosaic.rs:700-786.  hcd at a site depends on the already-refined hcd two
-// columns left, vcd on the refined vcd two rows up; the two are independent,
-// so each (row, parity) hcd chain and each (column, parity) vcd chain is one
-// thread walking in the reference's order.
+// ---------------------------------------------------------------------------
+// Per-site arithmetic of demosaic.rs:612-698 by direction.  n[0..4]: mosaic
+// at -2..+2 along the direction, w[0..4]: that direction's gradient weight
+// (dirwts) at -2..+2.
+
+// dirwts at a site from the mosaic at -2..+2 along the direction
+// (demosaic.rs:612-622): eps + |m+2 - m0| + |m0 - m-2| + |m+1 - m-1|.
+__device__ __forceinline__ float grad_w(float a, float b, float c, float d, float e) {
+    return 1e-5f + fabsf(e - c) + fabsf(c - a) + fabsf(d - b);
+}
+
+// The direction's blend weight (vwt / hwt) and Hamilton-Adams estimate
+// (gintvha / ginthha).
+__device__ __forceinline__ float dir_hha(const float* n, const float* w, float& wt) {
+    wt = w[1] / fmaxf(w[3] + w[1], 1e-10f);
+    const float lo = n[1] + (n[2] - n[0]) * 0.5f, hi = n[3] + (n[2] - n[4]) * 0.5f;
+    return wt * hi + (1.0f - wt) * lo;
+}
+
+// Colour difference along a direction (vcd / hcd), its alternative (vcdalt /
+// hcdalt), the min squared difference (dgintv / dginth) and the blend weight.
+// cross_hha: the other direction's Hamilton-Adams estimate (clip test).
+__device__ __forceinline__ void dir_cd(const float* n, const float* w, float cross_hha, bool gsite, float clip8,
+                                       float& val, float& alt, float& dg, float& wt) {
+    const float eps = 1e-5f, arth = 0.75f;
+    const float m0 = n[2];
+    const float cr_lo = n[1] * (w[0] + w[2]) / fmaxf(w[0] * (eps + m0) + w[2] * (eps + n[0]), 1e-10f);
+    const float cr_hi = n[3] * (w[4] + w[2]) / fmaxf(w[4] * (eps + m0) + w[2] * (eps + n[4]), 1e-10f);
+    const float ha_lo = n[1] + (m0 - n[0]) * 0.5f, ha_hi = n[3] + (m0 - n[4]) * 0.5f;
+    const float ar_lo = fabsf(1.0f - cr_lo) < arth ? m0 * cr_lo : ha_lo;
+    const float ar_hi = fabsf(1.0f - cr_hi) < arth ? m0 * cr_hi : ha_hi;
+    wt = w[1] / fmaxf(w[3] + w[1], 1e-10f);
+    const float hha = wt * ha_hi + (1.0f - wt) * ha_lo;
+    const float est = wt * ar_hi + (1.0f - wt) * ar_lo;
+    if (gsite) {
+        val = m0 - est;
+        alt = m0 - hha;
+    } else {
+        val = est - m0;
+        alt = hha - m0;
+    }
+    float glo = ar_lo, ghi = ar_hi;
+    if (m0 > clip8 || hha > clip8 || cross_hha > clip8) {
+        val = alt;
+        glo = ha_lo;
+        ghi = ha_hi;
+    }
+    dg = fminf(sqr(ha_lo - ha_hi), sqr(glo - ghi));
+}
+
+// The refinement chains of demosaic.rs:700-786 as scans.  At a chain
+// position the refined value is cd_bound() of either the alternative or the
+// raw colour difference; which one depends on the refined value two sites
+// back, itself one of that site's two candidates.  So each position is a map
+// on two states {0: alternative, 1: raw}, encoded f(0) | f(1) << 1, and the
+// chain is the composition of its maps: associative, hence a parallel scan.
+// The first position of a chain reads the zero before the band, which makes
+// its map constant.
+constexpr int MAP_ID = 2;
+__device__ __forceinline__ int map_at(int f, int x) { return (f >> x) & 1; }
+// g after f
+__device__ __forceinline__ int map_then(int f, int g) { return map_at(g, f & 1) | (map_at(g, (f >> 1) & 1) << 1); }
+
+// 3 * sum of squares - square of sum, in the reference's operation order
+__device__ __forceinline__ float var3(float a, float b, float c) {
+    return 3.0f * (sqr(a) + sqr(b) + sqr(c)) - sqr(a + b + c);
+}
+
+// Transition of one position: hav (variance of the alternatives at -2,0,+2),
+// the two candidates of the previous position and the raw values at 0, +2.
+__device__ __forceinline__ int chain_map(float hav, float prevA, float prevB, float raw0, float raw2) {
+    const int f0 = hav < var3(prevA, raw0, raw2) ? 0 : 1;
+    const int f1 = hav < var3(prevB, raw0, raw2) ? 0 : 1;
+    return f0 | (f1 << 1);
+}
+
+constexpr int VSEG = NTHREADS / TS;  // row segments of the column pass
+constexpr int VSEGLEN = 30;          // chain rows per segment
+static_assert(VSEG * VSEGLEN >= TS - 8, "column-pass segments must cover the band");
+
+// Column pass: demosaic.rs:612-698 (vertical half), the vcd chains of
+// :700-786 and the vertical half of :788-828.  Thread (column c, row segment
+// sg) walks rows t = r0-2 .. r1+1 of its column once, unrolled, with the
+// mosaic column, the vertical gradients and the colour differences held in
+// register windows.  At step t it forms the colour difference of row t and
+// the chain step of row u = t-2 (which needs rows u-2 .. u+2).  Outputs:
+//   b.vcd  <- alternative candidate of each chain row, then the refined vcd
+//   b.hcd  <- raw candidate of each chain row (read back before the barrier)
+//   b.hvwt <- vvar1 (the dgintv variance term) at the R/B sites
+// Rows 3 and rr1-4 of b.vcd are zeroed: the H/V weight reads them.
 template <class P>
-__device__ void st_cd_refine(const P& p, const Geo& g, const Bufs& b) {
-    const int nr = g.rr1 - 8, nc = g.cc1 - 8;
-    const int nh = nr > 0 ? 2 * nr : 0, nv = nc > 0 ? 2 * nc : 0;
+__device__ void st_vpass(const P& p, const Geo& g, const Bufs& b, uint8_t* segmap) {
+    const float epssq = 1e-10f;
+    const float clip8 = p.clip * 0.8f;
+    const int c = threadIdx.x & (TS - 1), sg = threadIdx.x / TS;
+    const int rhi = g.rr1 - 4;
+    const bool col_cd = c >= 4 && c < g.cc1 - 4;
+    const bool col_hv = c >= 6 && c < g.cc1 - 6;
+    const int r0 = 4 + VSEGLEN * sg, r1 = min(r0 + VSEGLEN, rhi);
+    const bool on = col_cd && r0 < r1;
     const float* m = b.mos;
-    for (int t = threadIdx.x; t < nh + nv; t += blockDim.x) {
-        if (t < nh) {
-            int rr = 4 + t / 2, cc0 = 4 + (t & 1);
-            bool gs = (p.cfa.at(g.top + rr, g.left + cc0) & 1) != 0;
-            float* hcd = b.hcd;
-            const float* ha = b.hcda;
-            for (int cc = cc0; cc < g.cc1 - 4; cc += 2) {
-                int i = rr * TS + cc;
-                float hv = 3.0f * (sqr(hcd[i - 2]) + sqr(hcd[i]) + sqr(hcd[i + 2])) -
-                           sqr(hcd[i - 2] + hcd[i] + hcd[i + 2]);
-                float hav = 3.0f * (sqr(ha[i - 2]) + sqr(ha[i]) + sqr(ha[i + 2])) -
-                            sqr(ha[i - 2] + ha[i] + ha[i + 2]);
-                float v = hav < hv ? ha[i] : hcd[i];
-                hcd[i] = cd_bound(v, m[i], m[i - 1], m[i + 1], gs, p.clip);
+    constexpr int NK = VSEGLEN + 4;   // steps t = r0-2+k
+    constexpr int NM = NK + 8;        // mosaic rows r0-6+j
+    unsigned run0 = 0, run1 = 0;
+    int x00 = 0, x01 = 1, x10 = 0, x11 = 1;
+    if (on) {
+        auto mrow = [&](int x, int dc) { return (x >= 0 && x < g.rr1) ? m[x * TS + c + dc] : 0.0f; };
+        float mc[NM];
+#pragma unroll
+        for (int j = 0; j < NM; j++) mc[j] = mrow(r0 - 6 + j, 0);
+        float wv[NM - 4];  // wv of row r0-4+j
+#pragma unroll
+        for (int j = 0; j < NM - 4; j++) wv[j] = grad_w(mc[j], mc[j + 1], mc[j + 2], mc[j + 3], mc[j + 4]);
+        float raw[NK], alt[NK], dg[NK], vw[NK], A[NK], B[NK];
+#pragma unroll
+        for (int k = 0; k < NK; k++) {
+            const int t = r0 - 2 + k;
+            raw[k] = alt[k] = dg[k] = vw[k] = A[k] = B[k] = 0.0f;
+            if (t >= 4 && t < rhi) {
+                const bool gs = (p.cfa.at(g.top + t, g.left + c) & 1) != 0;
+                const float* rowp = m + t * TS + c;
+                const float h[7] = {rowp[-3], rowp[-2], rowp[-1], mc[k + 4], rowp[1], rowp[2], rowp[3]};
+                const float whm = grad_w(h[0], h[1], h[2], h[3], h[4]), whp = grad_w(h[2], h[3], h[4], h[5], h[6]);
+                const float nh[5] = {h[1], h[2], h[3], h[4], h[5]};
+                const float wh5[5] = {0.0f, whm, 0.0f, whp, 0.0f};
+                float hwt;
+                const float hha = dir_hha(nh, wh5, hwt);
+                const float nv[5] = {mc[k + 2], mc[k + 3], mc[k + 4], mc[k + 5], mc[k + 6]};
+                const float wv5[5] = {wv[k], wv[k + 1], wv[k + 2], wv[k + 3], wv[k + 4]};
+                dir_cd(nv, wv5, hha, gs, clip8, raw[k], alt[k], dg[k], vw[k]);
+                A[k] = cd_bound(alt[k], mc[k + 4], mc[k + 3], mc[k + 5], gs, p.clip);
+                B[k] = cd_bound(raw[k], mc[k + 4], mc[k + 3], mc[k + 5], gs, p.clip);
             }
-        } else {
-            int tt = t - nh;
-            int cc = 4 + tt / 2, rr0 = 4 + (tt & 1);
-            bool gs = (p.cfa.at(g.top + rr0, g.left + cc) & 1) != 0;
-            float* vcd = b.vcd;
-            const float* va = b.vcda;
-            for (int rr = rr0; rr < g.rr1 - 4; rr += 2) {
-                int i = rr * TS + cc;
-                float vv = 3.0f * (sqr(vcd[i - V2]) + sqr(vcd[i]) + sqr(vcd[i + V2])) -
-                           sqr(vcd[i - V2] + vcd[i] + vcd[i + V2]);
-                float vav = 3.0f * (sqr(va[i - V2]) + sqr(va[i]) + sqr(va[i + V2])) -
-                            sqr(va[i - V2] + va[i] + va[i + V2]);
-                float v = vav < vv ? va[i] : vcd[i];
-                vcd[i] = cd_bound(v, m[i], m[i - V1], m[i + V1], gs, p.clip);
+            const int u = t - 2;  // chain row of this step
+            if (k >= 4 && u < r1) {
+                const int ku = k - 4;
+                const int f = chain_map(var3(alt[k - 4], alt[k - 2], alt[k]), A[k - 4], B[k - 4], raw[k - 2], raw[k]);
+                if (u & 1) {
+                    x10 = map_at(f, x10);
+                    x11 = map_at(f, x11);
+                    run0 |= (unsigned)x10 << ku;
+                    run1 |= (unsigned)x11 << ku;
+                } else {
+                    x00 = map_at(f, x00);
+                    x01 = map_at(f, x01);
+                    run0 |= (unsigned)x00 << ku;
+                    run1 |= (unsigned)x01 << ku;
+                }
+                const int i = u * TS + c;
+                b.vcd[i] = A[k - 2];
+                b.hcd[i] = B[k - 2];
+                if (col_hv && u >= 6 && u < g.rr1 - 6 && (p.cfa.at(g.top + u, g.left + c) & 1) == 0) {
+                    const float vu1 = dg[k - 2] + dg[k - 3] + dg[k - 4];
+                    const float vd1 = dg[k - 2] + dg[k - 1] + dg[k];
+                    b.hvwt[i >> 1] = epssq + vw[k - 2] * vd1 + (1.0f - vw[k - 2]) * vu1;
+                }
             }
         }
     }
+    segmap[(sg * TS + c) * 2] = (uint8_t)(x00 | (x01 << 1));
+    segmap[(sg * TS + c) * 2 + 1] = (uint8_t)(x10 | (x11 << 1));
     __syncthreads();
-    for_rb(p, g, 4, g.rr1 - 4, 4, g.cc1 - 4, [&](int rr, int cc) {
-        int i = rr * TS + cc;
-        b.cdd[i] = sqr(b.vcd[i] - b.hcd[i]);
-    });
+    if (!col_cd) return;
+    if (sg == 0) b.vcd[3 * TS + c] = 0.0f;
+    if (r0 <= rhi && rhi <= r0 + VSEGLEN) b.vcd[rhi * TS + c] = 0.0f;
+    if (!on) return;
+    int E0 = MAP_ID, E1 = MAP_ID;
+    for (int k = 0; k < sg; k++) {
+        E0 = map_then(E0, segmap[(k * TS + c) * 2]);
+        E1 = map_then(E1, segmap[(k * TS + c) * 2 + 1]);
+    }
+    const int e0 = map_at(E0, 0), e1 = map_at(E1, 0);
+#pragma unroll
+    for (int k = 0; k < VSEGLEN; k++) {
+        const int u = r0 + k;
+        if (u < r1) {
+            const int i = u * TS + c;
+            const int st = ((((u & 1) ? e1 : e0) ? run1 : run0) >> k) & 1;
+            if (st) b.vcd[i] = b.hcd[i];
+        }
+    }
 }
 
-// demosaic.rs:788-828
+// Row pass: demosaic.rs:612-698 (horizontal half), the hcd chains of
+// :700-786, the H/V weight of :788-828 and cddiffsq (:785).  One warp per
+// row r of [4, rr1-4); lane L owns columns c0 = 4+4L .. c0+3 and gets the
+// neighbouring columns from lanes L-1 / L+1.  Reads the refined vcd and
+// vvar1 the column pass left; writes hvwt over vvar1, and at the R/B sites
+// cdd to b.hcd[0 .. NH) and the refined hcd to b.hcd[NH .. 2 NH) (half
+// arrays indexed by flat index >> 1).
 template <class P>
-__device__ void st_hv_weight(const P& p, const Geo& g, const Bufs& b) {
+__device__ void st_hpass(const P& p, const Geo& g, const Bufs& b) {
     const float epssq = 1e-10f;
-    for_rb(p, g, 6, g.rr1 - 6, 6, g.cc1 - 6, [&](int rr, int cc) {
-        int i = rr * TS + cc;
-        const float *vcd = b.vcd, *hcd = b.hcd, *dv = b.dgv, *dh = b.dgh;
-        float uave = vcd[i] + vcd[i - V1] + vcd[i - V2] + vcd[i - V3];
-        float dave = vcd[i] + vcd[i + V1] + vcd[i + V2] + vcd[i + V3];
-        float lave = hcd[i] + hcd[i - 1] + hcd[i - 2] + hcd[i - 3];
-        float rave = hcd[i] + hcd[i + 1] + hcd[i + 2] + hcd[i + 3];
-        float vu = sqr(vcd[i] - uave) + sqr(vcd[i - V1] - uave) + sqr(vcd[i - V2] - uave) + sqr(vcd[i - V3] - uave);
-        float vd = sqr(vcd[i] - dave) + sqr(vcd[i + V1] - dave) + sqr(vcd[i + V2] - dave) + sqr(vcd[i + V3] - dave);
-        float hl = sqr(hcd[i] - lave) + sqr(hcd[i - 1] - lave) + sqr(hcd[i - 2] - lave) + sqr(hcd[i - 3] - lave);
-        float hr = sqr(hcd[i] - rave) + sqr(hcd[i + 1] - rave) + sqr(hcd[i + 2] - rave) + sqr(hcd[i + 3] - rave);
-        float hwt = b.wh[i - 1] / fmaxf(b.wh[i - 1] + b.wh[i + 1], 1e-10f);
-        float vwt = b.wv[i - V1] / fmaxf(b.wv[i + V1] + b.wv[i - V1], 1e-10f);
-        float vvar = epssq + vwt * vd + (1.0f - vwt) * vu;
-        float hvar = epssq + hwt * hr + (1.0f - hwt) * hl;
-        float vu1 = dv[i] + dv[i - V1] + dv[i - V2];
-        float vd1 = dv[i] + dv[i + V1] + dv[i + V2];
-        float hl1 = dh[i] + dh[i - 1] + dh[i - 2];
-        float hr1 = dh[i] + dh[i + 1] + dh[i + 2];
-        float vvar1 = epssq + vwt * vd1 + (1.0f - vwt) * vu1;
-        float hvar1 = epssq + hwt * hr1 + (1.0f - hwt) * hl1;
-        float varwt = hvar / fmaxf(vvar + hvar, 1e-10f);
-        float diffwt = hvar1 / fmaxf(vvar1 + hvar1, 1e-10f);
-        if ((0.5f - varwt) * (0.5f - diffwt) > 0.0f && fabsf(0.5f - diffwt) < fabsf(0.5f - varwt))
-            b.hvwt[i >> 1] = varwt;
-        else
-            b.hvwt[i >> 1] = diffwt;
-    });
+    const float clip8 = p.clip * 0.8f;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int cend = g.cc1 - 4;
+    const int c0 = 4 + 4 * lane;
+    float* cdd = b.hcd;
+    float* hcd_rb = b.hcd + NH;
+    for (int rr = 4 + (int)(threadIdx.x >> 5); rr < g.rr1 - 4; rr += NTHREADS / 32) {
+        // mosaic: row rr at columns c0-4 .. c0+7, rows rr-3 .. rr+3 at c0 .. c0+3
+        float mr[12], mv[7][4];
+        {
+            const float4* q = reinterpret_cast<const float4*>(b.mos + rr * TS + c0 - 4);
+            const float4 x0 = q[0], x1 = q[1], x2 = q[2];
+            const float t[12] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w, x2.x, x2.y, x2.z, x2.w};
+#pragma unroll
+            for (int k = 0; k < 12; k++) mr[k] = t[k];
+#pragma unroll
+            for (int d = 0; d < 7; d++) {
+                const float4 y = *reinterpret_cast<const float4*>(b.mos + (rr - 3 + d) * TS + c0);
+                mv[d][0] = y.x; mv[d][1] = y.y; mv[d][2] = y.z; mv[d][3] = y.w;
+            }
+        }
+        float wh[8];  // wh at columns c0-2 .. c0+5
+#pragma unroll
+        for (int k = 0; k < 8; k++) wh[k] = grad_w(mr[k], mr[k + 1], mr[k + 2], mr[k + 3], mr[k + 4]);
+        float raw[4], alt[4], dg[4], hw[4], vw[4], A[4], B[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            raw[j] = alt[j] = dg[j] = hw[j] = vw[j] = A[j] = B[j] = 0.0f;
+            const int c = c0 + j;
+            // vertical Hamilton-Adams estimate and weight (clip test, H/V weight)
+            const float nv[5] = {mv[1][j], mv[2][j], mv[3][j], mv[4][j], mv[5][j]};
+            const float wv5[5] = {0.0f, grad_w(mv[0][j], mv[1][j], mv[2][j], mv[3][j], mv[4][j]), 0.0f,
+                                  grad_w(mv[2][j], mv[3][j], mv[4][j], mv[5][j], mv[6][j]), 0.0f};
+            const float vha = dir_hha(nv, wv5, vw[j]);
+            if (c < cend) {
+                const bool gs = (p.cfa.at(g.top + rr, g.left + c) & 1) != 0;
+                const float nh[5] = {mr[j + 2], mr[j + 3], mr[j + 4], mr[j + 5], mr[j + 6]};
+                const float wh5[5] = {wh[j], wh[j + 1], wh[j + 2], wh[j + 3], wh[j + 4]};
+                dir_cd(nh, wh5, vha, gs, clip8, raw[j], alt[j], dg[j], hw[j]);
+                A[j] = cd_bound(alt[j], mr[j + 4], mr[j + 3], mr[j + 5], gs, p.clip);
+                B[j] = cd_bound(raw[j], mr[j + 4], mr[j + 3], mr[j + 5], gs, p.clip);
+            }
+        }
+        // neighbours: columns c0-2, c0-1 from lane L-1 (zero before the band),
+        // c0+4, c0+5 from lane L+1 (zero past it)
+        float altL2 = __shfl_up_sync(FULL, alt[2], 1), altL3 = __shfl_up_sync(FULL, alt[3], 1);
+        float aL2 = __shfl_up_sync(FULL, A[2], 1), aL3 = __shfl_up_sync(FULL, A[3], 1);
+        float bL2 = __shfl_up_sync(FULL, B[2], 1), bL3 = __shfl_up_sync(FULL, B[3], 1);
+        if (lane == 0) altL2 = altL3 = aL2 = aL3 = bL2 = bL3 = 0.0f;
+        const float altR0 = __shfl_down_sync(FULL, alt[0], 1), altR1 = __shfl_down_sync(FULL, alt[1], 1);
+        const float rawR0 = __shfl_down_sync(FULL, raw[0], 1), rawR1 = __shfl_down_sync(FULL, raw[1], 1);
+        const float altx[8] = {altL2, altL3, alt[0], alt[1], alt[2], alt[3], altR0, altR1};  // c0-2 .. c0+5
+        const float rawx[6] = {raw[0], raw[1], raw[2], raw[3], rawR0, rawR1};                 // c0 .. c0+5
+        const float pa[4] = {aL2, aL3, A[0], A[1]}, pb[4] = {bL2, bL3, B[0], B[1]};
+        int f[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            f[j] = c0 + j < cend ? chain_map(var3(altx[j], altx[j + 2], altx[j + 4]), pa[j], pb[j], rawx[j], rawx[j + 2])
+                                 : MAP_ID;
+        int G0 = map_then(f[0], f[2]), G1 = map_then(f[1], f[3]);
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u0 = __shfl_up_sync(FULL, G0, d), u1 = __shfl_up_sync(FULL, G1, d);
+            if (lane >= d) {
+                G0 = map_then(u0, G0);
+                G1 = map_then(u1, G1);
+            }
+        }
+        int E0 = __shfl_up_sync(FULL, G0, 1), E1 = __shfl_up_sync(FULL, G1, 1);
+        if (lane == 0) E0 = E1 = MAP_ID;
+        int st[4];
+        st[0] = map_at(f[0], map_at(E0, 0));
+        st[1] = map_at(f[1], map_at(E1, 0));
+        st[2] = map_at(f[2], st[0]);
+        st[3] = map_at(f[3], st[1]);
+        float hr[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) hr[j] = c0 + j < cend ? (st[j] ? B[j] : A[j]) : 0.0f;
+        // refined hcd at c0-3 .. c0+6 and dginth at c0-2 .. c0+5
+        float h1 = __shfl_up_sync(FULL, hr[1], 1), h2 = __shfl_up_sync(FULL, hr[2], 1), h3 = __shfl_up_sync(FULL, hr[3], 1);
+        if (lane == 0) h1 = h2 = h3 = 0.0f;
+        const float hx[10] = {h1, h2, h3, hr[0], hr[1], hr[2], hr[3], __shfl_down_sync(FULL, hr[0], 1),
+                              __shfl_down_sync(FULL, hr[1], 1), __shfl_down_sync(FULL, hr[2], 1)};
+        const float dx[8] = {__shfl_up_sync(FULL, dg[2], 1), __shfl_up_sync(FULL, dg[3], 1), dg[0], dg[1], dg[2], dg[3],
+                             __shfl_down_sync(FULL, dg[0], 1), __shfl_down_sync(FULL, dg[1], 1)};
+        const bool row_hv = rr >= 6 && rr < g.rr1 - 6;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int c = c0 + j;
+            if (c >= cend || (p.cfa.at(g.top + rr, g.left + c) & 1) != 0) continue;  // R/B sites of the band
+            const int i = rr * TS + c;
+            cdd[i >> 1] = sqr(b.vcd[i] - hr[j]);
+            hcd_rb[i >> 1] = hr[j];
+            if (!row_hv || c < 6 || c >= g.cc1 - 6) continue;
+            const float* h = hx + j + 3;  // h[0] = hcd at c
+            const float lave = h[0] + h[-1] + h[-2] + h[-3];
+            const float rave = h[0] + h[1] + h[2] + h[3];
+            const float hl = sqr(h[0] - lave) + sqr(h[-1] - lave) + sqr(h[-2] - lave) + sqr(h[-3] - lave);
+            const float hrr = sqr(h[0] - rave) + sqr(h[1] - rave) + sqr(h[2] - rave) + sqr(h[3] - rave);
+            const float* v = b.vcd + i;
+            const float uave = v[0] + v[-V1] + v[-V2] + v[-V3];
+            const float dave = v[0] + v[V1] + v[V2] + v[V3];
+            const float vu = sqr(v[0] - uave) + sqr(v[-V1] - uave) + sqr(v[-V2] - uave) + sqr(v[-V3] - uave);
+            const float vd = sqr(v[0] - dave) + sqr(v[V1] - dave) + sqr(v[V2] - dave) + sqr(v[V3] - dave);
+            const float vvar = epssq + vw[j] * vd + (1.0f - vw[j]) * vu;
+            const float hvar = epssq + hw[j] * hrr + (1.0f - hw[j]) * hl;
+            const float* d = dx + j + 2;  // d[0] = dginth at c
+            const float hl1 = d[0] + d[-1] + d[-2];
+            const float hr1 = d[0] + d[1] + d[2];
+            const float vvar1 = b.hvwt[i >> 1];
+            const float hvar1 = epssq + hw[j] * hr1 + (1.0f - hw[j]) * hl1;
+            const float varwt = hvar / fmaxf(vvar + hvar, 1e-10f);
+            const float diffwt = hvar1 / fmaxf(vvar1 + hvar1, 1e-10f);
+            b.hvwt[i >> 1] = ((0.5f - varwt) * (0.5f - diffwt) > 0.0f && fabsf(0.5f - diffwt) < fabsf(0.5f - varwt))
+                                 ? varwt : diffwt;
+        }
+    }
 }
 
 struct NyqBox {
     int on, r0, r1, c0, c1;
 };
 
-// demosaic.rs:830-869: Nyquist test, flags and their bounding box
-// (first/last flagged row, min/max flagged column).
+// demosaic.rs:830-869: the Nyquist texture test at the R/B sites of
+// [6, rr1-6) x [6, cc1-6), the flags and their bounding box (first / last
+// flagged row, min / max flagged column).  Thread (column c, segment sg)
+// walks the R/B rows of its column with the squared gradients delhvsqsum
+// (demosaic.rs:612-622) of the 5x5 neighbourhood in a register window;
+// cddiffsq comes from the row pass (b.hcd[0 .. NH)).
 template <class P>
-__device__ NyqBox st_nyquist_flags(const P& p, const Geo& g, const Bufs& b, int* sh) {
+__device__ NyqBox st_nyq_test(const P& p, const Geo& g, const Bufs& b, int* sh) {
     const float nyqthresh = 0.5f;
     const float go0 = 0.14659727707323927f, go1 = 0.103592713382435f, go2 = 0.0732036125103057f,
                 go3 = 0.0365543548389495f;
@@ -544,29 +711,63 @@ __device__ NyqBox st_nyquist_flags(const P& p, const Geo& g, const Bufs& b, int*
         sh[2] = TS + 1;   // min col
         sh[3] = 0;        // max col
     }
+    if (threadIdx.x < TS) {
+        b.nyqw[threadIdx.x] = 0ull;
+        b.nyq2w[threadIdx.x] = 0ull;
+    }
     __syncthreads();
+    constexpr int PER = 15;  // R/B rows per segment: 4 x 15 >= 58
+    static_assert(VSEG * PER * 2 >= TS - 12, "Nyquist segments must cover the rows");
+    const int c = threadIdx.x & (TS - 1), sg = threadIdx.x / TS;
     int lr0 = 1 << 30, lr1 = -1, lc0 = TS + 1, lc1 = 0;
-    for_rb(p, g, 6, g.rr1 - 6, 6, g.cc1 - 6, [&](int rr, int cc) {
-        int i = rr * TS + cc;
-        const float *q = b.cdd, *s = b.gsq;
-        float t = (go0 * q[i] + go1 * (q[i - M1] + q[i - P1] + q[i + P1] + q[i + M1]) +
-                   go2 * (q[i - V2] + q[i - 2] + q[i + 2] + q[i + V2]) +
-                   go3 * (q[i - M2] + q[i - P2] + q[i + P2] + q[i + M2])) -
-                  (gg0 * s[i] + gg1 * (s[i - V1] + s[i + 1] + s[i - 1] + s[i + V1]) +
-                   gg2 * (s[i - M1] + s[i - P1] + s[i + P1] + s[i + M1]) +
-                   gg3 * (s[i - V2] + s[i - 2] + s[i + 2] + s[i + V2]) +
-                   gg4 * (s[i - V2 - 1] + s[i - V2 + 1] + s[i - TS - 2] + s[i - TS + 2] + s[i + TS - 2] +
-                          s[i + TS + 2] + s[i + V2 - 1] + s[i + V2 + 1]) +
-                   gg5 * (s[i - M2] + s[i - P2] + s[i + P2] + s[i + M2]));
-        uint8_t f = t > 0.0f ? 1 : 0;
-        b.nyq[i >> 1] = f;
-        if (f) {
-            lr0 = min(lr0, rr);
-            lr1 = max(lr1, rr);
-            lc0 = min(lc0, cc);
-            lc1 = max(lc1, cc);
+    const int ufirst = 6 + ((p.cfa.at(g.top + 6, g.left + c) & 1) != 0 ? 1 : 0);
+    const int nrb = (g.rr1 - 6 - ufirst + 1) / 2;
+    const int n0 = sg * PER, n1 = min(n0 + PER, nrb);
+    if (c >= 6 && c < g.cc1 - 6 && n0 < n1) {
+        const float* q = b.hcd;  // cddiffsq, half array
+        auto gsq = [&](int x, int y) {
+            const float* o = b.mos + x * TS + y;
+            return sqr(o[1] - o[-1]) + sqr(o[TS] - o[-TS]);
+        };
+        float w[5][5];  // delhvsqsum at rows u-2 .. u+2, columns c-2 .. c+2
+        const int ub = ufirst + 2 * n0;
+#pragma unroll
+        for (int x = 0; x < 5; x++)
+#pragma unroll
+            for (int y = 0; y < 5; y++) w[x][y] = gsq(ub - 2 + x, c - 2 + y);
+#pragma unroll
+        for (int n = 0; n < PER; n++) {
+            if (n0 + n < n1) {
+                const int u = ub + 2 * n;
+                if (n > 0) {
+#pragma unroll
+                    for (int y = 0; y < 5; y++) {
+                        w[0][y] = w[2][y];
+                        w[1][y] = w[3][y];
+                        w[2][y] = w[4][y];
+                        w[3][y] = gsq(u + 1, c - 2 + y);
+                        w[4][y] = gsq(u + 2, c - 2 + y);
+                    }
+                }
+                const int i = u * TS + c;
+                auto Q = [&](int o) { return q[(i + o) >> 1]; };
+                const float qs = go0 * Q(0) + go1 * (Q(-M1) + Q(-P1) + Q(P1) + Q(M1)) +
+                                 go2 * (Q(-V2) + Q(-2) + Q(2) + Q(V2)) + go3 * (Q(-M2) + Q(-P2) + Q(P2) + Q(M2));
+                const float gs = gg0 * w[2][2] + gg1 * (w[1][2] + w[2][3] + w[2][1] + w[3][2]) +
+                                 gg2 * (w[1][1] + w[1][3] + w[3][1] + w[3][3]) +
+                                 gg3 * (w[0][2] + w[2][0] + w[2][4] + w[4][2]) +
+                                 gg4 * (w[0][1] + w[0][3] + w[1][0] + w[1][4] + w[3][0] + w[3][4] + w[4][1] + w[4][3]) +
+                                 gg5 * (w[0][0] + w[0][4] + w[4][0] + w[4][4]);
+                if (qs - gs > 0.0f) {
+                    rbflag_set(b.nyqw, i);
+                    lr0 = min(lr0, u);
+                    lr1 = max(lr1, u);
+                    lc0 = min(lc0, c);
+                    lc1 = max(lc1, c);
+                }
+            }
         }
-    });
+    }
     if (lr1 >= 0) {
         atomicMin(&sh[0], lr0);
         atomicMax(&sh[1], lr1);
@@ -595,21 +796,21 @@ __device__ void st_nyquist_area(const P& p, const Geo& g, const Bufs& b, const N
     const float epssq = 1e-10f;
     for_rb(p, g, box.r0, box.r1, box.c0, box.c1, [&](int rr, int cc) {
         int i = rr * TS + cc;
-        const uint8_t* n = b.nyq;
-        unsigned s = n[(i - V2) >> 1] + n[(i - M1) >> 1] + n[(i - P1) >> 1] + n[(i - 2) >> 1] + n[(i + 2) >> 1] +
-                     n[(i + P1) >> 1] + n[(i + M1) >> 1] + n[(i + V2) >> 1];
-        b.nyq2[i >> 1] = s > 4 ? 1 : (s < 4 ? 0 : n[i >> 1]);
+        const unsigned long long* n = b.nyqw;
+        unsigned s = rbflag(n, i - V2) + rbflag(n, i - M1) + rbflag(n, i - P1) + rbflag(n, i - 2) + rbflag(n, i + 2) +
+                     rbflag(n, i + P1) + rbflag(n, i + M1) + rbflag(n, i + V2);
+        if (s > 4 || (s == 4 && rbflag(n, i))) rbflag_set(b.nyq2w, i);
     });
     __syncthreads();
     for_rb(p, g, box.r0, box.r1, box.c0, box.c1, [&](int rr, int cc) {
         int i = rr * TS + cc;
-        if (!b.nyq2[i >> 1]) return;
+        if (!rbflag(b.nyq2w, i)) return;
         const float* m = b.mos;
         float sumcfa = 0.f, sumh = 0.f, sumv = 0.f, sumsqh = 0.f, sumsqv = 0.f, area = 0.f;
         for (int di = -6; di < 7; di += 2)
             for (int dj = -6; dj < 7; dj += 2) {
                 int j = i + di * TS + dj;
-                if (b.nyq2[j >> 1]) {
+                if (rbflag(b.nyq2w, j)) {
                     float v = m[j];
                     sumcfa += v;
                     sumh += m[j - 1] + m[j + 1];
@@ -640,11 +841,11 @@ __device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b, Team tm) {
     for_rb_team(p, g, tm, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
         int i = rr * TS + cc;
         float wt = b.hvwt[i >> 1];
-        float d0 = wt * b.vcd[i] + (1.0f - wt) * b.hcd[i];
+        float d0 = wt * b.vcd[i] + (1.0f - wt) * b.hcd[NH + (i >> 1)];
         b.dgrb0[i >> 1] = d0;
         float gr = b.mos[i] + d0;
         b.rg[i >> 1] = gr;
-        if (b.nyq2[i >> 1]) {
+        if (rbflag(b.nyq2w, i)) {
             // neighbours of an R/B site are green sites: rgbgreen == mosaic there
             b.d2h[i >> 1] = sqr(gr - (b.mos[i - 1] + b.mos[i + 1]) * 0.5f);
             b.d2v[i >> 1] = sqr(gr - (b.mos[i - V1] + b.mos[i + V1]) * 0.5f);
@@ -662,20 +863,19 @@ __device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const 
     const float q0 = 0.169917f, q1 = 0.108947f, q2 = 0.069855f, q3 = 0.0287182f;
     for_rb_team(p, g, tm, box.r0, box.r1, box.c0, box.c1, [&](int rr, int cc) {
         int i = rr * TS + cc;
-        if (!b.nyq2[i >> 1]) return;
+        if (!rbflag(b.nyq2w, i)) return;
         // dgrb2_h/v are zero wherever the vote map is zero (the reference
         // writes 0 there or never writes them); masking keeps a previous
         // tile's values in the reused scratch out of the sums
-        const uint8_t* n2 = b.nyq2;
-        auto h = [&](int s) { return n2[s] ? b.d2h[s] : 0.0f; };
-        auto v = [&](int s) { return n2[s] ? b.d2v[s] : 0.0f; };
-        float gvarh = epssq + (q0 * h(i >> 1) + q1 * (h((i - M1) >> 1) + h((i - P1) >> 1) + h((i + P1) >> 1) + h((i + M1) >> 1)) +
-                               q2 * (h((i - V2) >> 1) + h((i - 2) >> 1) + h((i + 2) >> 1) + h((i + V2) >> 1)) +
-                               q3 * (h((i - M2) >> 1) + h((i - P2) >> 1) + h((i + P2) >> 1) + h((i + M2) >> 1)));
-        float gvarv = epssq + (q0 * v(i >> 1) + q1 * (v((i - M1) >> 1) + v((i - P1) >> 1) + v((i + P1) >> 1) + v((i + M1) >> 1)) +
-                               q2 * (v((i - V2) >> 1) + v((i - 2) >> 1) + v((i + 2) >> 1) + v((i + V2) >> 1)) +
-                               q3 * (v((i - M2) >> 1) + v((i - P2) >> 1) + v((i + P2) >> 1) + v((i + M2) >> 1)));
-        float d0 = (b.hcd[i] * gvarv + b.vcd[i] * gvarh) / (gvarv + gvarh);
+        auto h = [&](int x) { return rbflag(b.nyq2w, x) ? b.d2h[x >> 1] : 0.0f; };
+        auto v = [&](int x) { return rbflag(b.nyq2w, x) ? b.d2v[x >> 1] : 0.0f; };
+        float gvarh = epssq + (q0 * h(i) + q1 * (h(i - M1) + h(i - P1) + h(i + P1) + h(i + M1)) +
+                               q2 * (h(i - V2) + h(i - 2) + h(i + 2) + h(i + V2)) +
+                               q3 * (h(i - M2) + h(i - P2) + h(i + P2) + h(i + M2)));
+        float gvarv = epssq + (q0 * v(i) + q1 * (v(i - M1) + v(i - P1) + v(i + P1) + v(i + M1)) +
+                               q2 * (v(i - V2) + v(i - 2) + v(i + 2) + v(i + V2)) +
+                               q3 * (v(i - M2) + v(i - P2) + v(i + P2) + v(i + M2)));
+        float d0 = (b.hcd[NH + (i >> 1)] * gvarv + b.vcd[i] * gvarh) / (gvarv + gvarh);
         b.dgrb0[i >> 1] = d0;
         b.rg[i >> 1] = b.mos[i] + d0;
     });
@@ -795,7 +995,12 @@ __device__ void st_green_refine(const P& p, const Geo& g, const Bufs& b) {
     for_rb(p, g, 12, g.rr1 - 12, 12, g.cc1 - 12, [&](int rr, int cc) {
         int i = rr * TS + cc, h = i >> 1;
         if (!(fabsf(0.5f - b.pmwt[h]) >= fabsf(0.5f - b.hvwt[h]))) return;
-        const float *m = b.mos, *rb = b.rbint, *wv = b.wv, *wh = b.wh;
+        const float *m = b.mos, *rb = b.rbint;
+        // dirwts (demosaic.rs:612-622) of the four neighbours, from the mosaic
+        const float wvu = grad_w(m[i - 3 * V1], m[i - V2], m[i - V1], m[i], m[i + V1]);
+        const float wvd = grad_w(m[i - V1], m[i], m[i + V1], m[i + V2], m[i + 3 * V1]);
+        const float whl = grad_w(m[i - 3], m[i - 2], m[i - 1], m[i], m[i + 1]);
+        const float whr = grad_w(m[i - 1], m[i], m[i + 1], m[i + 2], m[i + 3]);
         float cru = m[i - V1] * 2.0f / (eps + rb[h] + rb[h - V1]);
         float crd = m[i + V1] * 2.0f / (eps + rb[h] + rb[h + V1]);
         float crl = m[i - 1] * 2.0f / (eps + rb[h] + rb[h - 1]);
@@ -804,8 +1009,8 @@ __device__ void st_green_refine(const P& p, const Geo& g, const Bufs& b) {
         float gd = fabsf(1.0f - crd) < arth ? rb[h] * crd : m[i + V1] + (rb[h] - rb[h + V1]) * 0.5f;
         float gl = fabsf(1.0f - crl) < arth ? rb[h] * crl : m[i - 1] + (rb[h] - rb[h - 1]) * 0.5f;
         float gr = fabsf(1.0f - crr) < arth ? rb[h] * crr : m[i + 1] + (rb[h] - rb[h + 1]) * 0.5f;
-        float gintv = (wv[i - V1] * gd + wv[i + V1] * gu) / fmaxf(wv[i + V1] + wv[i - V1], 1e-10f);
-        float ginth = (wh[i - 1] * gr + wh[i + 1] * gl) / fmaxf(wh[i - 1] + wh[i + 1], 1e-10f);
+        float gintv = (wvu * gd + wvd * gu) / fmaxf(wvd + wvu, 1e-10f);
+        float ginth = (whl * gr + whr * gl) / fmaxf(whl + whr, 1e-10f);
         if (gintv < rb[h]) {
             if (2.0f * gintv < rb[h]) {
                 gintv = ulim(gintv, m[i - V1], m[i + V1]);
@@ -934,57 +1139,37 @@ template <class Src, class Epi>
 __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constant__ Params<Src> p, const __grid_constant__ Epi epi) {
     float* smem = amaze_smem;
     __shared__ int box_sh[4];
+    // chain segment maps of the column pass, later the Nyquist row masks
+    __shared__ __align__(8) unsigned long long rowbits[2 * TS];
+    static_assert(VSEG * TS * 2 <= sizeof(unsigned long long) * TS, "segment maps fit the first mask array");
+    uint8_t* segmap = reinterpret_cast<uint8_t*>(rowbits);
     Bufs b;
     b.mos = smem;
     b.hcd = smem + NF;
     b.vcd = smem + 2 * NF;
     b.hvwt = smem + 3 * NF;
+    b.nyqw = rowbits;
+    b.nyq2w = rowbits + TS;
     float* s = reinterpret_cast<float*>(p.scratch + (size_t)blockIdx.x * SLOT_BYTES);
-    b.wv = s; s += NF;
-    b.wh = s; s += NF;
-    b.gsq = s; s += NF;
-    b.vcda = s; s += NF;
-    b.hcda = s; s += NF;
-    b.cdd = s; s += NF;
-    b.dgv = s; s += NF;
-    b.dgh = s; s += NF;
     b.dgrb0 = s; s += NH;
     b.dgrb1 = s; s += NH;
-    b.delp = s; s += NH;
-    b.delm = s; s += NH;
-    b.rbint = s; s += NH;
-    b.q1m = s; s += NH;
-    b.q1p = s; s += NH;
-    b.pmwt = s; s += NH;
-    b.rbm = s; s += NH;
-    b.rbp = s; s += NH;
-    b.nyqt = s; s += NH;
     b.rg = s; s += NH;
     b.d2h = s; s += NH;
     b.d2v = s; s += NH;
-    b.nyq = reinterpret_cast<uint8_t*>(s);
-    b.nyq2 = b.nyq + NH;
 
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
         Geo g = tile_geo(p.W, p.H, -16 + (tile / p.ntx) * 96, -16 + (tile % p.ntx) * 96);
         // arrays whose unwritten entries the reference reads as zero
-        for (int k = threadIdx.x; k < NH; k += blockDim.x) {
-            b.dgrb1[k] = 0.0f;
-            b.nyq2[k] = 0;
-        }
+        for (int k = threadIdx.x; k < NH; k += blockDim.x) b.dgrb1[k] = 0.0f;
         for (int k = threadIdx.x; k < NF; k += blockDim.x) b.mos[k] = 0.0f;
         __syncthreads();
         fill(p, g, b.mos);
         __syncthreads();
-        st_gradients(g, b);
+        st_vpass(p, g, b, segmap);
         __syncthreads();
-        st_colour_diff(p, g, b);
+        st_hpass(p, g, b);
         __syncthreads();
-        st_cd_refine(p, g, b);
-        __syncthreads();
-        st_hv_weight(p, g, b);
-        __syncthreads();
-        NyqBox box = st_nyquist_flags(p, g, b, box_sh);
+        NyqBox box = st_nyq_test(p, g, b, box_sh);
         if (box.on) {
             st_nyquist_area(p, g, b, box);
             __syncthreads();
@@ -1159,15 +1344,15 @@ extern "C" int imops_demosaic_amaze(const float* mosaic, int w, int h, const cha
 // per-CTA scratch slots taken from the fixed pool below instead of the
 // library's cached cudaMalloc buffer.
 //
-// The pool holds NOALLOC_SLOTS slots of SLOT_BYTES (31,981,568 bytes in all);
+// The pool holds NOALLOC_SLOTS slots of SLOT_BYTES (24,248,320 bytes in all);
 // every GPU that loads this library holds it until the process exits.  A call
 // runs min(tiles, NOALLOC_SLOTS) persistent CTAs, one slot each, so any image
-// size the reference's tiling accepts fits in the pool (large frames are
-// slower than with imops_demosaic_amaze, which uses one CTA per SM).
+// size the reference's tiling accepts fits in the pool (one slot per B200 SM,
+// so on B200 a call runs as many CTAs as imops_demosaic_amaze).
 namespace imops {
 namespace amaze {
 
-constexpr int NOALLOC_SLOTS = 32;
+constexpr int NOALLOC_SLOTS = 148;
 constexpr size_t NOALLOC_BYTES = (size_t)NOALLOC_SLOTS * SLOT_BYTES;
 static_assert(SLOT_BYTES % 256 == 0, "scratch slots must stay 256-byte aligned");
 
@@ -1227,7 +1412,7 @@ extern "C" int imops_demosaic_amaze_noalloc(const float* mosaic, int w, int h, c
     p.ntiles = tiles_of(w, h, &p.ntx);
     int grid = p.ntiles < NOALLOC_SLOTS ? p.ntiles : NOALLOC_SLOTS;
     if ((size_t)grid * SLOT_BYTES > NOALLOC_BYTES)
-        return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "AMaZE no-alloc: request exceeds the 31,981,568-byte scratch pool");
+        return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "AMaZE no-alloc: request exceeds the 24,248,320-byte scratch pool");
     void* pool = nullptr;
     if ((rc = noalloc_pool(&pool))) return rc;
     p.scratch = static_cast<uint8_t*>(pool);

@@ -93,8 +93,9 @@ int imops_demosaic_amaze(const float *mosaic, int w, int h, const char *cfa, int
  * graph, host applications that own all device memory through their own
  * allocator, or latency-critical paths that cannot afford cudaMalloc's
  * implicit synchronisation.  Output is identical to imops_demosaic_amaze.
- * Scratch comes from a fixed 31,981,568-byte pool (32 tile slots) that every
- * GPU loading this library holds until exit; a call uses at most 32 CTAs, so
+ * Scratch comes from a fixed 24,248,320-byte pool (148 tile slots, one per
+ * B200 SM) that every GPU loading this library holds until exit; a call uses
+ * at most 148 CTAs, so
  * any size imops_demosaic_amaze accepts is accepted, and a request that
  * would need more than the pool is rejected with IMOPS_ERR_UNSUPPORTED_SIZE.
  * The first call on a device resolves the pool's device address
