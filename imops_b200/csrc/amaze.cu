@@ -1,32 +1,34 @@
 // amaze.cu -- AMaZE demosaic for sm_100a, bit-identical to the reference's
 // demosaic_algorithms::Amaze (pichromatic/src/demosaic.rs:358-1379).
 //
-// Why the structure looks like the reference's tile loop: the reference
+// Why the structure follows the reference's tile loop: the reference
 // demosaics 128x128 tiles stepped by 96 from (-16,-16), restarts every tile
 // from zeroed scratch, mirrors a 16-pixel border at the image edge, bounds a
 // per-tile "Nyquist" region, and several stages update arrays in place while
 // scanning (a site reads its left / upper neighbours' already-updated
-// values).  All of that decides output bits, so one CTA owns one reference
-// tile and each stage runs over the same index domain; only the iteration
-// order within a stage is parallel, except where the reference's scan order
+// values).  All of that decides output bits, so one persistent CTA works one
+// reference tile at a time over the same index domain.  Where the scan order
 // is observable:
 //   * the hcd / vcd refinement (demosaic.rs:700-786) is a chain along each
-//     row (hcd, step 2) and each column (vcd, step 2): one thread per chain;
+//     row and column (step 2).  Each chain position picks one of two
+//     candidates from the previous position's pick, so a position is a map
+//     on two states and the chain a composition of maps: a warp scan for
+//     hcd, segment-wise composition for vcd.
 //   * the hvwt smoothing (demosaic.rs:949-958) and pmwt smoothing
-//     (demosaic.rs:1109-1118) read the row above already updated: one row
-//     per step, with a block barrier between rows.
+//     (demosaic.rs:1109-1118) read the row above already updated: one warp
+//     walks the rows, the previous row's values in registers.
 // Divisions are IEEE (-prec-div) and the file is built with --fmad=false so
 // every a*b+c rounds twice, as in the reference's Rust f32 code.
 //
-// Memory: the per-tile arrays of the reference total ~1.2 MB; the mosaic,
-// hcd, vcd and hvwt (the most re-read) live in shared memory (224 KB), the
-// others in a per-CTA slot of a global scratch buffer that the persistent
-// grid reuses tile after tile, so it stays resident in L2.
+// Memory: the reference's per-tile arrays total ~1.2 MB.  Here the H/V stage
+// is fused into a column pass and a row pass that keep gradients, colour
+// differences and chain states in registers, so every array a later stage
+// reads fits four shared-memory regions (224 KB, see Bufs) whose contents
+// change as the tile advances.  Nothing goes to global memory but the
+// output.
 #include "amaze.cuh"
 #include "color.cuh"
 
-#include <mutex>
-#include <vector>
 
 namespace imops {
 namespace amaze {
@@ -36,20 +38,22 @@ constexpr int V1 = 128, V2 = 256, V3 = 384, P1 = 127, P2 = 254, P3 = 381, M1 = 1
 constexpr int NTHREADS = 512;
 static_assert(NTHREADS % TS == 0 && NTHREADS % TSH == 0, "row mapping of the stage loops");
 
-// global scratch per CTA slot: 5 half arrays
-constexpr size_t SLOT_FLOATS = 5 * (size_t)NH;
-constexpr size_t SLOT_BYTES = SLOT_FLOATS * 4;
 constexpr size_t SMEM_BYTES = (3 * (size_t)NF + (size_t)NH) * 4 + 64;
 
+// Shared-memory regions and what they hold over a tile:
+//   mos  [NF]  the tile's mosaic
+//   HCD  [NF]  column pass: raw candidates | row pass: cddiffsq (first
+//              half), refined hcd at R/B sites (second half) | dgrb0 (first
+//              half, once the Nyquist test is done), pmwt (second half)
+//   VCD  [NF]  alternative candidates, then the refined vcd | dgrbsq1m/p |
+//              rbm/rbp | rbint (first half), final green (second half) |
+//              dgrb1 (first half)
+//   hvwt [NH]  vvar1, then hvwt
 struct Bufs {
-    // shared memory: the mosaic; hcd / vcd regions (candidates and refined
-    // colour differences, later the diagonal stage's arrays); hvwt
     float *mos, *hcd, *vcd, *hvwt;
-    // per-CTA global scratch (half arrays, flat index >> 1)
-    float *dgrb0, *dgrb1, *rg, *d2h, *d2v;
-    // shared-memory half arrays of the diagonal stage (set per tile)
+    float *cdd, *hcd_rb, *dgrb0, *dgrb1, *rg;
     float *q1m, *q1p, *pmwt, *rbm, *rbp, *rbint;
-    unsigned long long *nyqw, *nyq2w;  // shared: per-row bit masks of the R/B sites
+    unsigned long long *nyqw, *nyq2w;  // per-row bit masks of the R/B sites
 };
 
 // Nyquist flags are kept as one 64-bit mask per tile row, bit k for the R/B
@@ -97,7 +101,6 @@ struct Params {
     Bayer cfa;
     float clip;
     int ntx, ntiles;
-    uint8_t* scratch;
 };
 
 __device__ __forceinline__ float sqr(float x) { return x * x; }
@@ -835,50 +838,70 @@ __device__ void wave_hvwt(const P& p, const Geo& g, const Bufs& b) {
     wavefront(p, g, 3 * NF, 8, [](int, int, int, float) {});
 }
 
-// demosaic.rs:959-976: green at R/B sites from the smoothed weights.
+// demosaic.rs:959-976: the colour difference at R/B sites from the smoothed
+// weights.  rgbgreen there is mos + dgrb0 (not stored; st_green_refine
+// stores the final green).  dgrb2h/v are formed where st_nyquist_green
+// reads them.
 template <class P>
-__device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b, Team tm) {
-    for_rb_team(p, g, tm, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
-        int i = rr * TS + cc;
-        float wt = b.hvwt[i >> 1];
-        float d0 = wt * b.vcd[i] + (1.0f - wt) * b.hcd[NH + (i >> 1)];
-        b.dgrb0[i >> 1] = d0;
-        float gr = b.mos[i] + d0;
-        b.rg[i >> 1] = gr;
-        if (rbflag(b.nyq2w, i)) {
-            // neighbours of an R/B site are green sites: rgbgreen == mosaic there
-            b.d2h[i >> 1] = sqr(gr - (b.mos[i - 1] + b.mos[i + 1]) * 0.5f);
-            b.d2v[i >> 1] = sqr(gr - (b.mos[i - V1] + b.mos[i + V1]) * 0.5f);
-        } else {
-            b.d2h[i >> 1] = 0.0f;
-            b.d2v[i >> 1] = 0.0f;
-        }
+__device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
+    for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
+        const int i = rr * TS + cc;
+        const float wt = b.hvwt[i >> 1];
+        b.dgrb0[i >> 1] = wt * b.vcd[i] + (1.0f - wt) * b.hcd_rb[i >> 1];
     });
 }
 
-// demosaic.rs:978-998
+// demosaic.rs:978-998.  dgrb2h/v of a voted site j are
+// (rgbgreen_j - mean of its horizontal / vertical green neighbours)^2 with
+// rgbgreen_j = mos_j + dgrb0_j as st_green_rb left it, and zero at the other
+// sites.  New values are computed by all sites first and stored after a
+// barrier, so every site reads the pre-update dgrb0.
+constexpr int NYQ_PER_THREAD = (TS - 16) * TSH / NTHREADS + 1;
 template <class P>
-__device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const NyqBox& box, Team tm) {
+__device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const NyqBox& box) {
     const float epssq = 1e-10f;
     const float q0 = 0.169917f, q1 = 0.108947f, q2 = 0.069855f, q3 = 0.0287182f;
-    for_rb_team(p, g, tm, box.r0, box.r1, box.c0, box.c1, [&](int rr, int cc) {
-        int i = rr * TS + cc;
-        if (!rbflag(b.nyq2w, i)) return;
-        // dgrb2_h/v are zero wherever the vote map is zero (the reference
-        // writes 0 there or never writes them); masking keeps a previous
-        // tile's values in the reused scratch out of the sums
-        auto h = [&](int x) { return rbflag(b.nyq2w, x) ? b.d2h[x >> 1] : 0.0f; };
-        auto v = [&](int x) { return rbflag(b.nyq2w, x) ? b.d2v[x >> 1] : 0.0f; };
-        float gvarh = epssq + (q0 * h(i) + q1 * (h(i - M1) + h(i - P1) + h(i + P1) + h(i + M1)) +
-                               q2 * (h(i - V2) + h(i - 2) + h(i + 2) + h(i + V2)) +
-                               q3 * (h(i - M2) + h(i - P2) + h(i + P2) + h(i + M2)));
-        float gvarv = epssq + (q0 * v(i) + q1 * (v(i - M1) + v(i - P1) + v(i + P1) + v(i + M1)) +
-                               q2 * (v(i - V2) + v(i - 2) + v(i + 2) + v(i + V2)) +
-                               q3 * (v(i - M2) + v(i - P2) + v(i + P2) + v(i + M2)));
-        float d0 = (b.hcd[NH + (i >> 1)] * gvarv + b.vcd[i] * gvarh) / (gvarv + gvarh);
-        b.dgrb0[i >> 1] = d0;
-        b.rg[i >> 1] = b.mos[i] + d0;
-    });
+    const float* m = b.mos;
+    auto d2 = [&](int j, float& h, float& v) {
+        if (!rbflag(b.nyq2w, j)) {
+            h = v = 0.0f;
+            return;
+        }
+        const float gr = m[j] + b.dgrb0[j >> 1];
+        h = sqr(gr - (m[j - 1] + m[j + 1]) * 0.5f);
+        v = sqr(gr - (m[j - V1] + m[j + V1]) * 0.5f);
+    };
+    float nd[NYQ_PER_THREAD];
+    const int n = (box.r1 - box.r0) * TSH;
+#pragma unroll
+    for (int s = 0; s < NYQ_PER_THREAD; s++) {
+        const int k = (int)threadIdx.x + s * NTHREADS;
+        nd[s] = 0.0f;
+        if (k >= n) continue;
+        const int rr = box.r0 + (k >> 6);
+        const int cc = box.c0 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k & (TSH - 1));
+        const int i = rr * TS + cc;
+        if (cc >= box.c1 || !rbflag(b.nyq2w, i)) continue;
+        float h[13], v[13];
+        const int off[13] = {0, -M1, -P1, P1, M1, -V2, -2, 2, V2, -M2, -P2, P2, M2};
+#pragma unroll
+        for (int t = 0; t < 13; t++) d2(i + off[t], h[t], v[t]);
+        const float gvarh = epssq + (q0 * h[0] + q1 * (h[1] + h[2] + h[3] + h[4]) + q2 * (h[5] + h[6] + h[7] + h[8]) +
+                                     q3 * (h[9] + h[10] + h[11] + h[12]));
+        const float gvarv = epssq + (q0 * v[0] + q1 * (v[1] + v[2] + v[3] + v[4]) + q2 * (v[5] + v[6] + v[7] + v[8]) +
+                                     q3 * (v[9] + v[10] + v[11] + v[12]));
+        nd[s] = (b.hcd_rb[i >> 1] * gvarv + b.vcd[i] * gvarh) / (gvarv + gvarh);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < NYQ_PER_THREAD; s++) {
+        const int k = (int)threadIdx.x + s * NTHREADS;
+        if (k >= n) continue;
+        const int rr = box.r0 + (k >> 6);
+        const int cc = box.c0 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k & (TSH - 1));
+        const int i = rr * TS + cc;
+        if (cc < box.c1 && rbflag(b.nyq2w, i)) b.dgrb0[i >> 1] = nd[s];
+    }
 }
 
 // demosaic.rs:1000-1019, the dgrbsq1m/p half: squared diagonal differences
@@ -971,11 +994,11 @@ __device__ void st_diag_rb(const P& p, const Geo& g, const Bufs& b, Team tm) {
     });
 }
 
-// demosaic.rs:1109-1118: pmwt smoothing (one warp); pmwt lives at the vcd
-// region of shared memory (amaze_smem + 2 NF) while it runs.
+// demosaic.rs:1109-1118: pmwt smoothing (one warp); pmwt lives in the
+// second half of the HCD region (amaze_smem + NF + NH).
 template <class P>
 __device__ void wave_pmwt(const P& p, const Geo& g) {
-    wavefront(p, g, 2 * NF, 10, [](int, int, int, float) {});
+    wavefront(p, g, NF + NH, 10, [](int, int, int, float) {});
 }
 
 // demosaic.rs:1119-1122: rbint from the final diagonal weight.
@@ -994,7 +1017,10 @@ __device__ void st_green_refine(const P& p, const Geo& g, const Bufs& b) {
     const float eps = 1e-5f, arth = 0.75f;
     for_rb(p, g, 12, g.rr1 - 12, 12, g.cc1 - 12, [&](int rr, int cc) {
         int i = rr * TS + cc, h = i >> 1;
-        if (!(fabsf(0.5f - b.pmwt[h]) >= fabsf(0.5f - b.hvwt[h]))) return;
+        if (!(fabsf(0.5f - b.pmwt[h]) >= fabsf(0.5f - b.hvwt[h]))) {
+            b.rg[h] = b.mos[i] + b.dgrb0[h];  // rgbgreen as st_green_rb / st_nyquist_green left it
+            return;
+        }
         const float *m = b.mos, *rb = b.rbint;
         // dirwts (demosaic.rs:612-622) of the four neighbours, from the mosaic
         const float wvu = grad_w(m[i - 3 * V1], m[i - V2], m[i - V1], m[i], m[i + V1]);
@@ -1150,17 +1176,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constan
     b.hvwt = smem + 3 * NF;
     b.nyqw = rowbits;
     b.nyq2w = rowbits + TS;
-    float* s = reinterpret_cast<float*>(p.scratch + (size_t)blockIdx.x * SLOT_BYTES);
-    b.dgrb0 = s; s += NH;
-    b.dgrb1 = s; s += NH;
-    b.rg = s; s += NH;
-    b.d2h = s; s += NH;
-    b.d2v = s; s += NH;
+    b.cdd = b.hcd;
+    b.hcd_rb = b.hcd + NH;
+    b.dgrb0 = b.hcd;
+    b.pmwt = b.hcd + NH;
+    b.q1m = b.rbm = b.rbint = b.dgrb1 = b.vcd;
+    b.q1p = b.rbp = b.rg = b.vcd + NH;
 
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
         Geo g = tile_geo(p.W, p.H, -16 + (tile / p.ntx) * 96, -16 + (tile % p.ntx) * 96);
-        // arrays whose unwritten entries the reference reads as zero
-        for (int k = threadIdx.x; k < NH; k += blockDim.x) b.dgrb1[k] = 0.0f;
         for (int k = threadIdx.x; k < NF; k += blockDim.x) b.mos[k] = 0.0f;
         __syncthreads();
         fill(p, g, b.mos);
@@ -1177,77 +1201,31 @@ __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constan
         // hvwt smoothing: one warp walks the rows (the others wait)
         if ((threadIdx.x >> 5) == 0) wave_hvwt(p, g, b);
         __syncthreads();
-        st_green_rb(p, g, b, whole_block());
+        st_green_rb(p, g, b);
         __syncthreads();
-        if (box.on) st_nyquist_green(p, g, b, box, whole_block());
+        if (box.on) st_nyquist_green(p, g, b, box);
         __syncthreads();
-        // hcd / vcd are dead from here: the diagonal stage keeps its arrays
-        // in their shared memory
-        Bufs d = b;
-        d.q1m = b.hcd;
-        d.q1p = b.hcd + NH;
-        d.pmwt = b.vcd;
-        d.rbint = b.vcd + NH;
-        st_diag_setup(p, g, d, whole_block());
+        // diagonal stage, in the regions the H/V stage no longer needs
+        st_diag_setup(p, g, b, whole_block());
         __syncthreads();
-        st_diag_weight(p, g, d, whole_block());
+        st_diag_weight(p, g, b, whole_block());
         __syncthreads();
-        d.rbm = b.hcd;  // over dgrbsq1m/p, no longer read
-        d.rbp = b.hcd + NH;
-        st_diag_rb(p, g, d, whole_block());
+        st_diag_rb(p, g, b, whole_block());
         __syncthreads();
         if ((threadIdx.x >> 5) == 0) wave_pmwt(p, g);
         __syncthreads();
-        st_rbint(p, g, d);
+        st_rbint(p, g, b);
         __syncthreads();
-        st_green_refine(p, g, d);
+        st_green_refine(p, g, b);
         __syncthreads();
-        st_chroma(p, g, d);
+        // dgrb1 starts at zero, as the reference's fresh array does
+        for (int k = threadIdx.x; k < NH; k += blockDim.x) b.dgrb1[k] = 0.0f;
         __syncthreads();
-        st_output(p, g, d, epi);
+        st_chroma(p, g, b);
+        __syncthreads();
+        st_output(p, g, b, epi);
         __syncthreads();
     }
-}
-
-// Per-(device, stream) scratch cache for the convenience entry point.
-struct ScratchCache {
-    std::mutex mu;
-    struct Entry {
-        int dev;
-        cudaStream_t stream;
-        void* ptr;
-        size_t bytes;
-    };
-    std::vector<Entry> entries;
-};
-ScratchCache g_cache;
-
-int get_scratch(cudaStream_t stream, size_t bytes, void** out) {
-    if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, "injected allocation failure (AMaZE scratch)");
-    int dev = 0;
-    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
-    std::lock_guard<std::mutex> lock(g_cache.mu);
-    for (auto& e : g_cache.entries) {
-        if (e.dev == dev && e.stream == stream) {
-            if (e.bytes >= bytes) {
-                *out = e.ptr;
-                return IMOPS_OK;
-            }
-            IMOPS_CUDA_TRY(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
-            IMOPS_CUDA_TRY(cudaFree(e.ptr), "cudaFree(AMaZE scratch)");
-            e.ptr = nullptr;
-            e.bytes = 0;
-            IMOPS_CUDA_TRY(cudaMalloc(&e.ptr, bytes), "cudaMalloc(AMaZE scratch)");
-            e.bytes = bytes;
-            *out = e.ptr;
-            return IMOPS_OK;
-        }
-    }
-    void* ptr = nullptr;
-    IMOPS_CUDA_TRY(cudaMalloc(&ptr, bytes), "cudaMalloc(AMaZE scratch)");
-    g_cache.entries.push_back({dev, stream, ptr, bytes});
-    *out = ptr;
-    return IMOPS_OK;
 }
 
 int tiles_of(int W, int H, int* ntx) {
@@ -1275,10 +1253,6 @@ int launch(const Src& src, int W, int H, const CfaDev& cfa, float clip, const Ep
     p.ntiles = tiles_of(W, H, &p.ntx);
     int grid = sm_count();
     if (grid > p.ntiles) grid = p.ntiles;
-    void* scratch = nullptr;
-    int rc = get_scratch(stream, SLOT_BYTES * (size_t)grid, &scratch);
-    if (rc) return rc;
-    p.scratch = static_cast<uint8_t*>(scratch);
     if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, "injected launch failure (AMaZE)");
     IMOPS_CUDA_TRY(cudaFuncSetAttribute(amaze_kernel<Src, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)SMEM_BYTES),
@@ -1334,92 +1308,25 @@ extern "C" int imops_demosaic_amaze(const float* mosaic, int w, int h, const cha
 }
 
 // ---------------------------------------------------------------------------
-// No-allocation variant.
+// No-allocation entry point.
 //
 // Some callers cannot call cudaMalloc: code recording work into a CUDA graph
 // (allocation is not a stream operation), host applications whose device
 // memory is owned by their own allocator or budget, and latency-critical
 // paths where cudaMalloc's implicit device synchronisation is unacceptable.
-// imops_demosaic_amaze_noalloc serves them: the same AMaZE kernel, with its
-// per-CTA scratch slots taken from the fixed pool below instead of the
-// library's cached cudaMalloc buffer.
-//
-// The pool holds NOALLOC_SLOTS slots of SLOT_BYTES (24,248,320 bytes in all);
-// every GPU that loads this library holds it until the process exits.  A call
-// runs min(tiles, NOALLOC_SLOTS) persistent CTAs, one slot each, so any image
-// size the reference's tiling accepts fits in the pool (one slot per B200 SM,
-// so on B200 a call runs as many CTAs as imops_demosaic_amaze).
-namespace imops {
-namespace amaze {
-
-constexpr int NOALLOC_SLOTS = 148;
-constexpr size_t NOALLOC_BYTES = (size_t)NOALLOC_SLOTS * SLOT_BYTES;
-static_assert(SLOT_BYTES % 256 == 0, "scratch slots must stay 256-byte aligned");
-
-static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_BYTES];
-
-struct NoallocSetup {
-    std::mutex mu;
-    void* ptr[128] = {};
-};
-NoallocSetup g_noalloc;
-
-// Once per device, with that device current: the device address of the pool
-// (host code must not pass the symbol itself to a kernel) and the kernel's
-// shared-memory opt-in.
-int noalloc_pool(void** out) {
-    int dev = 0;
-    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
-    if (dev < 0 || dev >= 128) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE no-alloc: device index above 127");
-    std::lock_guard<std::mutex> lock(g_noalloc.mu);
-    if (!g_noalloc.ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(AMaZE no-alloc pool)");
-        e = cudaFuncSetAttribute(amaze_kernel<SrcF32, EpiRGB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)SMEM_BYTES);
-        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(AMaZE no-alloc)");
-        g_noalloc.ptr[dev] = p;
-    }
-    *out = g_noalloc.ptr[dev];
-    return IMOPS_OK;
-}
-
-}  // namespace amaze
-}  // namespace imops
-
+// The AMaZE kernel keeps every per-tile array in shared memory, so it needs
+// no device scratch at all; imops_demosaic_amaze_noalloc states that as a
+// contract (imops_demosaic_amaze happens to allocate nothing either, but does
+// not promise it).  The first call on a device sets the kernel's
+// shared-memory limit (cudaFuncSetAttribute) and loads it: make that call
+// before any stream capture.
 extern "C" int imops_demosaic_amaze_noalloc(const float* mosaic, int w, int h, const char* cfa, int shift_x,
                                             int shift_y, float clip_pt, float* rgb, imops_stream_t stream) {
     using namespace imops;
-    using namespace imops::amaze;
     clear_error();
     CfaDev c;
     int rc = parse_cfa(cfa, shift_x, shift_y, &c);
     if (rc) return rc;
     if (!mosaic || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE no-alloc: NULL buffer");
-    if (w <= 0 || h <= 0) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE no-alloc: empty image");
-    if (!cfa_is_bayer(c)) return fail(IMOPS_ERR_UNSUPPORTED_CFA, "AMaZE needs a 2x2 Bayer CFA");
-    if (!size_supported(w, h))
-        return fail(IMOPS_ERR_UNSUPPORTED_SIZE,
-                    "AMaZE: for this image size the reference's 128x128 tile border fill indexes past its tile "
-                    "buffer (width or height mod 96 in 1..15)");
-    Params<SrcF32> p;
-    p.in = SrcF32{mosaic, w};
-    p.W = w;
-    p.H = h;
-    for (int i = 0; i < 4; i++) p.cfa.c[i] = c.col[i];
-    p.clip = clip_pt;
-    p.ntiles = tiles_of(w, h, &p.ntx);
-    int grid = p.ntiles < NOALLOC_SLOTS ? p.ntiles : NOALLOC_SLOTS;
-    if ((size_t)grid * SLOT_BYTES > NOALLOC_BYTES)
-        return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "AMaZE no-alloc: request exceeds the 24,248,320-byte scratch pool");
-    void* pool = nullptr;
-    if ((rc = noalloc_pool(&pool))) return rc;
-    p.scratch = static_cast<uint8_t*>(pool);
-    // nothing in the pool has to start at zero: every tile clears the arrays
-    // whose unwritten entries it reads before using them
-    amaze_kernel<SrcF32, EpiRGB><<<grid, NTHREADS, SMEM_BYTES, as_stream(stream)>>>(p, EpiRGB{rgb, w});
-    note_launch();
-    IMOPS_CUDA_TRY(cudaGetLastError(), "AMaZE no-alloc launch");
-    return IMOPS_OK;
+    return amaze::launch(amaze::SrcF32{mosaic, w}, w, h, c, clip_pt, amaze::EpiRGB{rgb, w}, as_stream(stream));
 }

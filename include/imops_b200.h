@@ -93,17 +93,11 @@ int imops_demosaic_amaze(const float *mosaic, int w, int h, const char *cfa, int
  * graph, host applications that own all device memory through their own
  * allocator, or latency-critical paths that cannot afford cudaMalloc's
  * implicit synchronisation.  Output is identical to imops_demosaic_amaze.
- * Scratch comes from a fixed 24,248,320-byte pool (148 tile slots, one per
- * B200 SM) that every GPU loading this library holds until exit; a call uses
- * at most 148 CTAs, so
- * any size imops_demosaic_amaze accepts is accepted, and a request that
- * would need more than the pool is rejected with IMOPS_ERR_UNSUPPORTED_SIZE.
- * The first call on a device resolves the pool's device address
- * (cudaGetSymbolAddress) and sets the kernel's shared-memory limit: make
- * that first call before any stream capture.  All calls share the pool and
- * it keeps the last call's contents (the kernel clears what must start at
- * zero per tile); calls that overlap on the GPU, e.g. on two streams, race
- * on it and must be serialised by the caller. */
+ * The kernel keeps all per-tile state in shared memory, so there is no
+ * scratch and no size limit beyond imops_amaze_size_supported.  The first
+ * call on a device sets the kernel's shared-memory limit
+ * (cudaFuncSetAttribute) and loads it: make that first call before any
+ * stream capture.  Calls on different streams may overlap. */
 int imops_demosaic_amaze_noalloc(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y,
                                  float clip_pt, float *rgb, imops_stream_t stream);
 

@@ -1,8 +1,8 @@
 """imops_demosaic_amaze_noalloc: AMaZE for callers that cannot allocate
 device memory (graph capture, host-owned allocators, latency-critical
 paths).  Its output must equal imops_demosaic_amaze's bit for bit, also on
-the second of two calls in a row, when its fixed scratch pool still holds
-the previous call's data.
+the second of two calls in a row (the kernel's shared memory then still
+holds the previous call's data).
 
 This file is named so pytest collects it last; it also passes when run
 alone in a fresh process.
@@ -31,7 +31,7 @@ def test_noalloc_matches_allocating_entry_twice(gpu):
 
     lib = im.lib()
     stream = torch.cuda.current_stream()
-    frames = [synthetic.mosaic_f32(1024, 1536, seed=41) * np.float32(1.2),  # 204 tiles: 32-CTA persistent grid
+    frames = [synthetic.mosaic_f32(1024, 1536, seed=41) * np.float32(1.2),  # 204 tiles: persistent grid, tiles per CTA > 1
               np.random.default_rng(42).random((320, 400), dtype=np.float32)]
     for m_np in frames:
         m = torch.from_numpy(m_np).to(gpu)
