@@ -40,19 +40,19 @@ static_assert(NTHREADS % TS == 0 && NTHREADS % TSH == 0, "row mapping of the sta
 
 constexpr size_t SMEM_BYTES = (3 * (size_t)NF + (size_t)NH) * 4 + 64;
 
-// Shared-memory regions and what they hold over a tile:
+// Shared-memory regions and what they hold over a tile (H0/H1, V0/V1: the
+// halves of HCD / VCD, each a half array indexed by flat index >> 1):
 //   mos  [NF]  the tile's mosaic
-//   HCD  [NF]  column pass: raw candidates | row pass: cddiffsq (first
-//              half), refined hcd at R/B sites (second half) | dgrb0 (first
-//              half, once the Nyquist test is done), pmwt (second half)
-//   VCD  [NF]  alternative candidates, then the refined vcd | dgrbsq1m/p |
-//              rbm/rbp | rbint (first half), final green (second half) |
-//              dgrb1 (first half)
+//   HCD  [NF]  column pass: raw candidates | row pass: H0 cddiffsq, H1
+//              refined hcd at R/B sites | H0 vcd at R/B sites (after the
+//              Nyquist test) | H0 rbint, H1 final green
+//   VCD  [NF]  alternative candidates, then the refined vcd | V0 dgrbsq1m,
+//              V1 dgrbsq1p | V0 pmwt, V1 dgrb0 | V0 dgrb1
 //   hvwt [NH]  vvar1, then hvwt
 struct Bufs {
     float *mos, *hcd, *vcd, *hvwt;
-    float *cdd, *hcd_rb, *dgrb0, *dgrb1, *rg;
-    float *q1m, *q1p, *pmwt, *rbm, *rbp, *rbint;
+    float *cdd, *hcd_rb, *vcd_rb, *dgrb0, *dgrb1, *rg;
+    float *q1m, *q1p, *pmwt, *rbint;
     unsigned long long *nyqw, *nyq2w;  // per-row bit masks of the R/B sites
 };
 
@@ -239,6 +239,10 @@ __device__ __forceinline__ void for_rb(const P& p, const Geo& g, int r0, int r1,
         if (cc < c1) f(rr, cc);
     }
 }
+
+// R/B sites of rows [8, rr1-8) per thread, for stages that keep their
+// results in registers across a barrier (two-phase in-place updates).
+constexpr int RB_PER_THREAD = (TS - 16) * TSH / NTHREADS + 1;
 
 // A subset of the block's threads working one stage: thread t of n.
 struct Team {
@@ -847,7 +851,7 @@ __device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
     for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
         const int i = rr * TS + cc;
         const float wt = b.hvwt[i >> 1];
-        b.dgrb0[i >> 1] = wt * b.vcd[i] + (1.0f - wt) * b.hcd_rb[i >> 1];
+        b.dgrb0[i >> 1] = wt * b.vcd_rb[i >> 1] + (1.0f - wt) * b.hcd_rb[i >> 1];
     });
 }
 
@@ -856,7 +860,7 @@ __device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
 // rgbgreen_j = mos_j + dgrb0_j as st_green_rb left it, and zero at the other
 // sites.  New values are computed by all sites first and stored after a
 // barrier, so every site reads the pre-update dgrb0.
-constexpr int NYQ_PER_THREAD = (TS - 16) * TSH / NTHREADS + 1;
+
 template <class P>
 __device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const NyqBox& box) {
     const float epssq = 1e-10f;
@@ -871,10 +875,10 @@ __device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const 
         h = sqr(gr - (m[j - 1] + m[j + 1]) * 0.5f);
         v = sqr(gr - (m[j - V1] + m[j + V1]) * 0.5f);
     };
-    float nd[NYQ_PER_THREAD];
+    float nd[RB_PER_THREAD];
     const int n = (box.r1 - box.r0) * TSH;
 #pragma unroll
-    for (int s = 0; s < NYQ_PER_THREAD; s++) {
+    for (int s = 0; s < RB_PER_THREAD; s++) {
         const int k = (int)threadIdx.x + s * NTHREADS;
         nd[s] = 0.0f;
         if (k >= n) continue;
@@ -890,11 +894,11 @@ __device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const 
                                      q3 * (h[9] + h[10] + h[11] + h[12]));
         const float gvarv = epssq + (q0 * v[0] + q1 * (v[1] + v[2] + v[3] + v[4]) + q2 * (v[5] + v[6] + v[7] + v[8]) +
                                      q3 * (v[9] + v[10] + v[11] + v[12]));
-        nd[s] = (b.hcd_rb[i >> 1] * gvarv + b.vcd[i] * gvarh) / (gvarv + gvarh);
+        nd[s] = (b.hcd_rb[i >> 1] * gvarv + b.vcd_rb[i >> 1] * gvarh) / (gvarv + gvarh);
     }
     __syncthreads();
 #pragma unroll
-    for (int s = 0; s < NYQ_PER_THREAD; s++) {
+    for (int s = 0; s < RB_PER_THREAD; s++) {
         const int k = (int)threadIdx.x + s * NTHREADS;
         if (k >= n) continue;
         const int rr = box.r0 + (k >> 6);
@@ -926,33 +930,63 @@ __device__ void st_diag_setup(const P& p, const Geo& g, const Bufs& b, Team tm) 
     }
 }
 
-// demosaic.rs:1021-1107, the diagonal weight pmwt (from dgrbsq1m/p).
+// demosaic.rs:1021-1107, the diagonal weight pmwt (from dgrbsq1m/p), at
+// the R/B sites of [8, rr1-8).  pmwt goes over dgrbsq1m, so every site is
+// computed before any is stored.
 template <class P>
-__device__ void st_diag_weight(const P& p, const Geo& g, const Bufs& b, Team tm) {
+__device__ void st_diag_weight(const P& p, const Geo& g, const Bufs& b) {
     const float epssq = 1e-10f;
     const float ge0 = 0.13719494435797422f, ge1 = 0.05640252782101291f;
-    for_rb_team(p, g, tm, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
-        int i = rr * TS + cc, h = i >> 1;
-        const float *qm = b.q1m, *qp = b.q1p;
+    const float *qm = b.q1m, *qp = b.q1p;
+    const int n = (g.rr1 - 16) * TSH;
+    float pw[RB_PER_THREAD];
+#pragma unroll
+    for (int t = 0; t < RB_PER_THREAD; t++) {
+        const int k = (int)threadIdx.x + t * NTHREADS;
+        const int rr = 8 + (k >> 6);
+        const int cc = 8 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k & (TSH - 1));
+        pw[t] = 0.0f;
+        if (k >= n || cc >= g.cc1 - 8) continue;
+        const int i = rr * TS + cc;
         float varm = epssq + ge0 * (qm[(i - V1) >> 1] + qm[(i - 1) >> 1] + qm[(i + 1) >> 1] + qm[(i + V1) >> 1]) +
                      ge1 * (qm[(i - V2 - 1) >> 1] + qm[(i - V2 + 1) >> 1] + qm[(i - 2 - V1) >> 1] + qm[(i + 2 - V1) >> 1] +
                             qm[(i - 2 + V1) >> 1] + qm[(i + 2 + V1) >> 1] + qm[(i + V2 - 1) >> 1] + qm[(i + V2 + 1) >> 1]);
         float varp = epssq + ge0 * (qp[(i - V1) >> 1] + qp[(i - 1) >> 1] + qp[(i + 1) >> 1] + qp[(i + V1) >> 1]) +
                      ge1 * (qp[(i - V2 - 1) >> 1] + qp[(i - V2 + 1) >> 1] + qp[(i - 2 - V1) >> 1] + qp[(i + 2 - V1) >> 1] +
                             qp[(i - 2 + V1) >> 1] + qp[(i + 2 + V1) >> 1] + qp[(i + V2 - 1) >> 1] + qp[(i + V2 + 1) >> 1]);
-        b.pmwt[h] = varm / (varp + varm);
+        pw[t] = varm / (varp + varm);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < RB_PER_THREAD; t++) {
+        const int k = (int)threadIdx.x + t * NTHREADS;
+        const int rr = 8 + (k >> 6);
+        const int cc = 8 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k & (TSH - 1));
+        if (k < n && cc < g.cc1 - 8) b.pmwt[(rr * TS + cc) >> 1] = pw[t];
+    }
+}
+
+// The refined vcd of the R/B sites of [8, rr1-8), the only ones read after
+// the Nyquist test, into a half array (frees the VCD region).
+template <class P>
+__device__ void st_compact_vcd(const P& p, const Geo& g, const Bufs& b) {
+    for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
+        const int i = rr * TS + cc;
+        b.vcd_rb[i >> 1] = b.vcd[i];
     });
 }
 
-// demosaic.rs:1021-1107, the diagonal R+B estimates rbm/rbp.  delm/delp of
-// the R/B site j are |m[j+M1] - m[j-M1]| and |m[j-P1] - m[j+P1]| (the
+// demosaic.rs:1021-1107 (the diagonal R+B estimates rbm / rbp) and
+// :1119-1122 (rbint from them and the final pmwt).  rbm / rbp are only read
+// by rbint, so they are formed here, at the sites rbint needs.  delm / delp
+// of the R/B site j are |m[j+M1] - m[j-M1]| and |m[j-P1] - m[j+P1]| (the
 // reference stores them per column pair; the sign inside fabs does not
 // change the value).
 template <class P>
-__device__ void st_diag_rb(const P& p, const Geo& g, const Bufs& b, Team tm) {
+__device__ void st_rbint(const P& p, const Geo& g, const Bufs& b) {
     const float eps = 1e-5f, arth = 0.75f;
-    for_rb_team(p, g, tm, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
-        int i = rr * TS + cc, h = i >> 1;
+    for_rb(p, g, 10, g.rr1 - 10, 10, g.cc1 - 10, [&](int rr, int cc) {
+        const int i = rr * TS + cc, h = i >> 1;
         const float* m = b.mos;
         auto dm = [&](int j) { return fabsf(m[j + M1] - m[j - M1]); };
         auto dp = [&](int j) { return fabsf(m[j - P1] - m[j + P1]); };
@@ -989,26 +1023,16 @@ __device__ void st_diag_rb(const P& p, const Geo& g, const Bufs& b, Team tm) {
         }
         if (rbp > p.clip) rbp = ulim(rbp, m[i - P1], m[i + P1]);
         if (rbm > p.clip) rbm = ulim(rbm, m[i - M1], m[i + M1]);
-        b.rbp[h] = rbp;
-        b.rbm[h] = rbm;
+        const float pm = b.pmwt[h];
+        b.rbint[h] = (m[i] + rbm * (1.0f - pm) + rbp * pm) * 0.5f;
     });
 }
 
 // demosaic.rs:1109-1118: pmwt smoothing (one warp); pmwt lives in the
-// second half of the HCD region (amaze_smem + NF + NH).
+// first half of the VCD region (amaze_smem + 2 NF).
 template <class P>
 __device__ void wave_pmwt(const P& p, const Geo& g) {
-    wavefront(p, g, NF + NH, 10, [](int, int, int, float) {});
-}
-
-// demosaic.rs:1119-1122: rbint from the final diagonal weight.
-template <class P>
-__device__ void st_rbint(const P& p, const Geo& g, const Bufs& b) {
-    for_rb(p, g, 10, g.rr1 - 10, 10, g.cc1 - 10, [&](int rr, int cc) {
-        const int i = rr * TS + cc, h = i >> 1;
-        const float pm = b.pmwt[h];
-        b.rbint[h] = (b.mos[i] + b.rbm[h] * (1.0f - pm) + b.rbp[h] * pm) * 0.5f;
-    });
+    wavefront(p, g, 2 * NF, 10, [](int, int, int, float) {});
 }
 
 // demosaic.rs:1125-1194
@@ -1176,12 +1200,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constan
     b.hvwt = smem + 3 * NF;
     b.nyqw = rowbits;
     b.nyq2w = rowbits + TS;
-    b.cdd = b.hcd;
-    b.hcd_rb = b.hcd + NH;
-    b.dgrb0 = b.hcd;
-    b.pmwt = b.hcd + NH;
-    b.q1m = b.rbm = b.rbint = b.dgrb1 = b.vcd;
-    b.q1p = b.rbp = b.rg = b.vcd + NH;
+    b.cdd = b.vcd_rb = b.rbint = b.hcd;
+    b.hcd_rb = b.rg = b.hcd + NH;
+    b.q1m = b.pmwt = b.dgrb1 = b.vcd;
+    b.q1p = b.dgrb0 = b.vcd + NH;
 
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
         Geo g = tile_geo(p.W, p.H, -16 + (tile / p.ntx) * 96, -16 + (tile % p.ntx) * 96);
@@ -1194,25 +1216,24 @@ __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constan
         st_hpass(p, g, b);
         __syncthreads();
         NyqBox box = st_nyq_test(p, g, b, box_sh);
-        if (box.on) {
-            st_nyquist_area(p, g, b, box);
-            __syncthreads();
+        if (box.on) st_nyquist_area(p, g, b, box);
+        st_compact_vcd(p, g, b);
+        __syncthreads();
+        // the diagonal weight (needs only the mosaic) before the smoothing,
+        // so both weight wavefronts run at once, one warp each
+        st_diag_setup(p, g, b, whole_block());
+        __syncthreads();
+        st_diag_weight(p, g, b);
+        __syncthreads();
+        if ((threadIdx.x >> 5) == 0) {
+            wave_hvwt(p, g, b);
+        } else if ((threadIdx.x >> 5) == 1) {
+            wave_pmwt(p, g);
         }
-        // hvwt smoothing: one warp walks the rows (the others wait)
-        if ((threadIdx.x >> 5) == 0) wave_hvwt(p, g, b);
         __syncthreads();
         st_green_rb(p, g, b);
         __syncthreads();
         if (box.on) st_nyquist_green(p, g, b, box);
-        __syncthreads();
-        // diagonal stage, in the regions the H/V stage no longer needs
-        st_diag_setup(p, g, b, whole_block());
-        __syncthreads();
-        st_diag_weight(p, g, b, whole_block());
-        __syncthreads();
-        st_diag_rb(p, g, b, whole_block());
-        __syncthreads();
-        if ((threadIdx.x >> 5) == 0) wave_pmwt(p, g);
         __syncthreads();
         st_rbint(p, g, b);
         __syncthreads();
