@@ -228,51 +228,43 @@ __global__ void finish_kernel(const double* __restrict__ p1, int nb1, const doub
     }
 }
 
-// Transposed mirror-reflect 1-D convolution (adjoint of blur.rs's pass):
-// out[y] = sum_k w_k * sum_{x: refl(x+k-R) = y} in[x].  Requires n > R + 1
-// (then only single reflections occur).
-__global__ void blurT_rows_kernel(const float* __restrict__ in, float* __restrict__ out, int W, int H, const float* __restrict__ taps, int R) {
-    size_t n = (size_t)W * H;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
-        int y = (int)(p % W);
-        const float* row = in + (p - y);
-        float acc = 0.0f;
-        for (int k = 0; k <= 2 * R; k++) {
-            float wk = taps[k];
-            int x0 = y - k + R;
-            if (x0 >= 0 && x0 < W) acc = fmaf(wk, row[x0], acc);
-            if (y >= 1) {
-                int x1 = -y - k + R;
-                if (x1 >= 0 && x1 < W) acc = fmaf(wk, row[x1], acc);
-            }
-            if (y <= W - 2) {
-                int x2 = 2 * W - 2 - y - k + R;
-                if (x2 >= 0 && x2 < W) acc = fmaf(wk, row[x2], acc);
-            }
+// Transpose of the mirror-reflect blur pass (blur.rs:70-89) for symmetric
+// taps and a line length n > R + 1 (one reflection at most).  The blur reads
+// index -j as j; its transpose sends the weight meant for -j to j.  So the
+// transpose is the blur itself plus terms at the ends only: at distance
+// d (1 <= d <= R) from an end, + w[R - d] * g[end]; at the end itself,
+// - sum_{j=1..R} w[R - j] * g[end -+ j].  This kernel adds those terms to
+// `out`, which already holds the blur of g.  along_cols: the pass runs down
+// the columns (y), else along the rows (x).
+__global__ void blurT_edges_kernel(const float* __restrict__ g, float* __restrict__ out, int W, int H,
+                                   const float* __restrict__ taps, int R, int along_cols) {
+    const int n = along_cols ? H : W;   // length of a line
+    const int lines = along_cols ? W : H;
+    const size_t step = along_cols ? (size_t)W : 1;   // along a line
+    const size_t lstep = along_cols ? 1 : (size_t)W;  // between lines
+    const size_t total = (size_t)lines * (2 * R + 2);
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int line = (int)(t % lines), r = (int)(t / lines);
+        const int pos = r <= R ? r : n - 1 - (r - R - 1);
+        if (r > R && pos <= R) continue;  // the first-end thread of this position adds both ends' terms
+        const float* gl = g + line * lstep;
+        float d = 0.0f;
+        if (pos == 0) {
+            float acc = 0.0f;
+            for (int j = 1; j <= R; j++) acc = fmaf(taps[R - j], gl[j * step], acc);
+            d -= acc;
+        } else if (pos <= R) {
+            d = fmaf(taps[R - pos], gl[0], d);
         }
-        out[p] = acc;
-    }
-}
-
-__global__ void blurT_cols_kernel(const float* __restrict__ in, float* __restrict__ out, int W, int H, const float* __restrict__ taps, int R) {
-    size_t n = (size_t)W * H;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
-        int xcol = (int)(p % W), y = (int)(p / W);
-        float acc = 0.0f;
-        for (int k = 0; k <= 2 * R; k++) {
-            float wk = taps[k];
-            int y0 = y - k + R;
-            if (y0 >= 0 && y0 < H) acc = fmaf(wk, in[(size_t)y0 * W + xcol], acc);
-            if (y >= 1) {
-                int y1 = -y - k + R;
-                if (y1 >= 0 && y1 < H) acc = fmaf(wk, in[(size_t)y1 * W + xcol], acc);
-            }
-            if (y <= H - 2) {
-                int y2 = 2 * H - 2 - y - k + R;
-                if (y2 >= 0 && y2 < H) acc = fmaf(wk, in[(size_t)y2 * W + xcol], acc);
-            }
+        const int q = n - 1 - pos;
+        if (q == 0) {
+            float acc = 0.0f;
+            for (int j = 1; j <= R; j++) acc = fmaf(taps[R - j], gl[(size_t)(n - 1 - j) * step], acc);
+            d -= acc;
+        } else if (q <= R) {
+            d = fmaf(taps[R - q], gl[(size_t)(n - 1) * step], d);
         }
-        out[p] = acc;
+        out[line * lstep + pos * step] += d;
     }
 }
 
@@ -384,6 +376,7 @@ int build_const(const ImopsFilmGradParams& P, const ImopsBaselineFilm& F, Const*
 struct Bufs {
     Const* c;
     float *taps, *dtaps;
+    float htaps[2 * HAL_R + 1];  // host copy of the halation taps
     float *h, *t1, *B, *t2, *Bs, *gB, *t3, *gh, *ga;
     double *p1, *p2;
     int nb;
@@ -425,6 +418,7 @@ int prepare(const float* x, int W, int H, const ImopsFilmGradParams* P, const Im
     Const hc;
     std::vector<float> taps(2 * HAL_R + 1), dtaps(2 * HAL_R + 1);
     if ((rc = build_const(*P, Fd, &hc, taps.data(), dtaps.data()))) return rc;
+    for (int i = 0; i < 2 * HAL_R + 1; i++) b->htaps[i] = taps[i];
     IMOPS_CUDA_TRY(cudaMemcpyAsync(b->c, &hc, sizeof(Const), cudaMemcpyHostToDevice, s), "copy constants");
     IMOPS_CUDA_TRY(cudaMemcpyAsync(b->taps, taps.data(), taps.size() * 4, cudaMemcpyHostToDevice, s), "copy taps");
     IMOPS_CUDA_TRY(cudaMemcpyAsync(b->dtaps, dtaps.data(), dtaps.size() * 4, cudaMemcpyHostToDevice, s), "copy taps");
@@ -480,10 +474,15 @@ extern "C" int imops_param_backward(const float* cam_rgb, const float* g_out, co
     adj::pixel_kernel<1><<<b.nb, adj::BLK, 0, s>>>(cam_rgb, b.B, b.Bs, g_out, target, loss_scale, n, b.c, nullptr,
                                                    b.gB, b.ga, b.p1);
     note_launch();
-    // gh = rows^T(cols^T(gB)) with the same taps (the blur is rows then cols)
-    adj::blurT_cols_kernel<<<b.nb, adj::BLK, 0, s>>>(b.gB, b.t3, w, h, b.taps, R);
+    // gh = rows^T(cols^T(gB)) (the blur is rows then cols): each transposed
+    // pass is the tiled blur plus its end terms
+    if ((rc = film::blur_cols(b.gB, b.t3, w, h, b.htaps, R, 0, s))) return rc;
+    adj::blurT_edges_kernel<<<film::grid_for_n((size_t)w * (2 * R + 2)), adj::BLK, 0, s>>>(b.gB, b.t3, w, h, b.taps,
+                                                                                          R, 1);
     note_launch();
-    adj::blurT_rows_kernel<<<b.nb, adj::BLK, 0, s>>>(b.t3, b.gh, w, h, b.taps, R);
+    if ((rc = film::blur_rows(b.t3, b.gh, w, h, b.htaps, R, s))) return rc;
+    adj::blurT_edges_kernel<<<film::grid_for_n((size_t)h * (2 * R + 2)), adj::BLK, 0, s>>>(b.t3, b.gh, w, h, b.taps,
+                                                                                          R, 0);
     note_launch();
     adj::color_back_kernel<<<b.nb, adj::BLK, 0, s>>>(cam_rgb, b.ga, b.gh, n, b.c, b.p2);
     note_launch();
