@@ -98,6 +98,81 @@ __global__ void blur_cols_kernel(const float* __restrict__ in, int W, int H, Tap
     }
 }
 
+// Radius-64 specialisations (the baseline preset's halation and the adjoint):
+// the 129 taps are compile-time indexed parameter-bank operands and each
+// thread slides one window of loaded samples over several outputs, so the
+// loop is nearly all FMAs.  Every output still sums its taps in ascending
+// order: results are bit-identical to the generic kernels.
+constexpr int R64 = 64;
+constexpr int R64_ROW_OUT = 4;                      // outputs per thread
+constexpr int R64_ROW_THREADS = 256;
+constexpr int R64_ROW_TILE = R64_ROW_OUT * R64_ROW_THREADS;  // 1024 outputs per block
+
+__global__ void __launch_bounds__(R64_ROW_THREADS) blur_rows_r64_kernel(const float* __restrict__ in,
+                                                                       float* __restrict__ out, int W, int H, Taps tp) {
+    __shared__ __align__(16) float s[R64_ROW_TILE + 2 * R64];
+    const int y = blockIdx.y, x0 = blockIdx.x * R64_ROW_TILE;
+    const float* row = in + (size_t)y * W;
+    for (int j = threadIdx.x; j < R64_ROW_TILE + 2 * R64; j += blockDim.x)
+        s[j] = __ldg(row + reflect(x0 - R64 + j, W));
+    __syncthreads();
+    const int xb = R64_ROW_OUT * threadIdx.x;
+    float acc[R64_ROW_OUT];
+#pragma unroll
+    for (int j = 0; j < R64_ROW_OUT; j++) acc[j] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < (R64_ROW_OUT + 2 * R64) / 4; q++) {
+        const float4 v4 = *reinterpret_cast<const float4*>(s + xb + 4 * q);
+        const float v[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int j = 0; j < R64_ROW_OUT; j++) {
+                const int k = 4 * q + u - j;
+                if (k >= 0 && k <= 2 * R64) acc[j] = fmaf(v[u], tp.t[k], acc[j]);
+            }
+    }
+    float* o = out + (size_t)y * W;
+#pragma unroll
+    for (int j = 0; j < R64_ROW_OUT; j++)
+        if (x0 + xb + j < W) o[x0 + xb + j] = acc[j];
+}
+
+constexpr int R64_COL_TW = 32, R64_COL_GROUPS = 8, R64_COL_OUT = 16;  // 32x8 threads, 16 rows each
+constexpr int R64_COL_TH = R64_COL_GROUPS * R64_COL_OUT;              // 128 output rows per block
+
+template <class Epi>
+__global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) blur_cols_r64_kernel(const float* __restrict__ in,
+                                                                                     int W, int H, Taps tp, Epi epi) {
+    __shared__ float s[(R64_COL_TH + 2 * R64) * R64_COL_TW];
+    const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x = x0 + tx;
+    if (x < W)
+        for (int j = ty; j < R64_COL_TH + 2 * R64; j += R64_COL_GROUPS)
+            s[j * R64_COL_TW + tx] = __ldg(in + (size_t)reflect(y0 - R64 + j, H) * W + x);
+    __syncthreads();
+    if (x >= W) return;
+    const int rb = ty * R64_COL_OUT;
+    float acc[R64_COL_OUT];
+#pragma unroll
+    for (int j = 0; j < R64_COL_OUT; j++) acc[j] = 0.0f;
+#pragma unroll
+    for (int m = 0; m < R64_COL_OUT + 2 * R64; m++) {
+        const float v = s[(rb + m) * R64_COL_TW + tx];
+#pragma unroll
+        for (int j = 0; j < R64_COL_OUT; j++) {
+            const int k = m - j;
+            if (k >= 0 && k <= 2 * R64) acc[j] = fmaf(v, tp.t[k], acc[j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < R64_COL_OUT; j++) {
+        const int yy = y0 + rb + j;
+        if (yy < H) epi((size_t)yy * W + x, acc[j]);
+    }
+}
+
 struct EpiStore {
     float* out;
     __device__ __forceinline__ void operator()(size_t i, float v) const { out[i] = v; }
@@ -155,8 +230,13 @@ int blur_rows(const float* in, float* out, int W, int H, const float* taps, int 
     Taps tp;
     tp.R = R;
     for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
-    dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
-    blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(in, out, W, H, tp);
+    if (R == R64) {
+        dim3 rg((W + R64_ROW_TILE - 1) / R64_ROW_TILE, H);
+        blur_rows_r64_kernel<<<rg, R64_ROW_THREADS, 0, s>>>(in, out, W, H, tp);
+    } else {
+        dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
+        blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(in, out, W, H, tp);
+    }
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "blur rows");
     return IMOPS_OK;
@@ -167,9 +247,15 @@ int blur_cols(const float* in, float* out, int W, int H, const float* taps, int 
     Taps tp;
     tp.R = R;
     for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
-    dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
-    if (add) blur_cols_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiAdd{out});
-    else blur_cols_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiStore{out});
+    if (R == R64) {
+        dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + R64_COL_TH - 1) / R64_COL_TH);
+        if (add) blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiAdd{out});
+        else blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiStore{out});
+    } else {
+        dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
+        if (add) blur_cols_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiAdd{out});
+        else blur_cols_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiStore{out});
+    }
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "blur cols");
     return IMOPS_OK;

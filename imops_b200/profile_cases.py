@@ -2,6 +2,7 @@
 
   python -m imops_b200.profile_cases amaze --width 4096 --height 3072
   python -m imops_b200.profile_cases film81 --width 4096 --height 3072
+  python -m imops_b200.profile_cases fwdbwd --width 6048 --height 4024
 
 Each case builds a seeded synthetic input, runs the stage once and
 synchronises, so `ncu -k regex:<kernel> -c 1` captures exactly one launch.
@@ -15,7 +16,7 @@ import numpy as np
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["amaze", "film81", "develop"])
+    ap.add_argument("case", choices=["amaze", "film81", "develop", "fwdbwd"])
     ap.add_argument("--width", type=int, default=4096)
     ap.add_argument("--height", type=int, default=3072)
     a = ap.parse_args()
@@ -27,6 +28,22 @@ def main() -> None:
 
     W, H = a.width, a.height
     raw = torch.from_numpy(synthetic.mosaic_u16(H, W, seed=5).view(np.int16)).cuda()
+    if a.case == "fwdbwd":
+        # the differentiable model: AMaZE to camera RGB, forward, adjoint
+        # against a target rendered with perturbed parameters
+        p = im.DevelopParams()
+        p.demosaic, p.cfa, p.clip_pt, p.target, p.film = im.DEMOSAIC_AMAZE, b"RGGB", 1.0, im.CS_CAMERA, 0
+        for i in range(4):
+            p.wb[i] = 1.0
+        cam = im.develop_u16(raw, (0, 0, W, H), synthetic.BLACK, synthetic.WHITE, p)
+        target = im.param_forward(cam, im.FilmGradParams.from_vector(synthetic.film_grad_perturbed(2)))
+        theta = im.FilmGradParams.from_vector(synthetic.film_grad_base())
+        out = im.param_forward(cam, theta)
+        grad = torch.zeros(25, dtype=torch.float64, device=cam.device)
+        im.param_backward(cam, theta, grad, target=target, loss_scale=1.0 / (H * W * 3))
+        torch.cuda.synchronize()
+        print(f"{a.case} {W}x{H} ok, loss {float(grad[24]):.6e}")
+        return
     p = im.DevelopParams()
     p.demosaic, p.cfa, p.clip_pt = im.DEMOSAIC_AMAZE, b"RGGB", 1.0
     for i in range(4):
