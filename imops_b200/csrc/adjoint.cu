@@ -49,8 +49,8 @@ __device__ __forceinline__ void color_fwd(const Const& c, const float* x, float 
     for (int i = 0; i < 3; i++) a[i] = c.C[3 * i] * y[0] + c.C[3 * i + 1] * y[1] + c.C[3 * i + 2] * y[2];
 }
 
-__global__ void prep_kernel(const float* __restrict__ x, size_t n, const Const* __restrict__ cp, float* __restrict__ h) {
-    const Const& c = *cp;
+__global__ void prep_kernel(const float* __restrict__ x, size_t n, const __grid_constant__ Const c,
+                            float* __restrict__ h) {
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
         float y[3], a[3];
         color_fwd(c, x + 3 * p, y, a);
@@ -65,13 +65,9 @@ template <int MODE>
 __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x, const float* __restrict__ B,
                                                     const float* __restrict__ Bs, const float* __restrict__ g_out,
                                                     const float* __restrict__ target, float loss_scale, size_t n,
-                                                    const Const* __restrict__ cp, float* __restrict__ out,
+                                                    const __grid_constant__ Const c, float* __restrict__ out,
                                                     float* __restrict__ gB, float* __restrict__ ga,
                                                     double* __restrict__ partial) {
-    __shared__ Const c;
-    for (int k = threadIdx.x; k < (int)(sizeof(Const) / 4); k += blockDim.x)
-        reinterpret_cast<float*>(&c)[k] = reinterpret_cast<const float*>(cp)[k];
-    __syncthreads();
     // partials: dmax0-2 (0..2), k0-2 (3..5), x00-2 (6..8), s (9), sigma (10), loss (11)
     float acc[12];
     for (int i = 0; i < 12; i++) acc[i] = 0.0f;
@@ -90,7 +86,7 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
             D[l] = c.dmax[l] * sg[l];
         }
         float o0 = 0.f, o1 = 0.f, o2 = 0.f;
-#pragma unroll 9
+#pragma unroll
         for (int l = 0; l < NB81; l++) {
             float d = D[0] * c.eps[0][l];
             d = fmaf(D[1], c.eps[1][l], d);
@@ -121,7 +117,7 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
         // scan backward: gD_l = sum_lambda eps'_l (-ln2 T gT); T is recomputed
         // (same arithmetic as above) instead of kept per bin
         float gD0 = 0.f, gD1 = 0.f, gD2 = 0.f;
-#pragma unroll 9
+#pragma unroll
         for (int l = 0; l < NB81; l++) {
             float d = D[0] * c.eps[0][l];
             d = fmaf(D[1], c.eps[1][l], d);
@@ -171,12 +167,8 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
 // Colour backward: ga (+ the halation path through h) -> C, ev, wb partials.
 __global__ void __launch_bounds__(BLK) color_back_kernel(const float* __restrict__ x, const float* __restrict__ ga,
                                                          const float* __restrict__ gh, size_t n,
-                                                         const Const* __restrict__ cp,
+                                                         const __grid_constant__ Const c,
                                                          double* __restrict__ partial) {
-    __shared__ Const c;
-    for (int k = threadIdx.x; k < (int)(sizeof(Const) / 4); k += blockDim.x)
-        reinterpret_cast<float*>(&c)[k] = reinterpret_cast<const float*>(cp)[k];
-    __syncthreads();
     // wb0-2 (0..2), C00..C22 (3..11), ev (12)
     float acc[13];
     for (int i = 0; i < 13; i++) acc[i] = 0.0f;
@@ -374,7 +366,7 @@ int build_const(const ImopsFilmGradParams& P, const ImopsBaselineFilm& F, Const*
 }
 
 struct Bufs {
-    Const* c;
+    Const c;  // passed to the kernels by value
     float *taps, *dtaps;
     float htaps[2 * HAL_R + 1];  // host copy of the halation taps
     float *h, *t1, *B, *t2, *Bs, *gB, *t3, *gh, *ga;
@@ -393,13 +385,12 @@ int prepare(const float* x, int W, int H, const ImopsFilmGradParams* P, const Im
         return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "param film backward: image sides must exceed the halation radius + 1");
     const size_t n = (size_t)W * H;
     b->nb = film::grid_for_n(n);
-    size_t bytes = sizeof(Const) + 2 * (2 * HAL_R + 1) * 4 + (backward ? 12 : 3) * n * 4 +
+    size_t bytes = 2 * (2 * HAL_R + 1) * 4 + (backward ? 12 : 3) * n * 4 +
                    (size_t)b->nb * 25 * 8 + 8192;
     void* ws = nullptr;
     int rc = workspace(s, bytes, &ws);
     if (rc) return rc;
     Arena A{static_cast<char*>(ws), 0};
-    b->c = A.take<Const>(1);
     b->taps = A.take<float>(2 * HAL_R + 1);
     b->dtaps = A.take<float>(2 * HAL_R + 1);
     b->h = A.take<float>(n);
@@ -415,11 +406,9 @@ int prepare(const float* x, int W, int H, const ImopsFilmGradParams* P, const Im
         b->p1 = A.take<double>((size_t)b->nb * 12);
         b->p2 = A.take<double>((size_t)b->nb * 13);
     }
-    Const hc;
     std::vector<float> taps(2 * HAL_R + 1), dtaps(2 * HAL_R + 1);
-    if ((rc = build_const(*P, Fd, &hc, taps.data(), dtaps.data()))) return rc;
+    if ((rc = build_const(*P, Fd, &b->c, taps.data(), dtaps.data()))) return rc;
     for (int i = 0; i < 2 * HAL_R + 1; i++) b->htaps[i] = taps[i];
-    IMOPS_CUDA_TRY(cudaMemcpyAsync(b->c, &hc, sizeof(Const), cudaMemcpyHostToDevice, s), "copy constants");
     IMOPS_CUDA_TRY(cudaMemcpyAsync(b->taps, taps.data(), taps.size() * 4, cudaMemcpyHostToDevice, s), "copy taps");
     IMOPS_CUDA_TRY(cudaMemcpyAsync(b->dtaps, dtaps.data(), dtaps.size() * 4, cudaMemcpyHostToDevice, s), "copy taps");
     const int R = Fd.hal_radius;

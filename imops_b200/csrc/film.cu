@@ -462,19 +462,20 @@ struct Base81 {
     float taps[2 * HAL_R + 1];
 };
 
-__global__ void __launch_bounds__(256) scan81_fused_kernel(const float* __restrict__ a, const float* __restrict__ hr,
-                                                           const float* __restrict__ noise,
-                                                           const double* __restrict__ sumsq, int W, int H,
-                                                           const Base81* __restrict__ P, float* __restrict__ rgb) {
-    __shared__ float s[(COL_TH + 2 * HAL_R) * COL_TW];
-    __shared__ Base81 c;
-    for (int k = threadIdx.y * blockDim.x + threadIdx.x; k < (int)(sizeof(Base81) / 4); k += blockDim.x * blockDim.y)
-        reinterpret_cast<float*>(&c)[k] = reinterpret_cast<const float*>(P)[k];
-    int x0 = blockIdx.x * COL_TW, y0 = blockIdx.y * COL_TH;
-    int tx = threadIdx.x, ty = threadIdx.y, x = x0 + tx;
-    const int span = COL_TH + 2 * HAL_R;
+// One thread per 16 consecutive rows of a column: the halation column pass
+// (register sliding window, taps as parameter-bank operands, ascending tap
+// order as in blur_cols), then per pixel the logistic curves, grain and the
+// 81-bin scan with its tables as parameter-bank operands.
+__global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kernel(
+    const float* __restrict__ a, const float* __restrict__ hr, const float* __restrict__ noise,
+    const double* __restrict__ sumsq, int W, int H, const __grid_constant__ Base81 c, float* __restrict__ rgb) {
+    static_assert(HAL_R == R64, "the fused scan's column pass is the radius-64 window");
+    __shared__ float s[(R64_COL_TH + 2 * HAL_R) * R64_COL_TW];
+    const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
+    const int tx = threadIdx.x, ty = threadIdx.y, x = x0 + tx;
     if (x < W)
-        for (int j = ty; j < span; j += blockDim.y) s[j * COL_TW + tx] = __ldg(hr + (size_t)reflect(y0 - HAL_R + j, H) * W + x);
+        for (int j = ty; j < R64_COL_TH + 2 * HAL_R; j += R64_COL_GROUPS)
+            s[j * R64_COL_TW + tx] = __ldg(hr + (size_t)reflect(y0 - HAL_R + j, H) * W + x);
     __syncthreads();
     if (x >= W) return;
     const size_t n = (size_t)W * H;
@@ -484,12 +485,28 @@ __global__ void __launch_bounds__(256) scan81_fused_kernel(const float* __restri
             double var = sumsq[e] / (double)n;
             norm[e] = var > 1e-12 ? (float)(1.0 / sqrt(var)) : 1.0f;
         }
-    for (int r = 0; r < COL_RPT; r++) {
-        int ly = ty * COL_RPT + r, y = y0 + ly;
+    const int rb = ty * R64_COL_OUT;
+    float bs[R64_COL_OUT];
+#pragma unroll
+    for (int j = 0; j < R64_COL_OUT; j++) bs[j] = 0.0f;
+#pragma unroll
+    for (int m = 0; m < R64_COL_OUT + 2 * HAL_R; m++) {
+        const float v = s[(rb + m) * R64_COL_TW + tx];
+#pragma unroll
+        for (int j = 0; j < R64_COL_OUT; j++) {
+            const int k = m - j;
+            if (k >= 0 && k <= 2 * HAL_R) bs[j] = fmaf(v, c.taps[k], bs[j]);
+        }
+    }
+#pragma unroll 1
+    for (int j = 0; j < R64_COL_OUT; j++) {
+        const int y = y0 + rb + j;
         if (y >= H) break;
-        size_t p = (size_t)y * W + x;
-        float bsum = 0.0f;
-        for (int k = 0; k <= 2 * HAL_R; k++) bsum = fmaf(s[(ly + k) * COL_TW + tx], c.taps[k], bsum);
+        const size_t p = (size_t)y * W + x;
+        float bsum = bs[0];
+#pragma unroll
+        for (int q = 1; q < R64_COL_OUT; q++)
+            if (q == j) bsum = bs[q];
         float D[3];
         for (int e = 0; e < 3; e++) {
             float E = a[e * n + p] + c.B.hal_strength * c.B.bleed[e] * bsum;
@@ -498,7 +515,7 @@ __global__ void __launch_bounds__(256) scan81_fused_kernel(const float* __restri
             if (c.B.grain_sigma > 0.0f) D[e] += c.B.grain_sigma * noise[e * n + p] * norm[e];
         }
         float o0 = 0.f, o1 = 0.f, o2 = 0.f;
-#pragma unroll 9
+#pragma unroll
         for (int l = 0; l < NB81; l++) {
             float d = D[0] * c.S.eps[0][l];
             d = fmaf(D[1], c.S.eps[1][l], d);
@@ -701,11 +718,10 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
     int rc = build_stock(IMOPS_STOCK_BASELINE81, 0, W, -1.0f, &P, &st, &pitch);
     if (rc) return rc;
     const size_t n = (size_t)W * H;
-    size_t bytes = (3 + 1 + 1 + 3 + 1) * n * 4 + sizeof(Base81) + 4096;
+    size_t bytes = (3 + 1 + 1 + 3 + 1) * n * 4 + 4096;
     void* ws = nullptr;
     if ((rc = workspace(s, bytes, &ws))) return rc;
     Arena A{static_cast<char*>(ws), 0};
-    Base81* dP = A.take<Base81>(1);
     double* sums = A.take<double>(4);
     float* a = A.take<float>(3 * n);
     float* hal = A.take<float>(n);
@@ -716,18 +732,10 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
     hp.B = st.base;
     hp.S = st.scan81;
     for (int i = 0; i < 2 * HAL_R + 1; i++) hp.taps[i] = st.hal_taps[i];
-    IMOPS_CUDA_TRY(cudaMemcpyAsync(dP, &hp, sizeof(Base81), cudaMemcpyHostToDevice, s), "copy spec");
     int g = grid_for(n);
     expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
     note_launch();
-    {
-        Taps tp;
-        tp.R = HAL_R;
-        for (int i = 0; i < 2 * HAL_R + 1; i++) tp.t[i] = st.hal_taps[i];
-        dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
-        blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(hal, hr, W, H, tp);
-        note_launch();
-    }
+    if ((rc = blur_rows(hal, hr, W, H, st.hal_taps, HAL_R, s))) return rc;
     if (P.grain_on && P.grain_sigma != 0.0f) {
         Taps tp;
         if ((rc = taps_for(fmaxf(P.grain_blur, 1.0f), &tp))) return rc;
@@ -740,8 +748,8 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
             note_launch();
         }
     }
-    dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
-    scan81_fused_kernel<<<cg, cb, 0, s>>>(a, hr, noise, sums, W, H, dP, rgb);
+    dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + R64_COL_TH - 1) / R64_COL_TH);
+    scan81_fused_kernel<<<cg, cb, 0, s>>>(a, hr, noise, sums, W, H, hp, rgb);
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "baseline film kernels");
     return IMOPS_OK;
