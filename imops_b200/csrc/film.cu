@@ -203,22 +203,6 @@ struct EpiAdjacency {
         plane[i] = d + beta * (d - v);
     }
 };
-// Sum of squares of a plane into *out (f64), one atomic per block.
-__global__ void sumsq_kernel(const float* __restrict__ v, size_t n, double* __restrict__ out) {
-    __shared__ double sh[256];
-    double a = 0.0;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
-        double x = (double)v[p];
-        a += x * x;
-    }
-    sh[threadIdx.x] = a;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) atomicAdd(out, sh[0]);
-}
 
 struct EpiAdd {
     float* out;
@@ -340,22 +324,117 @@ __global__ void dir_apply_kernel(float* __restrict__ planes, const float* __rest
 // grain (grain.rs:20-100): SplitMix64 is counter based, so pixel x of row y
 // uses draws 12x+1..12x+12 of the row stream and is generated independently.
 
-__device__ __forceinline__ uint64_t splitmix_at(uint64_t s0, uint64_t k) {
-    uint64_t z = s0 + k * 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
+// The blurred grain field of one layer in one pass: Irwin-Hall noise over a
+// tile plus its halo (grain_noise_at), mirrored at the
+// image edge; the row then column passes of blur() in shared memory with the
+// same taps and summation order (so the field equals blur(noise) bit for
+// bit); the field written, and the block's sum of squares (f64) stored in
+// partial[plane][block] for the variance.  Plane z holds RNG layer
+// layer0 + z.  Radius <= GR_MAXR.
+constexpr int GR_TW = 64, GR_TH = 64, GR_MAXR = 16;
+
+// Noise of pixel (y, x) of a layer (grain.rs:20-45, 53-66): the sum of 12
+// uniforms minus 6, the uniforms being draws 12x+1 .. 12x+12 of the row's
+// SplitMix64 stream, seeded seed*0xD1B54A32D192ED03 + layer*0x9E3779B97F4A7C15 + y.
+__device__ __forceinline__ float grain_noise_at(uint64_t seed, int layer, int y, int x) {
+    const uint64_t golden = 0x9E3779B97F4A7C15ull;
+    // state of draw k is s0 + k * golden (mod 2^64): stepped, not multiplied
+    uint64_t z0 = seed * 0xD1B54A32D192ED03ull + (uint64_t)layer * golden + (uint64_t)y + 12 * (uint64_t)x * golden;
+    float acc = 0.0f;
+#pragma unroll
+    for (int k = 1; k <= 12; k++) {
+        z0 += golden;
+        uint64_t z = (z0 ^ (z0 >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        acc += __ull2float_rn(z ^ (z >> 31)) / 18446744073709551616.0f;
+    }
+    return acc - 6.0f;
 }
 
-__global__ void grain_noise_kernel(float* __restrict__ noise, int W, int H, uint64_t seed, int layer) {
-    size_t n = (size_t)W * H;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
-        uint64_t y = p / W, x = p % W;
-        uint64_t s0 = seed * 0xD1B54A32D192ED03ull + (uint64_t)layer * 0x9E3779B97F4A7C15ull + y;
-        float acc = 0.0f;
-        for (int k = 1; k <= 12; k++) acc += __ull2float_rn(splitmix_at(s0, 12 * x + k)) / 18446744073709551616.0f;
-        noise[p] = acc - 6.0f;
+__global__ void __launch_bounds__(256) grain_field_kernel(float* __restrict__ noise, int W, int H, uint64_t seed,
+                                                          int layer0, Taps tp, double* __restrict__ partial) {
+    extern __shared__ float gsm[];
+    __shared__ double red[8];
+    const int layer = layer0 + (int)blockIdx.z, R = tp.R;
+    const int x0 = blockIdx.x * GR_TW, y0 = blockIdx.y * GR_TH;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const int NW = GR_TW + 2 * R, NH = GR_TH + 2 * R;
+    const int GR_SW = NW;
+    float* sn = gsm;             // noise, tile + halo: NH x NW
+    float* sr = gsm + NH * NW;   // row-blurred: NH x GR_TW
+    // flat over the tile + halo so every lane draws (the halo row is not a
+    // multiple of the warp width)
+    for (int idx = tid; idx < NH * NW; idx += 256) {
+        const int r = idx / NW, c = idx - r * NW;
+        sn[idx] = grain_noise_at(seed, layer, reflect(y0 - R + r, H), reflect(x0 - R + c, W));
     }
+    __syncthreads();
+    for (int r = ty; r < NH; r += 8)
+        for (int c = tx; c < GR_TW; c += 32) {
+            float acc = 0.0f;
+            for (int k = 0; k <= 2 * R; k++) acc = fmaf(sn[r * GR_SW + c + k], tp.t[k], acc);
+            sr[r * GR_TW + c] = acc;
+        }
+    __syncthreads();
+    const size_t n = (size_t)W * H;
+    double sq = 0.0;
+    for (int r = ty; r < GR_TH; r += 8)
+        for (int c = tx; c < GR_TW; c += 32) {
+            const int y = y0 + r, x = x0 + c;
+            if (y >= H || x >= W) continue;
+            float acc = 0.0f;
+            for (int k = 0; k <= 2 * R; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
+            noise[blockIdx.z * n + (size_t)y * W + x] = acc;
+            sq += (double)acc * (double)acc;
+        }
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+    if (tx == 0) red[ty] = sq;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += red[w];
+        partial[(size_t)blockIdx.z * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// sums[layer] = sum of partial[layer][0 .. nb) in a fixed order (one block
+// per layer): deterministic run to run.
+__global__ void __launch_bounds__(1024) sum_partials_kernel(const double* __restrict__ partial, int nb,
+                                                            double* __restrict__ sums) {
+    __shared__ double red[1024];
+    const double* p = partial + (size_t)blockIdx.x * nb;
+    double a = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) a += p[i];
+    red[threadIdx.x] = a;
+    __syncthreads();
+    for (int w = 512; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = red[0];
+}
+
+// Blurred grain fields of RNG layers layer0 .. layer0+layers-1 (planes
+// noise[z * n]) and their sums of squares sums[z].  partial: scratch of
+// grain_partials(W, H, layers) doubles.
+size_t grain_partials(int W, int H, int layers) {
+    return (size_t)((W + GR_TW - 1) / GR_TW) * ((H + GR_TH - 1) / GR_TH) * layers;
+}
+
+int grain_fields(float* noise, int W, int H, uint64_t seed, int layer0, int layers, const Taps& tp, double* partial,
+                 double* sums, cudaStream_t s) {
+    if (tp.R > GR_MAXR) return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "film: grain blur radius above 16 px");
+    dim3 b(32, 8), g((W + GR_TW - 1) / GR_TW, (H + GR_TH - 1) / GR_TH, layers);
+    const int NW = GR_TW + 2 * tp.R, NH = GR_TH + 2 * tp.R;
+    const size_t smem = (size_t)NH * (NW + GR_TW) * sizeof(float);
+    IMOPS_CUDA_TRY(cudaFuncSetAttribute(grain_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                   "cudaFuncSetAttribute(grain)");
+    grain_field_kernel<<<g, b, smem, s>>>(noise, W, H, seed, layer0, tp, partial);
+    note_launch();
+    sum_partials_kernel<<<layers, 1024, 0, s>>>(partial, (int)(g.x * g.y), sums);
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "grain fields");
+    return IMOPS_OK;
 }
 
 // D <- clamp(D + kappa*taper*sqrt(D(Dmax-D))*n*norm, 0, 1.05 Dmax)
@@ -649,11 +728,9 @@ int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int 
         IMOPS_CUDA_TRY(cudaMemsetAsync(sums, 0, MAXE * sizeof(double), s), "memset");
         for (int e = 0; e < E; e++) {
             if (R.kappa[e] <= 0.0f || R.dmax[e] <= 0.0f) continue;
-            grain_noise_kernel<<<g, 256, 0, s>>>(inh, W, H, seed, e);
-            note_launch();
-            if ((rc = blur(inh, tmp, W, H, tp, EpiStore{noise}, s))) return rc;
-            sumsq_kernel<<<g, 256, 0, s>>>(noise, n, sums + e);
-            note_launch();
+            // the inhibition planes are free here: they hold the block sums
+            if ((rc = grain_fields(noise, W, H, seed, e, 1, tp, reinterpret_cast<double*>(inh), sums + e, s)))
+                return rc;
             grain_apply_kernel<<<g, 256, 0, s>>>(planes + e * n, noise, n, sums + e, R.kappa[e], R.dmax[e]);
             note_launch();
         }
@@ -718,7 +795,7 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
     int rc = build_stock(IMOPS_STOCK_BASELINE81, 0, W, -1.0f, &P, &st, &pitch);
     if (rc) return rc;
     const size_t n = (size_t)W * H;
-    size_t bytes = (3 + 1 + 1 + 3 + 1) * n * 4 + 4096;
+    size_t bytes = (3 + 1 + 1 + 3) * n * 4 + grain_partials(W, H, 3) * 8 + 4096;
     void* ws = nullptr;
     if ((rc = workspace(s, bytes, &ws))) return rc;
     Arena A{static_cast<char*>(ws), 0};
@@ -727,7 +804,7 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
     float* hal = A.take<float>(n);
     float* hr = A.take<float>(n);
     float* noise = A.take<float>(3 * n);
-    float* tmp = A.take<float>(n);
+    double* gpart = A.take<double>(grain_partials(W, H, 3));
     Base81 hp;
     hp.B = st.base;
     hp.S = st.scan81;
@@ -739,14 +816,7 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
     if (P.grain_on && P.grain_sigma != 0.0f) {
         Taps tp;
         if ((rc = taps_for(fmaxf(P.grain_blur, 1.0f), &tp))) return rc;
-        IMOPS_CUDA_TRY(cudaMemsetAsync(sums, 0, 4 * sizeof(double), s), "memset");
-        for (int e = 0; e < 3; e++) {
-            grain_noise_kernel<<<g, 256, 0, s>>>(tmp, W, H, P.seed, e);
-            note_launch();
-            if ((rc = blur(tmp, hal, W, H, tp, EpiStore{noise + e * n}, s))) return rc;
-            sumsq_kernel<<<g, 256, 0, s>>>(noise + e * n, n, sums + e);
-            note_launch();
-        }
+        if ((rc = grain_fields(noise, W, H, P.seed, 0, 3, tp, gpart, sums, s))) return rc;
     }
     dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + R64_COL_TH - 1) / R64_COL_TH);
     scan81_fused_kernel<<<cg, cb, 0, s>>>(a, hr, noise, sums, W, H, hp, rgb);
