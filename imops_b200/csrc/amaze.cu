@@ -482,42 +482,42 @@ __device__ void st_vpass(const P& p, const Geo& g, const Bufs& b, uint8_t* segma
     const int r0 = 4 + VSEGLEN * sg, r1 = min(r0 + VSEGLEN, rhi);
     const bool on = col_cd && r0 < r1;
     const float* m = b.mos;
-    constexpr int NK = VSEGLEN + 4;   // steps t = r0-2+k
-    constexpr int NM = NK + 8;        // mosaic rows r0-6+j
     unsigned run0 = 0, run1 = 0;
     int x00 = 0, x01 = 1, x10 = 0, x11 = 1;
     if (on) {
-        auto mrow = [&](int x, int dc) { return (x >= 0 && x < g.rr1) ? m[x * TS + c + dc] : 0.0f; };
-        float mc[NM];
+        auto mrow = [&](int x) { return (x >= 0 && x < g.rr1) ? m[x * TS + c] : 0.0f; };
+        // windows, for step t: mosaic rows t-4 .. t+4, dirwts rows t-2 .. t+2,
+        // and the last four rows' colour differences and candidates
+        float mw[9], wv[5];
 #pragma unroll
-        for (int j = 0; j < NM; j++) mc[j] = mrow(r0 - 6 + j, 0);
-        float wv[NM - 4];  // wv of row r0-4+j
+        for (int j = 0; j < 9; j++) mw[j] = mrow(r0 - 6 + j);
 #pragma unroll
-        for (int j = 0; j < NM - 4; j++) wv[j] = grad_w(mc[j], mc[j + 1], mc[j + 2], mc[j + 3], mc[j + 4]);
-        float raw[NK], alt[NK], dg[NK], vw[NK], A[NK], B[NK];
-#pragma unroll
-        for (int k = 0; k < NK; k++) {
+        for (int j = 0; j < 5; j++) wv[j] = grad_w(mw[j], mw[j + 1], mw[j + 2], mw[j + 3], mw[j + 4]);
+        float rawp[2] = {0.f, 0.f}, altp[4] = {0.f, 0.f, 0.f, 0.f}, dgp[4] = {0.f, 0.f, 0.f, 0.f};
+        float vwp[2] = {0.f, 0.f}, Ap[4] = {0.f, 0.f, 0.f, 0.f}, Bp[4] = {0.f, 0.f, 0.f, 0.f};
+        const int nk = r1 - r0 + 4;  // steps t = r0-2 .. r1+1
+#pragma unroll 1
+        for (int k = 0; k < nk; k++) {
             const int t = r0 - 2 + k;
-            raw[k] = alt[k] = dg[k] = vw[k] = A[k] = B[k] = 0.0f;
+            float raw = 0.f, alt = 0.f, dg = 0.f, vw = 0.f, A = 0.f, B = 0.f;
             if (t >= 4 && t < rhi) {
                 const bool gs = (p.cfa.at(g.top + t, g.left + c) & 1) != 0;
                 const float* rowp = m + t * TS + c;
-                const float h[7] = {rowp[-3], rowp[-2], rowp[-1], mc[k + 4], rowp[1], rowp[2], rowp[3]};
+                const float h[7] = {rowp[-3], rowp[-2], rowp[-1], mw[4], rowp[1], rowp[2], rowp[3]};
                 const float whm = grad_w(h[0], h[1], h[2], h[3], h[4]), whp = grad_w(h[2], h[3], h[4], h[5], h[6]);
                 const float nh[5] = {h[1], h[2], h[3], h[4], h[5]};
                 const float wh5[5] = {0.0f, whm, 0.0f, whp, 0.0f};
                 float hwt;
                 const float hha = dir_hha(nh, wh5, hwt);
-                const float nv[5] = {mc[k + 2], mc[k + 3], mc[k + 4], mc[k + 5], mc[k + 6]};
-                const float wv5[5] = {wv[k], wv[k + 1], wv[k + 2], wv[k + 3], wv[k + 4]};
-                dir_cd(nv, wv5, hha, gs, clip8, raw[k], alt[k], dg[k], vw[k]);
-                A[k] = cd_bound(alt[k], mc[k + 4], mc[k + 3], mc[k + 5], gs, p.clip);
-                B[k] = cd_bound(raw[k], mc[k + 4], mc[k + 3], mc[k + 5], gs, p.clip);
+                const float nv[5] = {mw[2], mw[3], mw[4], mw[5], mw[6]};
+                dir_cd(nv, wv, hha, gs, clip8, raw, alt, dg, vw);
+                A = cd_bound(alt, mw[4], mw[3], mw[5], gs, p.clip);
+                B = cd_bound(raw, mw[4], mw[3], mw[5], gs, p.clip);
             }
             const int u = t - 2;  // chain row of this step
-            if (k >= 4 && u < r1) {
+            if (k >= 4) {
                 const int ku = k - 4;
-                const int f = chain_map(var3(alt[k - 4], alt[k - 2], alt[k]), A[k - 4], B[k - 4], raw[k - 2], raw[k]);
+                const int f = chain_map(var3(altp[0], altp[2], alt), Ap[0], Bp[0], rawp[0], raw);
                 if (u & 1) {
                     x10 = map_at(f, x10);
                     x11 = map_at(f, x11);
@@ -530,14 +530,31 @@ __device__ void st_vpass(const P& p, const Geo& g, const Bufs& b, uint8_t* segma
                     run1 |= (unsigned)x01 << ku;
                 }
                 const int i = u * TS + c;
-                b.vcd[i] = A[k - 2];
-                b.hcd[i] = B[k - 2];
+                b.vcd[i] = Ap[2];
+                b.hcd[i] = Bp[2];
                 if (col_hv && u >= 6 && u < g.rr1 - 6 && (p.cfa.at(g.top + u, g.left + c) & 1) == 0) {
-                    const float vu1 = dg[k - 2] + dg[k - 3] + dg[k - 4];
-                    const float vd1 = dg[k - 2] + dg[k - 1] + dg[k];
-                    b.hvwt[i >> 1] = epssq + vw[k - 2] * vd1 + (1.0f - vw[k - 2]) * vu1;
+                    const float vu1 = dgp[2] + dgp[1] + dgp[0];
+                    const float vd1 = dgp[2] + dgp[3] + dg;
+                    b.hvwt[i >> 1] = epssq + vwp[0] * vd1 + (1.0f - vwp[0]) * vu1;
                 }
             }
+            // advance the windows by one row
+            rawp[0] = rawp[1]; rawp[1] = raw;
+            vwp[0] = vwp[1]; vwp[1] = vw;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                altp[j] = altp[j + 1];
+                dgp[j] = dgp[j + 1];
+                Ap[j] = Ap[j + 1];
+                Bp[j] = Bp[j + 1];
+            }
+            altp[3] = alt; dgp[3] = dg; Ap[3] = A; Bp[3] = B;
+#pragma unroll
+            for (int j = 0; j < 8; j++) mw[j] = mw[j + 1];
+            mw[8] = mrow(t + 5);
+#pragma unroll
+            for (int j = 0; j < 4; j++) wv[j] = wv[j + 1];
+            wv[4] = grad_w(mw[4], mw[5], mw[6], mw[7], mw[8]);
         }
     }
     segmap[(sg * TS + c) * 2] = (uint8_t)(x00 | (x01 << 1));
@@ -742,9 +759,9 @@ __device__ NyqBox st_nyq_test(const P& p, const Geo& g, const Bufs& b, int* sh) 
         for (int x = 0; x < 5; x++)
 #pragma unroll
             for (int y = 0; y < 5; y++) w[x][y] = gsq(ub - 2 + x, c - 2 + y);
-#pragma unroll
-        for (int n = 0; n < PER; n++) {
-            if (n0 + n < n1) {
+#pragma unroll 1
+        for (int n = 0; n < n1 - n0; n++) {
+            {
                 const int u = ub + 2 * n;
                 if (n > 0) {
 #pragma unroll
