@@ -474,7 +474,7 @@ __global__ void scan16_kernel(const float* __restrict__ img, const float* __rest
         for (int l = 0; l < NB16; l++) {
             float d = 0.0f;
             for (int e = 0; e < E; e++) d = fmaf(di[e], sc.eps[e][l], fmaf(dm[e], sc.meps[e][l], d));
-            float t = exp2f(-d);
+            float t = ex2_fast(-d);
             o0 = fmaf(sc.C[l][0], t, o0);
             o1 = fmaf(sc.C[l][1], t, o1);
             o2 = fmaf(sc.C[l][2], t, o2);
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
             float d = D[0] * c.S.eps[0][l];
             d = fmaf(D[1], c.S.eps[1][l], d);
             d = fmaf(D[2], c.S.eps[2][l], d);
-            float t = exp2f(-d);
+            float t = ex2_fast(-d);
             o0 = fmaf(c.S.C[l][0], t, o0);
             o1 = fmaf(c.S.C[l][1], t, o1);
             o2 = fmaf(c.S.C[l][2], t, o2);

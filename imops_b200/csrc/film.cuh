@@ -91,6 +91,16 @@ struct Stock {
     float grain_blur;               // baseline preset noise blur sigma (px)
 };
 
+// 2^x with the hardware approximation (PTX ex2.approx.ftz.f32: relative error
+// about 2^-22, subnormal results flushed).  The spectral scans raise 2 to
+// minus an optical density; with densities of a few units no result is
+// subnormal, and the film's tolerance is 1e-4.
+__device__ __forceinline__ float ex2_fast(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Builds the device description of stock `stock_id` for an image of width W
 // (pixel pitch = frame width / W, types.rs:45-48) and the given shutter.
 // Returns IMOPS_OK or an error code (unknown stock / format).
