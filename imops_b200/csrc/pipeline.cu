@@ -29,9 +29,14 @@ namespace pipe {
 
 // ---- device memory and stream ---------------------------------------------
 
+// Each image gets one of a few library-owned streams, round robin, so the
+// frames a host submits one after another can overlap on the GPU (one
+// frame's compute with the previous frame's download).
+constexpr int POOL_STREAMS = 3;
 struct DevState {
     bool init = false;
-    cudaStream_t stream = nullptr;
+    cudaStream_t streams[POOL_STREAMS] = {};
+    unsigned next = 0;
 };
 std::mutex g_dev_mu;
 DevState g_dev[128];
@@ -43,7 +48,8 @@ int device_stream(cudaStream_t* out) {
     std::lock_guard<std::mutex> lock(g_dev_mu);
     DevState& d = g_dev[dev];
     if (!d.init) {
-        IMOPS_CUDA_TRY(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (int i = 0; i < POOL_STREAMS; i++)
+            IMOPS_CUDA_TRY(cudaStreamCreateWithFlags(&d.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
         // keep freed image memory in the device pool so images can be
         // created and freed per frame without returning memory to the OS
         cudaMemPool_t pool;
@@ -53,7 +59,7 @@ int device_stream(cudaStream_t* out) {
         }
         d.init = true;
     }
-    *out = d.stream;
+    *out = d.streams[d.next++ % POOL_STREAMS];
     return IMOPS_OK;
 }
 
@@ -601,7 +607,8 @@ extern "C" ImopsImage* new_raw_image_u16_c(const uint16_t* raw, size_t width, si
         delete img;
         return nullptr;
     }
-    if (cudaMemcpyAsync(img->raw.p, raw, width * height * 2, cudaMemcpyHostToDevice, img->stream) != cudaSuccess) {
+    if (cudaMemcpyAsync(img->raw.p, raw, width * height * 2, cudaMemcpyHostToDevice, img->stream) != cudaSuccess ||
+        cudaStreamSynchronize(img->stream) != cudaSuccess) {
         fail(IMOPS_ERR_CUDA, "new_raw_image_u16_c: upload failed");
         pipe::buf_free(img->raw, img->stream);
         delete img;
@@ -628,7 +635,8 @@ extern "C" ImopsImage* new_raw_image_f32_c(const float* raw_data, size_t width, 
         return nullptr;
     }
     if (cudaMemcpyAsync(img->raw.p, raw_data, width * height * 4, cudaMemcpyHostToDevice, img->stream) !=
-        cudaSuccess) {
+            cudaSuccess ||
+        cudaStreamSynchronize(img->stream) != cudaSuccess) {
         fail(IMOPS_ERR_CUDA, "new_raw_image_f32_c: upload failed");
         pipe::buf_free(img->raw, img->stream);
         delete img;
@@ -658,7 +666,8 @@ extern "C" ImopsImage* new_rgb_image_c(const float* rgb, size_t width, size_t he
         delete img;
         return nullptr;
     }
-    if (cudaMemcpyAsync(img->rgb.p, rgb, width * height * 12, cudaMemcpyHostToDevice, img->stream) != cudaSuccess) {
+    if (cudaMemcpyAsync(img->rgb.p, rgb, width * height * 12, cudaMemcpyHostToDevice, img->stream) != cudaSuccess ||
+        cudaStreamSynchronize(img->stream) != cudaSuccess) {
         fail(IMOPS_ERR_CUDA, "new_rgb_image_c: upload failed");
         pipe::buf_free(img->rgb, img->stream);
         delete img;
@@ -732,7 +741,11 @@ extern "C" ImopsImage* run_pixel_pipeline_c(ImopsImage* image, ImopsPipeline* pi
         if (mods[k]->process(*image) != IMOPS_OK) return nullptr;
         k = fused_until;
     }
-    cudaError_t e = cudaStreamSynchronize(image->stream);
+    // Returns once the work is queued on the image's stream: every call that
+    // reads the image's pixels waits for it, so results are as if it had
+    // waited here, and frames submitted one after another overlap.  An error
+    // raised while the kernels run is reported by that reading call.
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         cuda_status(e, "run_pixel_pipeline_c");
         return nullptr;
