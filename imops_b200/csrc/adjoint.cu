@@ -42,6 +42,9 @@ struct Const {
     float bleed[3];
     float eps[3][NB81];
     float Cs[NB81][3];
+    // Q[l][e][c] = -ln2 eps[e][l] Cs[l][c]: dL/dD_e = sum_c go_c sum_l Q[l][e][c] T_l,
+    // so the backward needs only the forward's T_l, weighted before go is known
+    float Q[NB81][3][3];
 };
 
 __device__ __forceinline__ void color_fwd(const Const& c, const float* x, float y[3], float a[3]) {
@@ -86,6 +89,7 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
             D[l] = c.dmax[l] * sg[l];
         }
         float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+        float M[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
 #pragma unroll
         for (int l = 0; l < NB81; l++) {
             float d = D[0] * c.eps[0][l];
@@ -95,6 +99,12 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
             o0 = fmaf(c.Cs[l][0], t, o0);
             o1 = fmaf(c.Cs[l][1], t, o1);
             o2 = fmaf(c.Cs[l][2], t, o2);
+            if (MODE == 1) {
+#pragma unroll
+                for (int e = 0; e < 3; e++)
+#pragma unroll
+                    for (int j = 0; j < 3; j++) M[e][j] = fmaf(c.Q[l][e][j], t, M[e][j]);
+            }
         }
         if (MODE == 0) {
             out[3 * p] = o0;
@@ -114,21 +124,10 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
             go[1] = 2.0f * loss_scale * r1;
             go[2] = 2.0f * loss_scale * r2;
         }
-        // scan backward: gD_l = sum_lambda eps'_l (-ln2 T gT); T is recomputed
-        // (same arithmetic as above) instead of kept per bin
-        float gD0 = 0.f, gD1 = 0.f, gD2 = 0.f;
-#pragma unroll
-        for (int l = 0; l < NB81; l++) {
-            float d = D[0] * c.eps[0][l];
-            d = fmaf(D[1], c.eps[1][l], d);
-            d = fmaf(D[2], c.eps[2][l], d);
-            float t = exp2f(-d);
-            float gT = c.Cs[l][0] * go[0] + c.Cs[l][1] * go[1] + c.Cs[l][2] * go[2];
-            float gd = -0.69314718055994531f * t * gT;
-            gD0 = fmaf(c.eps[0][l], gd, gD0);
-            gD1 = fmaf(c.eps[1][l], gd, gD1);
-            gD2 = fmaf(c.eps[2][l], gd, gD2);
-        }
+        // scan backward: dL/dD_e = sum_c M[e][c] go_c (see Const::Q)
+        const float gD0 = M[0][0] * go[0] + M[0][1] * go[1] + M[0][2] * go[2];
+        const float gD1 = M[1][0] * go[0] + M[1][1] * go[1] + M[1][2] * go[2];
+        const float gD2 = M[2][0] * go[0] + M[2][1] * go[1] + M[2][2] * go[2];
         float gD[3] = {gD0, gD1, gD2};
         float gE[3];
         for (int l = 0; l < 3; l++) {
@@ -359,6 +358,10 @@ int build_const(const ImopsFilmGradParams& P, const ImopsBaselineFilm& F, Const*
         for (int i = 0; i < NB81; i++) c->eps[l][i] = st.scan81.eps[l][i];
     for (int i = 0; i < NB81; i++)
         for (int j = 0; j < 3; j++) c->Cs[i][j] = st.scan81.C[i][j];
+    for (int i = 0; i < NB81; i++)
+        for (int e = 0; e < 3; e++)
+            for (int j = 0; j < 3; j++)
+                c->Q[i][e][j] = (float)(-0.69314718055994531 * (double)st.scan81.eps[e][i] * (double)st.scan81.C[i][j]);
     if (F.hal_radius < 1 || F.hal_radius > HAL_R) return fail(IMOPS_ERR_INVALID_ARGUMENT, "hal_radius must be 1..64");
     if (!(P.hal_sigma > 0.0f)) return fail(IMOPS_ERR_INVALID_ARGUMENT, "hal_sigma must be > 0");
     halation_taps(P.hal_sigma, F.hal_radius, taps, dtaps);
