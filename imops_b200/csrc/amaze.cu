@@ -45,9 +45,9 @@ constexpr size_t SMEM_BYTES = (3 * (size_t)NF + (size_t)NH) * 4 + 64;
 //   mos  [NF]  the tile's mosaic
 //   HCD  [NF]  column pass: raw candidates | row pass: H0 cddiffsq, H1
 //              refined hcd at R/B sites | H0 vcd at R/B sites (after the
-//              Nyquist test) | H0 rbint, H1 final green
+//              Nyquist test), replaced in place by dgrb0 | H1 final green
 //   VCD  [NF]  alternative candidates, then the refined vcd | V0 dgrbsq1m,
-//              V1 dgrbsq1p | V0 pmwt, V1 dgrb0 | V0 dgrb1
+//              V1 dgrbsq1p | V0 pmwt, V1 rbint | V0 dgrb1
 //   hvwt [NH]  vvar1, then hvwt
 struct Bufs {
     float *mos, *hcd, *vcd, *hvwt;
@@ -867,6 +867,9 @@ template <class P>
 __device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
     for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
         const int i = rr * TS + cc;
+        // dgrb0 replaces vcd in place; the voted Nyquist sites keep vcd for
+        // st_nyquist_green, which stores their dgrb0
+        if (rbflag(b.nyq2w, i)) return;
         const float wt = b.hvwt[i >> 1];
         b.dgrb0[i >> 1] = wt * b.vcd_rb[i >> 1] + (1.0f - wt) * b.hcd_rb[i >> 1];
     });
@@ -874,8 +877,8 @@ __device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
 
 // demosaic.rs:978-998.  dgrb2h/v of a voted site j are
 // (rgbgreen_j - mean of its horizontal / vertical green neighbours)^2 with
-// rgbgreen_j = mos_j + dgrb0_j as st_green_rb left it, and zero at the other
-// sites.  New values are computed by all sites first and stored after a
+// rgbgreen_j = mos_j + the colour difference st_green_rb forms at j, and
+// zero at the other sites.  New values are computed by all sites first and stored after a
 // barrier, so every site reads the pre-update dgrb0.
 
 template <class P>
@@ -888,7 +891,10 @@ __device__ void st_nyquist_green(const P& p, const Geo& g, const Bufs& b, const 
             h = v = 0.0f;
             return;
         }
-        const float gr = m[j] + b.dgrb0[j >> 1];
+        // j is voted: its colour difference as st_green_rb forms it (not
+        // stored there for voted sites)
+        const float wt = b.hvwt[j >> 1];
+        const float gr = m[j] + (wt * b.vcd_rb[j >> 1] + (1.0f - wt) * b.hcd_rb[j >> 1]);
         h = sqr(gr - (m[j - 1] + m[j + 1]) * 0.5f);
         v = sqr(gr - (m[j - V1] + m[j + V1]) * 0.5f);
     };
@@ -993,20 +999,14 @@ __device__ void st_compact_vcd(const P& p, const Geo& g, const Bufs& b) {
     });
 }
 
-// demosaic.rs:1021-1107 (the diagonal R+B estimates rbm / rbp) and
-// :1119-1122 (rbint from them and the final pmwt).  rbm / rbp are only read
-// by rbint, so they are formed here, at the sites rbint needs.  delm / delp
-// of the R/B site j are |m[j+M1] - m[j-M1]| and |m[j-P1] - m[j+P1]| (the
-// reference stores them per column pair; the sign inside fabs does not
+// demosaic.rs:1021-1107: the diagonal R+B estimates rbm / rbp at R/B site i.
+// delm / delp of the R/B site j are |m[j+M1] - m[j-M1]| and |m[j-P1] - m[j+P1]|
+// (the reference stores them per column pair; the sign inside fabs does not
 // change the value).
-template <class P>
-__device__ void st_rbint(const P& p, const Geo& g, const Bufs& b) {
+__device__ __forceinline__ void diag_rb(const float* m, int i, float clip, float& rbm_out, float& rbp_out) {
     const float eps = 1e-5f, arth = 0.75f;
-    for_rb(p, g, 10, g.rr1 - 10, 10, g.cc1 - 10, [&](int rr, int cc) {
-        const int i = rr * TS + cc, h = i >> 1;
-        const float* m = b.mos;
-        auto dm = [&](int j) { return fabsf(m[j + M1] - m[j - M1]); };
-        auto dp = [&](int j) { return fabsf(m[j - P1] - m[j + P1]); };
+    auto dm = [&](int j) { return fabsf(m[j + M1] - m[j - M1]); };
+    auto dp = [&](int j) { return fabsf(m[j - P1] - m[j + P1]); };
         float crse = (m[i + M1] * 2.0f) / (eps + m[i] + m[i + M2]);
         float crnw = (m[i - M1] * 2.0f) / (eps + m[i] + m[i - M2]);
         float crne = (m[i - P1] * 2.0f) / (eps + m[i] + m[i - P2]);
@@ -1038,11 +1038,50 @@ __device__ void st_rbint(const P& p, const Geo& g, const Bufs& b) {
                 rbm = mw * rbm + (1.0f - mw) * ulim(rbm, m[i - M1], m[i + M1]);
             }
         }
-        if (rbp > p.clip) rbp = ulim(rbp, m[i - P1], m[i + P1]);
-        if (rbm > p.clip) rbm = ulim(rbm, m[i - M1], m[i + M1]);
-        const float pm = b.pmwt[h];
-        b.rbint[h] = (m[i] + rbm * (1.0f - pm) + rbp * pm) * 0.5f;
-    });
+        if (rbp > clip) rbp = ulim(rbp, m[i - P1], m[i + P1]);
+        if (rbm > clip) rbm = ulim(rbm, m[i - M1], m[i + M1]);
+    rbm_out = rbm;
+    rbp_out = rbp;
+}
+
+// rbm / rbp are read only by rbint (demosaic.rs:1119-1122), which needs the
+// final pmwt.  Warps 2.. form them for the R/B sites of [10, rr1-10) while
+// warps 0 and 1 run the weight wavefronts, keep them in registers, and form
+// rbint once the wavefronts are done.
+constexpr int RB_WORKERS = NTHREADS - 64;
+constexpr int RB_SLOTS = ((TS - 20) * TSH + RB_WORKERS - 1) / RB_WORKERS;
+
+template <class P>
+__device__ __forceinline__ bool rb_slot(const P& p, const Geo& g, int s, int& i) {
+    const int k = (int)threadIdx.x - 64 + s * RB_WORKERS;
+    if (k >= (g.rr1 - 20) * TSH) return false;
+    const int rr = 10 + (k >> 6);
+    const int cc = 10 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k & (TSH - 1));
+    if (cc >= g.cc1 - 10) return false;
+    i = rr * TS + cc;
+    return true;
+}
+
+template <class P>
+__device__ void st_rb_early(const P& p, const Geo& g, const Bufs& b, float (&rbm)[RB_SLOTS], float (&rbp)[RB_SLOTS]) {
+#pragma unroll
+    for (int s = 0; s < RB_SLOTS; s++) {
+        int i;
+        rbm[s] = rbp[s] = 0.0f;
+        if (rb_slot(p, g, s, i)) diag_rb(b.mos, i, p.clip, rbm[s], rbp[s]);
+    }
+}
+
+template <class P>
+__device__ void st_rbint_late(const P& p, const Geo& g, const Bufs& b, const float (&rbm)[RB_SLOTS],
+                              const float (&rbp)[RB_SLOTS]) {
+#pragma unroll
+    for (int s = 0; s < RB_SLOTS; s++) {
+        int i;
+        if (!rb_slot(p, g, s, i)) continue;
+        const float pm = b.pmwt[i >> 1];
+        b.rbint[i >> 1] = (b.mos[i] + rbm[s] * (1.0f - pm) + rbp[s] * pm) * 0.5f;
+    }
 }
 
 // demosaic.rs:1109-1118: pmwt smoothing (one warp); pmwt lives in the
@@ -1217,10 +1256,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constan
     b.hvwt = smem + 3 * NF;
     b.nyqw = rowbits;
     b.nyq2w = rowbits + TS;
-    b.cdd = b.vcd_rb = b.rbint = b.hcd;
+    b.cdd = b.vcd_rb = b.dgrb0 = b.hcd;
     b.hcd_rb = b.rg = b.hcd + NH;
     b.q1m = b.pmwt = b.dgrb1 = b.vcd;
-    b.q1p = b.dgrb0 = b.vcd + NH;
+    b.q1p = b.rbint = b.vcd + NH;
 
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
         Geo g = tile_geo(p.W, p.H, -16 + (tile / p.ntx) * 96, -16 + (tile % p.ntx) * 96);
@@ -1242,17 +1281,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constan
         __syncthreads();
         st_diag_weight(p, g, b);
         __syncthreads();
-        if ((threadIdx.x >> 5) == 0) {
-            wave_hvwt(p, g, b);
-        } else if ((threadIdx.x >> 5) == 1) {
-            wave_pmwt(p, g);
+        {
+            float rbm[RB_SLOTS], rbp[RB_SLOTS];
+            const int warp = threadIdx.x >> 5;
+            if (warp == 0) {
+                wave_hvwt(p, g, b);
+            } else if (warp == 1) {
+                wave_pmwt(p, g);
+            } else {
+                st_rb_early(p, g, b, rbm, rbp);
+            }
+            __syncthreads();
+            if (warp >= 2) st_rbint_late(p, g, b, rbm, rbp);
         }
-        __syncthreads();
         st_green_rb(p, g, b);
         __syncthreads();
         if (box.on) st_nyquist_green(p, g, b, box);
-        __syncthreads();
-        st_rbint(p, g, b);
         __syncthreads();
         st_green_refine(p, g, b);
         __syncthreads();
