@@ -183,7 +183,8 @@ def camera_cst(rgb, calib, target: int, stream=None):
 
 # ---- film -------------------------------------------------------------------
 
-STOCK_BWSTUB, STOCK_COLORNEG200, STOCK_BASELINE81 = 0, 1, 100
+STOCK_BWSTUB, STOCK_COLORNEG200, STOCK_PORTRA400, STOCK_EKTAR100, STOCK_FUJIPRO400H = 0, 1, 2, 3, 4
+STOCK_EKTACHROMEE100, STOCK_TRIX400, STOCK_BASELINE81 = 5, 6, 100
 FORMAT_35MM, FORMAT_6X6, FORMAT_4X5 = 0, 1, 2
 FILM_NEGATIVE_LINEAR, FILM_POSITIVE_LINEAR = 0, 1
 

@@ -8,7 +8,7 @@
 namespace imops {
 namespace film {
 
-constexpr int MAXE = 6;     // emulsion layers (Portra400 has 6)
+constexpr int MAXE = 8;     // emulsion layers (FujiPro400H has 7)
 constexpr int NB16 = 16;    // the reference grid, 400..700 nm step 20
 constexpr int NB81 = 81;    // the baseline preset grid, 380..780 nm step 5
 constexpr int LUTN = 64;    // DevelopableFractionLut entries (capture.rs:37-58)

@@ -75,103 +75,181 @@ struct StockDef {
     std::vector<double> scanner;
 };
 
-std::vector<double> gaussian16(double peak, double sigma, double amp) {
-    std::vector<double> s(NB16);
+// A stock as the reference's stock files list it: one row per EmulsionLayer,
+// in stack order (film/stock/ files).  Curves: 'g' gaussian_curve(a, b, c),
+// 'c' SpectralCurve::constant(a), 'p' panchromatic a + b * max(0, sin(pi t))
+// with t = (lambda - 400) / 300 (bw_stub.rs, trix_400.rs).
+struct LayerRow {
+    Kind kind;
+    float thick;
+    char sens;
+    double sa, sb, sc;
+    double mean_um, sig_ln;
+    float frac;
+    char eps;
+    double ea, eb, ec;
+    bool mask;
+    float dmax, gamma;
+    double k;
+    float p;
+};
+
+struct StockRow {
+    float box_iso;
+    double mask_b, mask_g, mask_0;  // orange mask: mask_b*blue + mask_g*green + mask_0
+    char refl;
+    double ra, rb, rc;
+    float psf_local, psf_halation, dev_diff, adj_beta, dir_diff;
+    bool reversal;
+    std::vector<LayerRow> layers;
+    std::vector<std::vector<float>> dir;
+};
+
+std::vector<double> curve16(char kind, double a, double b, double c) {
+    std::vector<double> s(NB16, 0.0);
     for (int i = 0; i < NB16; i++) {
-        double d = (lam16(i) - peak) / sigma;
-        s[i] = amp * std::exp(-0.5 * d * d);
+        if (kind == 'g') {
+            double d = (lam16(i) - a) / b;
+            s[i] = c * std::exp(-0.5 * d * d);
+        } else if (kind == 'c') {
+            s[i] = a;
+        } else if (kind == 'p') {
+            double t = (lam16(i) - 400.0) / 300.0;
+            double env = std::sin(PI * t);
+            if (env < 0.0) env = 0.0;
+            s[i] = a + b * env;
+        }
     }
     return s;
 }
 
-std::vector<double> orange_mask16() {
-    std::vector<double> s(NB16);
-    for (int i = 0; i < NB16; i++) {
-        double l = lam16(i), bd = (l - 450.0) / 50.0, gd = (l - 520.0) / 60.0;
-        s[i] = 0.35 * std::exp(-0.5 * (bd * bd)) + 0.25 * (0.6 * std::exp(-0.5 * (gd * gd))) * 1.0 + 0.05;
+StockDef from_rows(const StockRow& R) {
+    StockDef sd;
+    sd.box_iso = R.box_iso;
+    for (const LayerRow& r : R.layers) {
+        Layer l;
+        l.kind = r.kind;
+        l.thickness = r.thick;
+        l.sens = curve16(r.sens, r.sa, r.sb, r.sc);
+        l.gamma = r.gamma;
+        l.capture_k = r.k;
+        l.recip_p = r.p;
+        l.reversal = R.reversal;
+        if (r.kind == EMULSION) {
+            l.mu_ln = std::log(r.mean_um);
+            l.sigma_ln = r.sig_ln;
+            l.fraction = r.frac;
+            l.eps = curve16(r.eps, r.ea, r.eb, r.ec);
+            if (r.mask) {
+                l.mask_eps.resize(NB16);
+                for (int i = 0; i < NB16; i++) {
+                    double lm = lam16(i), bd = (lm - 450.0) / 50.0, gd = (lm - 520.0) / 60.0;
+                    double blue = std::exp(-0.5 * (bd * bd));
+                    double green = 0.6 * std::exp(-0.5 * (gd * gd));
+                    l.mask_eps[i] = R.mask_b * blue + R.mask_g * green + R.mask_0;
+                }
+            }
+            l.dmax = r.dmax;
+        }
+        sd.layers.push_back(l);
     }
-    return s;
+    sd.refl = curve16(R.refl, R.ra, R.rb, R.rc);
+    sd.psf_local = R.psf_local;
+    sd.psf_halation = R.psf_halation;
+    sd.dev_diff = R.dev_diff;
+    sd.adj_beta = R.adj_beta;
+    sd.dir_diff = R.dir_diff;
+    sd.dir = R.dir;
+    sd.scanner.assign(NB16, 1.0);
+    return sd;
 }
 
-Layer absorber(Kind k, float thick, std::vector<double> curve) {
-    Layer l;
-    l.kind = k;
-    l.thickness = thick;
-    l.sens = std::move(curve);
-    return l;
+constexpr LayerRow overcoat_row() { return {OVERCOAT, 1.0f, 'c', 0.01, 0, 0, 0, 0, 0.0f, 0, 0, 0, 0, false, 0.0f, 1.0f, 1.0, 1.0f}; }
+constexpr LayerRow absorber_row(Kind k, float thick, double a, double b, double c) {
+    return {k, thick, 'g', a, b, c, 0, 0, 0.0f, 0, 0, 0, 0, false, 0.0f, 1.0f, 1.0, 1.0f};
+}
+constexpr LayerRow emulsion_row(float thick, double sa, double sb, double sc, double mean, double sig, float frac,
+                                double ea, double eb, double ec, bool mask, float dmax, float gamma, double k, float p) {
+    return {EMULSION, thick, 'g', sa, sb, sc, mean, sig, frac, 'g', ea, eb, ec, mask, dmax, gamma, k, p};
 }
 
-Layer emulsion(float thick, double speak, double ssig, double mean_um, double sig_ln, double epeak, double esig,
-               float gamma, double k, float p) {
-    Layer l;
-    l.kind = EMULSION;
-    l.thickness = thick;
-    l.sens = gaussian16(speak, ssig, 1.0);
-    l.mu_ln = std::log(mean_um);
-    l.sigma_ln = sig_ln;
-    l.fraction = 0.18f;
-    l.eps = gaussian16(epeak, esig, 1.0);
-    l.mask_eps = orange_mask16();
-    l.dmax = 2.2f;
-    l.gamma = gamma;
-    l.capture_k = k;
-    l.recip_p = p;
-    return l;
-}
-
-// ColorNeg200 (film/stock/color_neg_200.rs:67-208)
-StockDef colorneg200() {
-    StockDef s;
-    s.box_iso = 200.0f;
-    s.layers.push_back(absorber(OVERCOAT, 1.0f, std::vector<double>(NB16, 0.01)));
-    s.layers.push_back(emulsion(4.0f, 450.0, 35.0, 0.55, 0.30, 450.0, 40.0, 0.65f, 4.2, 0.88f));
-    s.layers.push_back(absorber(FILTER, 2.0f, gaussian16(430.0, 40.0, 1.2)));
-    s.layers.push_back(emulsion(5.0f, 550.0, 40.0, 0.60, 0.32, 550.0, 40.0, 0.65f, 2.1, 0.90f));
-    s.layers.push_back(emulsion(6.0f, 650.0, 45.0, 0.70, 0.35, 650.0, 45.0, 0.65f, 1.35, 0.92f));
-    s.layers.push_back(absorber(ANTIHALATION, 2.0f, gaussian16(650.0, 80.0, 0.3)));
-    s.refl = gaussian16(680.0, 60.0, 0.08);
-    s.psf_local = 3.0f;
-    s.psf_halation = 80.0f;
-    s.dev_diff = 8.0f;
-    s.adj_beta = 0.35f;
-    s.dir_diff = 15.0f;
-    s.dir = {{0.02f, 0.05f, 0.03f}, {0.05f, 0.02f, 0.06f}, {0.03f, 0.06f, 0.02f}};
-    s.scanner.assign(NB16, 1.0);
-    return s;
-}
-
-// BwStub (film/stock/bw_stub.rs:18-82)
-StockDef bwstub() {
-    StockDef s;
-    s.box_iso = 100.0f;
-    Layer l;
-    l.kind = EMULSION;
-    l.thickness = 10.0f;
-    l.sens.resize(NB16);
-    for (int i = 0; i < NB16; i++) {
-        double t = (lam16(i) - 400.0) / 300.0;
-        double env = std::sin(PI * t);
-        if (env < 0.0) env = 0.0;
-        l.sens[i] = 0.3 + 0.7 * env;
+// The stocks, in StockId order (film/stock/mod.rs:126-147).
+StockRow stock_row(int id) {
+    switch (id) {
+    case 0:  // BwStub (film/stock/bw_stub.rs:18-82)
+        return StockRow{100.0f, 0.0, 0.0, 0.0, 'c', 0.0, 0.0, 0.0,
+                        2.0f, 40.0f, 5.0f, 0.3f, 10.0f, false,
+                        {LayerRow{EMULSION, 10.0f, 'p', 0.3, 0.7, 0, 0.7, 0.35, 0.2f, 'c', 1.0, 0, 0, false, 2.5f, 0.65f, 1.0, 1.0f}},
+                        {{0.0f}}};
+    case 1:  // ColorNeg200 (film/stock/color_neg_200.rs:67-208)
+        return StockRow{200.0f, 0.35, 0.25, 0.05, 'g', 680.0, 60.0, 0.08,
+                        3.0f, 80.0f, 8.0f, 0.35f, 15.0f, false,
+                        {overcoat_row(),
+                         emulsion_row(4.0f, 450.0, 35.0, 1.0, 0.55, 0.3, 0.18f, 450.0, 40.0, 1.0, true, 2.2f, 0.65f, 4.2, 0.88f),
+                         absorber_row(FILTER, 2.0f, 430.0, 40.0, 1.2),
+                         emulsion_row(5.0f, 550.0, 40.0, 1.0, 0.6, 0.32, 0.18f, 550.0, 40.0, 1.0, true, 2.2f, 0.65f, 2.1, 0.9f),
+                         emulsion_row(6.0f, 650.0, 45.0, 1.0, 0.7, 0.35, 0.18f, 650.0, 45.0, 1.0, true, 2.2f, 0.65f, 1.35, 0.92f),
+                         absorber_row(ANTIHALATION, 2.0f, 650.0, 80.0, 0.3)},
+                        {{0.02f, 0.05f, 0.03f}, {0.05f, 0.02f, 0.06f}, {0.03f, 0.06f, 0.02f}}};
+    case 2:  // Portra400 (film/stock/portra_400.rs:42-245)
+        return StockRow{400.0f, 0.32, 0.22, 0.04, 'g', 680.0, 60.0, 0.06,
+                        3.0f, 70.0f, 7.0f, 0.3f, 16.0f, false,
+                        {overcoat_row(),
+                         emulsion_row(2.5f, 450.0, 35.0, 1.0, 0.85, 0.35, 0.16f, 450.0, 40.0, 1.0, true, 1.1f, 0.54f, 4.8, 0.85f),
+                         emulsion_row(2.5f, 450.0, 35.0, 0.8, 0.42, 0.28, 0.2f, 450.0, 40.0, 1.0, true, 1.1f, 0.54f, 2.2, 0.89f),
+                         absorber_row(FILTER, 2.0f, 430.0, 40.0, 1.3),
+                         emulsion_row(3.0f, 550.0, 40.0, 1.0, 0.9, 0.35, 0.16f, 550.0, 40.0, 1.0, true, 1.1f, 0.54f, 2.4, 0.87f),
+                         emulsion_row(3.0f, 550.0, 40.0, 0.8, 0.45, 0.28, 0.2f, 550.0, 40.0, 1.0, true, 1.1f, 0.54f, 1.1, 0.91f),
+                         emulsion_row(3.5f, 650.0, 45.0, 1.0, 0.95, 0.35, 0.16f, 650.0, 45.0, 1.0, true, 1.1f, 0.54f, 1.5, 0.89f),
+                         emulsion_row(3.5f, 650.0, 45.0, 0.8, 0.48, 0.28, 0.2f, 650.0, 45.0, 1.0, true, 1.1f, 0.54f, 0.7, 0.93f),
+                         absorber_row(ANTIHALATION, 2.0f, 650.0, 80.0, 0.3)},
+                        {{0.02f, 0.01f, 0.04f, 0.02f, 0.03f, 0.01f}, {0.01f, 0.01f, 0.02f, 0.01f, 0.02f, 0.01f}, {0.04f, 0.02f, 0.02f, 0.01f, 0.05f, 0.02f}, {0.02f, 0.01f, 0.01f, 0.01f, 0.02f, 0.01f}, {0.03f, 0.01f, 0.05f, 0.02f, 0.02f, 0.01f}, {0.01f, 0.01f, 0.02f, 0.01f, 0.01f, 0.01f}}};
+    case 3:  // Ektar100 (film/stock/ektar_100.rs:46-270)
+        return StockRow{100.0f, 0.38, 0.26, 0.05, 'g', 680.0, 60.0, 0.05,
+                        2.5f, 55.0f, 6.0f, 0.55f, 14.0f, false,
+                        {overcoat_row(),
+                         emulsion_row(2.8f, 450.0, 32.0, 1.0, 0.82, 0.32, 0.17f, 450.0, 30.0, 1.25, true, 1.25f, 0.58f, 4.8, 0.86f),
+                         emulsion_row(2.5f, 450.0, 32.0, 0.85, 0.38, 0.24, 0.21f, 450.0, 30.0, 1.25, true, 1.9f, 0.34f, 6.5, 0.9f),
+                         absorber_row(FILTER, 2.0f, 430.0, 38.0, 1.35),
+                         emulsion_row(3.2f, 545.0, 36.0, 1.0, 0.88, 0.32, 0.17f, 545.0, 30.0, 1.25, true, 1.25f, 0.58f, 2.6, 0.88f),
+                         emulsion_row(3.0f, 545.0, 36.0, 0.85, 0.4, 0.24, 0.21f, 545.0, 30.0, 1.25, true, 1.9f, 0.34f, 3.6, 0.92f),
+                         emulsion_row(3.6f, 650.0, 40.0, 1.0, 0.92, 0.32, 0.17f, 650.0, 32.0, 1.25, true, 1.25f, 0.58f, 1.6, 0.9f),
+                         emulsion_row(3.5f, 650.0, 40.0, 0.85, 0.42, 0.24, 0.21f, 650.0, 32.0, 1.25, true, 1.9f, 0.34f, 2.4, 0.94f),
+                         absorber_row(ANTIHALATION, 2.0f, 650.0, 80.0, 0.25)},
+                        {{0.03f, 0.02f, 0.09f, 0.04f, 0.07f, 0.03f}, {0.02f, 0.02f, 0.04f, 0.02f, 0.04f, 0.02f}, {0.09f, 0.04f, 0.03f, 0.02f, 0.1f, 0.04f}, {0.04f, 0.02f, 0.02f, 0.02f, 0.04f, 0.02f}, {0.07f, 0.03f, 0.1f, 0.04f, 0.03f, 0.02f}, {0.03f, 0.02f, 0.04f, 0.02f, 0.02f, 0.02f}}};
+    case 4:  // FujiPro400H (film/stock/fuji_pro_400h.rs:43-271)
+        return StockRow{400.0f, 0.28, 0.2, 0.03, 'g', 670.0, 50.0, 0.05,
+                        2.5f, 65.0f, 6.5f, 0.32f, 14.0f, false,
+                        {overcoat_row(),
+                         emulsion_row(2.5f, 445.0, 35.0, 1.0, 0.82, 0.33, 0.17f, 445.0, 40.0, 1.0, true, 1.1f, 0.56f, 4.5, 0.86f),
+                         emulsion_row(2.5f, 445.0, 35.0, 0.8, 0.4, 0.28, 0.19f, 445.0, 40.0, 1.0, true, 1.1f, 0.56f, 2.1, 0.9f),
+                         absorber_row(FILTER, 2.0f, 430.0, 40.0, 1.3),
+                         emulsion_row(2.0f, 490.0, 30.0, 0.9, 0.5, 0.3, 0.15f, 650.0, 45.0, 0.6, true, 0.5f, 0.56f, 2.0, 0.88f),
+                         emulsion_row(3.0f, 545.0, 40.0, 1.0, 0.88, 0.34, 0.17f, 545.0, 40.0, 1.0, true, 1.1f, 0.56f, 2.3, 0.87f),
+                         emulsion_row(3.0f, 545.0, 40.0, 0.8, 0.44, 0.28, 0.19f, 545.0, 40.0, 1.0, true, 1.1f, 0.56f, 1.1, 0.91f),
+                         emulsion_row(3.5f, 650.0, 45.0, 1.0, 0.92, 0.34, 0.17f, 650.0, 45.0, 1.0, true, 1.1f, 0.56f, 1.4, 0.89f),
+                         emulsion_row(3.5f, 650.0, 45.0, 0.8, 0.46, 0.28, 0.19f, 650.0, 45.0, 1.0, true, 1.1f, 0.56f, 0.7, 0.93f),
+                         absorber_row(ANTIHALATION, 2.0f, 650.0, 80.0, 0.3)},
+                        {{0.02f, 0.01f, 0.03f, 0.04f, 0.02f, 0.03f, 0.01f}, {0.01f, 0.01f, 0.02f, 0.02f, 0.01f, 0.02f, 0.01f}, {0.03f, 0.02f, 0.02f, 0.06f, 0.03f, 0.04f, 0.02f}, {0.04f, 0.02f, 0.05f, 0.02f, 0.01f, 0.05f, 0.02f}, {0.02f, 0.01f, 0.02f, 0.01f, 0.01f, 0.02f, 0.01f}, {0.03f, 0.01f, 0.04f, 0.05f, 0.02f, 0.02f, 0.01f}, {0.01f, 0.01f, 0.02f, 0.02f, 0.01f, 0.01f, 0.01f}}};
+    case 5:  // EktachromeE100 (film/stock/ektachrome_e100.rs:28-157)
+        return StockRow{100.0f, 0.0, 0.0, 0.0, 'g', 660.0, 40.0, 0.02,
+                        1.5f, 40.0f, 4.0f, 0.4f, 8.0f, true,
+                        {overcoat_row(),
+                         emulsion_row(4.0f, 440.0, 30.0, 1.0, 0.42, 0.25, 0.22f, 440.0, 35.0, 1.0, false, 3.2f, 1.65f, 3.5, 0.93f),
+                         absorber_row(FILTER, 2.0f, 430.0, 35.0, 1.4),
+                         emulsion_row(4.0f, 545.0, 35.0, 1.0, 0.45, 0.25, 0.22f, 545.0, 35.0, 1.0, false, 3.2f, 1.65f, 1.8, 0.94f),
+                         emulsion_row(5.0f, 650.0, 40.0, 1.0, 0.5, 0.26, 0.22f, 650.0, 40.0, 1.0, false, 3.2f, 1.65f, 1.1, 0.95f),
+                         absorber_row(ANTIHALATION, 2.0f, 650.0, 80.0, 0.3)},
+                        {{0.01f, 0.02f, 0.01f}, {0.02f, 0.01f, 0.02f}, {0.01f, 0.02f, 0.01f}}};
+    case 6:  // TriX400 (film/stock/trix_400.rs:30-91)
+        return StockRow{400.0f, 0.0, 0.0, 0.0, 'c', 0.01, 0.0, 0.0,
+                        3.5f, 50.0f, 6.0f, 0.35f, 12.0f, false,
+                        {LayerRow{EMULSION, 6.0f, 'p', 0.35, 0.65, 0, 0.95, 0.38, 0.22f, 'c', 1.0, 0, 0, false, 1.5f, 0.70f, 2.2, 0.85f},
+                         LayerRow{EMULSION, 6.0f, 'p', 0.35, 0.65, 0, 0.45, 0.28, 0.24f, 'c', 1.0, 0, 0, false, 1.5f, 0.70f, 0.9, 0.89f}},
+                        {{0.03f, 0.02f}, {0.02f, 0.02f}}};
+    default:
+        return StockRow{};
     }
-    l.mu_ln = std::log(0.7);
-    l.sigma_ln = 0.35;
-    l.fraction = 0.2f;
-    l.eps.assign(NB16, 1.0);
-    l.dmax = 2.5f;
-    l.gamma = 0.65f;
-    l.capture_k = 1.0;
-    l.recip_p = 1.0f;
-    s.layers.push_back(l);
-    s.refl.assign(NB16, 0.0);
-    s.psf_local = 2.0f;
-    s.psf_halation = 40.0f;
-    s.dev_diff = 5.0f;
-    s.adj_beta = 0.3f;
-    s.dir_diff = 10.0f;
-    s.dir = {{0.0f}};
-    s.scanner.assign(NB16, 1.0);
-    return s;
 }
 
 double integrate_cmf16(const double* s, const double* cmf) {
@@ -289,7 +367,7 @@ int build_reference(const StockDef& sd, int W, float shutter, Stock* st, float* 
         }
     }
     const int E = (int)em.size();
-    if (E < 1 || E > MAXE) return fail(IMOPS_ERR_INVALID_STOCK, "stock must have 1..6 emulsion layers");
+    if (E < 1 || E > MAXE) return fail(IMOPS_ERR_INVALID_STOCK, "stock must have 1..8 emulsion layers");
     X.E = E;
     R.E = E;
     // band-mean weights: trapezoid over 20 nm, divided by the 300 nm span
@@ -566,10 +644,9 @@ int build_stock(int stock_id, int film_format, int W, float shutter_seconds, con
         return build_baseline(baseline ? *baseline : d, out);
     }
     if (film_format < 0 || film_format > 2) return fail(IMOPS_ERR_INVALID_ARGUMENT, "unknown film format");
-    StockDef sd;
-    if (stock_id == IMOPS_STOCK_COLORNEG200) sd = colorneg200();
-    else if (stock_id == IMOPS_STOCK_BWSTUB) sd = bwstub();
-    else return fail(IMOPS_ERR_INVALID_STOCK, "unknown or unsupported film stock id");
+    if (stock_id < IMOPS_STOCK_BWSTUB || stock_id > IMOPS_STOCK_TRIX400)
+        return fail(IMOPS_ERR_INVALID_STOCK, "unknown film stock id");
+    StockDef sd = from_rows(stock_row(stock_id));
     return build_reference(sd, W, shutter_seconds, out, pitch_um, frames[film_format]);
 }
 

@@ -535,10 +535,12 @@ std::unique_ptr<Module> create(const ModDef& d, const Value& table) {
         m->stock_name = st;
         if (st == "BwStub") m->p.stock = IMOPS_STOCK_BWSTUB;
         else if (st == "ColorNeg200") m->p.stock = IMOPS_STOCK_COLORNEG200;
+        else if (st == "Portra400") m->p.stock = IMOPS_STOCK_PORTRA400;
+        else if (st == "Ektar100") m->p.stock = IMOPS_STOCK_EKTAR100;
+        else if (st == "FujiPro400H") m->p.stock = IMOPS_STOCK_FUJIPRO400H;
+        else if (st == "EktachromeE100") m->p.stock = IMOPS_STOCK_EKTACHROMEE100;
+        else if (st == "TriX400") m->p.stock = IMOPS_STOCK_TRIX400;
         else if (st == "Baseline81") m->p.stock = IMOPS_STOCK_BASELINE81;
-        else if (st == "Portra400" || st == "Ektar100" || st == "FujiPro400H" || st == "EktachromeE100" ||
-                 st == "TriX400")
-            m->p.stock = -2;  // known to the reference, not ported yet
         else
             throw ParamError{"Unknown film stock: " + st};
         if (fm == "Film35mm") m->p.film_format = IMOPS_FORMAT_35MM;
@@ -727,13 +729,6 @@ extern "C" ImopsImage* run_pixel_pipeline_c(ImopsImage* image, ImopsPipeline* pi
     if (dev != image->dev) cudaSetDevice(image->dev);
     auto& mods = pipeline->modules;
     for (size_t k = 0; k < mods.size(); k++) {
-        auto* film = dynamic_cast<pipe::Film*>(mods[k].get());
-        if (film && film->p.stock == -2) {
-            fail(IMOPS_ERR_NOT_IMPLEMENTED,
-                 "film stock " + film->stock_name + " is not ported to the GPU path yet (BwStub, ColorNeg200, "
-                 "Baseline81 are)");
-            return nullptr;
-        }
         auto* dem = dynamic_cast<pipe::Demosaic*>(mods[k].get());
         size_t fused_until = k;
         if (dem && dem->algorithm == IMOPS_DEMOSAIC_AMAZE && image->raw_kind != 0 && !image->cfa.empty())

@@ -144,6 +144,11 @@ int imops_camera_cst(float *rgb, size_t n_pixels, const float calib_d65[9], int 
  * ImopsBaselineFilm). */
 #define IMOPS_STOCK_BWSTUB 0
 #define IMOPS_STOCK_COLORNEG200 1
+#define IMOPS_STOCK_PORTRA400 2
+#define IMOPS_STOCK_EKTAR100 3
+#define IMOPS_STOCK_FUJIPRO400H 4
+#define IMOPS_STOCK_EKTACHROMEE100 5
+#define IMOPS_STOCK_TRIX400 6
 #define IMOPS_STOCK_BASELINE81 100
 
 /* FilmFormat (film/types.rs:24-49). */

@@ -35,7 +35,7 @@
 #endif
 
 #define NB 16          /* reference grid: 400..700 nm step 20 */
-#define MAXL 8
+#define MAXL 12
 
 /* ----------------------------------------------------------------------- */
 /* constants (film/constants.rs:14-67, upsample.rs:17-45, pixel.rs:33-36)   */
@@ -259,107 +259,222 @@ static void finalize(OStock *S)
         }
 }
 
-static void absorber(OLayer *L, int kind, float thick, double peak, double sig, double amp)
-{
-    memset(L, 0, sizeof(*L));
-    L->kind = kind;
-    L->thickness = thick;
-    L->has_sens = 1;
-    gaussian_curve(peak, sig, amp, L->sens);
-    L->gamma = 1.0f;
-    L->capture_k = 1.0;
-    L->recip_p = 1.0f;
-}
+/* A stock as the reference's stock files list it: one row per EmulsionLayer
+ * (the film/stock/ files), in stack order.  Curves: 'g' gaussian_curve(a, b, c),
+ * 'c' SpectralCurve::constant(a), 'p' panchromatic a + b * max(0, sin(pi t))
+ * with t = (lambda - 400) / 300 (bw_stub.rs, trix_400.rs). */
+typedef struct {
+    int kind;
+    float thick;
+    char sens;
+    double sa, sb, sc;
+    double mean_um, sig_ln;
+    float frac;
+    char eps;
+    double ea, eb, ec;
+    int mask;
+    float dmax, gamma;
+    double k;
+    float p;
+} LayerRow;
 
-static void emulsion(OLayer *L, float thick, double speak, double ssig, double mean_um, double sig_ln, double epeak,
-                     double esig, float gamma, double k, float p)
-{
-    memset(L, 0, sizeof(*L));
-    L->kind = LK_EMULSION;
-    L->thickness = thick;
-    L->has_sens = 1;
-    gaussian_curve(speak, ssig, 1.0, L->sens);
-    L->mu_ln = log(mean_um);
-    L->sigma_ln = sig_ln;
-    L->fraction = 0.18f;
-    gaussian_curve(epeak, esig, 1.0, L->eps);
-    L->has_mask = 1;
-    orange_mask(L->mask_eps);
-    L->dmax = 2.2f;
-    L->gamma = gamma;
-    L->capture_k = k;
-    L->recip_p = p;
-}
+typedef struct {
+    float box_iso;
+    double mask_b, mask_g, mask_0; /* orange mask: mask_b*blue + mask_g*green + mask_0 */
+    char refl;
+    double ra, rb, rc;
+    float psf_local, psf_halation, dev_diff, adj_beta, dir_diff;
+    int reversal;
+    int nl;
+    LayerRow l[MAXL];
+    int dir_n;
+    float dir[MAXL][MAXL];
+} StockRow;
 
-/* ColorNeg200 (film/stock/color_neg_200.rs:67-208). */
-static void stock_colorneg200(OStock *S)
+static void row_curve(char kind, double a, double b, double c, double *s)
 {
-    memset(S, 0, sizeof(*S));
-    S->box_iso = 200.0f;
-    S->nl = 6;
-    absorber(&S->l[0], LK_OVERCOAT, 1.0f, 0, 1, 0);
-    for (int i = 0; i < NB; i++) S->l[0].sens[i] = 0.01;
-    emulsion(&S->l[1], 4.0f, 450.0, 35.0, 0.55, 0.30, 450.0, 40.0, 0.65f, 4.2, 0.88f);
-    absorber(&S->l[2], LK_FILTER, 2.0f, 430.0, 40.0, 1.2);
-    emulsion(&S->l[3], 5.0f, 550.0, 40.0, 0.60, 0.32, 550.0, 40.0, 0.65f, 2.1, 0.90f);
-    emulsion(&S->l[4], 6.0f, 650.0, 45.0, 0.70, 0.35, 650.0, 45.0, 0.65f, 1.35, 0.92f);
-    absorber(&S->l[5], LK_AH, 2.0f, 650.0, 80.0, 0.3);
-    gaussian_curve(680.0, 60.0, 0.08, S->refl);
-    S->psf_local = 3.0f;
-    S->psf_halation = 80.0f;
-    S->dev_diff = 8.0f;
-    S->adj_beta = 0.35f;
-    S->dir_diff = 15.0f;
-    S->dir_n = 3;
-    const float dm[3][3] = {{0.02f, 0.05f, 0.03f}, {0.05f, 0.02f, 0.06f}, {0.03f, 0.06f, 0.02f}};
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) S->dir[i][j] = dm[i][j];
-    for (int i = 0; i < NB; i++) S->scanner[i] = 1.0;
-    finalize(S);
-}
-
-/* BwStub (film/stock/bw_stub.rs:18-82). */
-static void stock_bwstub(OStock *S)
-{
-    memset(S, 0, sizeof(*S));
-    S->box_iso = 100.0f;
-    S->nl = 1;
-    OLayer *L = &S->l[0];
-    L->kind = LK_EMULSION;
-    L->thickness = 10.0f;
-    L->has_sens = 1;
     for (int i = 0; i < NB; i++) {
-        double t = (grid_nm(i) - 400.0) / 300.0;
-        double env = sin(3.14159265358979323846 * t);
-        if (env < 0.0) env = 0.0;
-        L->sens[i] = 0.3 + 0.7 * env;
-        L->eps[i] = 1.0;
+        if (kind == 'g') {
+            double d = (grid_nm(i) - a) / b;
+            s[i] = c * exp(-0.5 * d * d);
+        } else if (kind == 'c') {
+            s[i] = a;
+        } else if (kind == 'p') {
+            double t = (grid_nm(i) - 400.0) / 300.0;
+            double env = sin(3.14159265358979323846 * t);
+            if (env < 0.0) env = 0.0;
+            s[i] = a + b * env;
+        } else {
+            s[i] = 0.0;
+        }
     }
-    L->mu_ln = log(0.7);
-    L->sigma_ln = 0.35;
-    L->fraction = 0.2f;
-    L->has_mask = 0;
-    L->dmax = 2.5f;
-    L->gamma = 0.65f;
-    L->capture_k = 1.0;
-    L->recip_p = 1.0f;
-    for (int i = 0; i < NB; i++) S->refl[i] = 0.0;
-    S->psf_local = 2.0f;
-    S->psf_halation = 40.0f;
-    S->dev_diff = 5.0f;
-    S->adj_beta = 0.3f;
-    S->dir_diff = 10.0f;
-    S->dir_n = 1;
-    S->dir[0][0] = 0.0f;
+}
+
+static void build_from_rows(const StockRow *R, OStock *S)
+{
+    memset(S, 0, sizeof(*S));
+    S->box_iso = R->box_iso;
+    S->nl = R->nl;
+    for (int li = 0; li < R->nl; li++) {
+        const LayerRow *r = &R->l[li];
+        OLayer *L = &S->l[li];
+        L->kind = r->kind;
+        L->thickness = r->thick;
+        L->has_sens = r->sens != 0;
+        row_curve(r->sens, r->sa, r->sb, r->sc, L->sens);
+        L->gamma = r->gamma;
+        L->capture_k = r->k;
+        L->recip_p = r->p;
+        L->reversal = R->reversal;
+        if (r->kind != LK_EMULSION) continue;
+        L->mu_ln = log(r->mean_um);
+        L->sigma_ln = r->sig_ln;
+        L->fraction = r->frac;
+        row_curve(r->eps, r->ea, r->eb, r->ec, L->eps);
+        L->has_mask = r->mask;
+        if (r->mask)
+            for (int i = 0; i < NB; i++) {
+                double l = grid_nm(i);
+                double bd = (l - 450.0) / 50.0, gd = (l - 520.0) / 60.0;
+                double blue = exp(-0.5 * (bd * bd));
+                double green = 0.6 * exp(-0.5 * (gd * gd));
+                L->mask_eps[i] = R->mask_b * blue + R->mask_g * green + R->mask_0;
+            }
+        L->dmax = r->dmax;
+    }
+    row_curve(R->refl, R->ra, R->rb, R->rc, S->refl);
+    S->psf_local = R->psf_local;
+    S->psf_halation = R->psf_halation;
+    S->dev_diff = R->dev_diff;
+    S->adj_beta = R->adj_beta;
+    S->dir_diff = R->dir_diff;
+    S->dir_n = R->dir_n;
+    for (int i = 0; i < R->dir_n; i++)
+        for (int j = 0; j < R->dir_n; j++) S->dir[i][j] = R->dir[i][j];
     for (int i = 0; i < NB; i++) S->scanner[i] = 1.0;
     finalize(S);
 }
 
+#define OVERCOAT_ROW {LK_OVERCOAT, 1.0f, 'c', 0.01, 0, 0, 0, 0, 0.0f, 0, 0, 0, 0, 0, 0.0f, 1.0f, 1.0, 1.0f}
+#define ABSORBER_ROW(kind, thick, a, b, c) {kind, thick, 'g', a, b, c, 0, 0, 0.0f, 0, 0, 0, 0, 0, 0.0f, 1.0f, 1.0, 1.0f}
+#define EMULSION_ROW(thick, sa, sb, sc, mean, sig, frac, ea, eb, ec, mask, dmax, gamma, k, p) \
+    {LK_EMULSION, thick, 'g', sa, sb, sc, mean, sig, frac, 'g', ea, eb, ec, mask, dmax, gamma, k, p}
+
+/* ColorNeg200 (film/stock/color_neg_200.rs:67-208) */
+static const StockRow ROW_COLORNEG200 = {
+    200.0f, 0.35, 0.25, 0.05, 'g', 680.0, 60.0, 0.08,
+    3.0f, 80.0f, 8.0f, 0.35f, 15.0f, 0, 6,
+    {
+        OVERCOAT_ROW,
+        EMULSION_ROW(4.0f, 450.0, 35.0, 1.0, 0.55, 0.3, 0.18f, 450.0, 40.0, 1.0, 1, 2.2f, 0.65f, 4.2, 0.88f),
+        ABSORBER_ROW(LK_FILTER, 2.0f, 430.0, 40.0, 1.2),
+        EMULSION_ROW(5.0f, 550.0, 40.0, 1.0, 0.6, 0.32, 0.18f, 550.0, 40.0, 1.0, 1, 2.2f, 0.65f, 2.1, 0.9f),
+        EMULSION_ROW(6.0f, 650.0, 45.0, 1.0, 0.7, 0.35, 0.18f, 650.0, 45.0, 1.0, 1, 2.2f, 0.65f, 1.35, 0.92f),
+        ABSORBER_ROW(LK_AH, 2.0f, 650.0, 80.0, 0.3),
+    },
+    3,
+    {{0.02f, 0.05f, 0.03f}, {0.05f, 0.02f, 0.06f}, {0.03f, 0.06f, 0.02f}},
+};
+/* Portra400 (film/stock/portra_400.rs:42-245) */
+static const StockRow ROW_PORTRA400 = {
+    400.0f, 0.32, 0.22, 0.04, 'g', 680.0, 60.0, 0.06,
+    3.0f, 70.0f, 7.0f, 0.3f, 16.0f, 0, 9,
+    {
+        OVERCOAT_ROW,
+        EMULSION_ROW(2.5f, 450.0, 35.0, 1.0, 0.85, 0.35, 0.16f, 450.0, 40.0, 1.0, 1, 1.1f, 0.54f, 4.8, 0.85f),
+        EMULSION_ROW(2.5f, 450.0, 35.0, 0.8, 0.42, 0.28, 0.2f, 450.0, 40.0, 1.0, 1, 1.1f, 0.54f, 2.2, 0.89f),
+        ABSORBER_ROW(LK_FILTER, 2.0f, 430.0, 40.0, 1.3),
+        EMULSION_ROW(3.0f, 550.0, 40.0, 1.0, 0.9, 0.35, 0.16f, 550.0, 40.0, 1.0, 1, 1.1f, 0.54f, 2.4, 0.87f),
+        EMULSION_ROW(3.0f, 550.0, 40.0, 0.8, 0.45, 0.28, 0.2f, 550.0, 40.0, 1.0, 1, 1.1f, 0.54f, 1.1, 0.91f),
+        EMULSION_ROW(3.5f, 650.0, 45.0, 1.0, 0.95, 0.35, 0.16f, 650.0, 45.0, 1.0, 1, 1.1f, 0.54f, 1.5, 0.89f),
+        EMULSION_ROW(3.5f, 650.0, 45.0, 0.8, 0.48, 0.28, 0.2f, 650.0, 45.0, 1.0, 1, 1.1f, 0.54f, 0.7, 0.93f),
+        ABSORBER_ROW(LK_AH, 2.0f, 650.0, 80.0, 0.3),
+    },
+    6,
+    {{0.02f, 0.01f, 0.04f, 0.02f, 0.03f, 0.01f}, {0.01f, 0.01f, 0.02f, 0.01f, 0.02f, 0.01f}, {0.04f, 0.02f, 0.02f, 0.01f, 0.05f, 0.02f}, {0.02f, 0.01f, 0.01f, 0.01f, 0.02f, 0.01f}, {0.03f, 0.01f, 0.05f, 0.02f, 0.02f, 0.01f}, {0.01f, 0.01f, 0.02f, 0.01f, 0.01f, 0.01f}},
+};
+/* Ektar100 (film/stock/ektar_100.rs:46-270) */
+static const StockRow ROW_EKTAR100 = {
+    100.0f, 0.38, 0.26, 0.05, 'g', 680.0, 60.0, 0.05,
+    2.5f, 55.0f, 6.0f, 0.55f, 14.0f, 0, 9,
+    {
+        OVERCOAT_ROW,
+        EMULSION_ROW(2.8f, 450.0, 32.0, 1.0, 0.82, 0.32, 0.17f, 450.0, 30.0, 1.25, 1, 1.25f, 0.58f, 4.8, 0.86f),
+        EMULSION_ROW(2.5f, 450.0, 32.0, 0.85, 0.38, 0.24, 0.21f, 450.0, 30.0, 1.25, 1, 1.9f, 0.34f, 6.5, 0.9f),
+        ABSORBER_ROW(LK_FILTER, 2.0f, 430.0, 38.0, 1.35),
+        EMULSION_ROW(3.2f, 545.0, 36.0, 1.0, 0.88, 0.32, 0.17f, 545.0, 30.0, 1.25, 1, 1.25f, 0.58f, 2.6, 0.88f),
+        EMULSION_ROW(3.0f, 545.0, 36.0, 0.85, 0.4, 0.24, 0.21f, 545.0, 30.0, 1.25, 1, 1.9f, 0.34f, 3.6, 0.92f),
+        EMULSION_ROW(3.6f, 650.0, 40.0, 1.0, 0.92, 0.32, 0.17f, 650.0, 32.0, 1.25, 1, 1.25f, 0.58f, 1.6, 0.9f),
+        EMULSION_ROW(3.5f, 650.0, 40.0, 0.85, 0.42, 0.24, 0.21f, 650.0, 32.0, 1.25, 1, 1.9f, 0.34f, 2.4, 0.94f),
+        ABSORBER_ROW(LK_AH, 2.0f, 650.0, 80.0, 0.25),
+    },
+    6,
+    {{0.03f, 0.02f, 0.09f, 0.04f, 0.07f, 0.03f}, {0.02f, 0.02f, 0.04f, 0.02f, 0.04f, 0.02f}, {0.09f, 0.04f, 0.03f, 0.02f, 0.1f, 0.04f}, {0.04f, 0.02f, 0.02f, 0.02f, 0.04f, 0.02f}, {0.07f, 0.03f, 0.1f, 0.04f, 0.03f, 0.02f}, {0.03f, 0.02f, 0.04f, 0.02f, 0.02f, 0.02f}},
+};
+/* FujiPro400H (film/stock/fuji_pro_400h.rs:43-271) */
+static const StockRow ROW_FUJIPRO400H = {
+    400.0f, 0.28, 0.2, 0.03, 'g', 670.0, 50.0, 0.05,
+    2.5f, 65.0f, 6.5f, 0.32f, 14.0f, 0, 10,
+    {
+        OVERCOAT_ROW,
+        EMULSION_ROW(2.5f, 445.0, 35.0, 1.0, 0.82, 0.33, 0.17f, 445.0, 40.0, 1.0, 1, 1.1f, 0.56f, 4.5, 0.86f),
+        EMULSION_ROW(2.5f, 445.0, 35.0, 0.8, 0.4, 0.28, 0.19f, 445.0, 40.0, 1.0, 1, 1.1f, 0.56f, 2.1, 0.9f),
+        ABSORBER_ROW(LK_FILTER, 2.0f, 430.0, 40.0, 1.3),
+        EMULSION_ROW(2.0f, 490.0, 30.0, 0.9, 0.5, 0.3, 0.15f, 650.0, 45.0, 0.6, 1, 0.5f, 0.56f, 2.0, 0.88f),
+        EMULSION_ROW(3.0f, 545.0, 40.0, 1.0, 0.88, 0.34, 0.17f, 545.0, 40.0, 1.0, 1, 1.1f, 0.56f, 2.3, 0.87f),
+        EMULSION_ROW(3.0f, 545.0, 40.0, 0.8, 0.44, 0.28, 0.19f, 545.0, 40.0, 1.0, 1, 1.1f, 0.56f, 1.1, 0.91f),
+        EMULSION_ROW(3.5f, 650.0, 45.0, 1.0, 0.92, 0.34, 0.17f, 650.0, 45.0, 1.0, 1, 1.1f, 0.56f, 1.4, 0.89f),
+        EMULSION_ROW(3.5f, 650.0, 45.0, 0.8, 0.46, 0.28, 0.19f, 650.0, 45.0, 1.0, 1, 1.1f, 0.56f, 0.7, 0.93f),
+        ABSORBER_ROW(LK_AH, 2.0f, 650.0, 80.0, 0.3),
+    },
+    7,
+    {{0.02f, 0.01f, 0.03f, 0.04f, 0.02f, 0.03f, 0.01f}, {0.01f, 0.01f, 0.02f, 0.02f, 0.01f, 0.02f, 0.01f}, {0.03f, 0.02f, 0.02f, 0.06f, 0.03f, 0.04f, 0.02f}, {0.04f, 0.02f, 0.05f, 0.02f, 0.01f, 0.05f, 0.02f}, {0.02f, 0.01f, 0.02f, 0.01f, 0.01f, 0.02f, 0.01f}, {0.03f, 0.01f, 0.04f, 0.05f, 0.02f, 0.02f, 0.01f}, {0.01f, 0.01f, 0.02f, 0.02f, 0.01f, 0.01f, 0.01f}},
+};
+/* EktachromeE100 (film/stock/ektachrome_e100.rs:28-157) */
+static const StockRow ROW_EKTACHROMEE100 = {
+    100.0f, 0.0, 0.0, 0.0, 'g', 660.0, 40.0, 0.02,
+    1.5f, 40.0f, 4.0f, 0.4f, 8.0f, 1, 6,
+    {
+        OVERCOAT_ROW,
+        EMULSION_ROW(4.0f, 440.0, 30.0, 1.0, 0.42, 0.25, 0.22f, 440.0, 35.0, 1.0, 0, 3.2f, 1.65f, 3.5, 0.93f),
+        ABSORBER_ROW(LK_FILTER, 2.0f, 430.0, 35.0, 1.4),
+        EMULSION_ROW(4.0f, 545.0, 35.0, 1.0, 0.45, 0.25, 0.22f, 545.0, 35.0, 1.0, 0, 3.2f, 1.65f, 1.8, 0.94f),
+        EMULSION_ROW(5.0f, 650.0, 40.0, 1.0, 0.5, 0.26, 0.22f, 650.0, 40.0, 1.0, 0, 3.2f, 1.65f, 1.1, 0.95f),
+        ABSORBER_ROW(LK_AH, 2.0f, 650.0, 80.0, 0.3),
+    },
+    3,
+    {{0.01f, 0.02f, 0.01f}, {0.02f, 0.01f, 0.02f}, {0.01f, 0.02f, 0.01f}},
+};
+/* BwStub (film/stock/bw_stub.rs:18-82) */
+static const StockRow ROW_BWSTUB = {
+    100.0f, 0.0, 0.0, 0.0, 'c', 0.0, 0.0, 0.0,
+    2.0f, 40.0f, 5.0f, 0.3f, 10.0f, 0, 1,
+    {
+        {LK_EMULSION, 10.0f, 'p', 0.3, 0.7, 0, 0.7, 0.35, 0.2f, 'c', 1.0, 0, 0, 0, 2.5f, 0.65f, 1.0, 1.0f},
+    },
+    1,
+    {{0.0f}},
+};
+/* TriX400 (film/stock/trix_400.rs:30-91) */
+static const StockRow ROW_TRIX400 = {
+    400.0f, 0.0, 0.0, 0.0, 'c', 0.01, 0.0, 0.0,
+    3.5f, 50.0f, 6.0f, 0.35f, 12.0f, 0, 2,
+    {
+        {LK_EMULSION, 6.0f, 'p', 0.35, 0.65, 0, 0.95, 0.38, 0.22f, 'c', 1.0, 0, 0, 0, 1.5f, 0.70f, 2.2, 0.85f},
+        {LK_EMULSION, 6.0f, 'p', 0.35, 0.65, 0, 0.45, 0.28, 0.24f, 'c', 1.0, 0, 0, 0, 1.5f, 0.70f, 0.9, 0.89f},
+    },
+    2,
+    {{0.03f, 0.02f}, {0.02f, 0.02f}},
+};
+
+/* StockId order (film/stock/mod.rs:126-147). */
 static int load_stock(int id, OStock *S)
 {
-    if (id == 0) { stock_bwstub(S); return 1; }
-    if (id == 1) { stock_colorneg200(S); return 1; }
-    return 0;
+    static const StockRow *const rows[] = {&ROW_BWSTUB, &ROW_COLORNEG200, &ROW_PORTRA400, &ROW_EKTAR100,
+                                          &ROW_FUJIPRO400H, &ROW_EKTACHROMEE100, &ROW_TRIX400};
+    if (id < 0 || id > 6) return 0;
+    build_from_rows(rows[id], S);
+    return 1;
 }
 
 /* ----------------------------------------------------------------------- */

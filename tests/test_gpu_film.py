@@ -95,3 +95,27 @@ def test_baseline_preset_against_fp64_oracle(oracle_lib, gpu, grain_on):
     out = _run(gpu, x, stock=im.STOCK_BASELINE81, baseline=p)
     err = np.abs(out - ref)
     assert err.max() < TOL, f"max {err.max():.3g} rms {np.sqrt((err**2).mean()):.3g}"
+
+
+# Portra400, Ektar100, FujiPro400H (7 emulsions), EktachromeE100 (reversal),
+# TriX400 (two silver layers)
+OTHER_STOCKS = [2, 3, 4, 5, 6]
+
+
+@pytest.mark.parametrize("stock", OTHER_STOCKS)
+@pytest.mark.parametrize("grain,output", [(False, 0), (True, 0), (True, 1)])
+def test_other_stocks_strip_match_oracle(oracle_lib, gpu, stock, grain, output):
+    x = _abs_scene(32, 6048, seed=10 + stock)
+    ref = oracle_lib.film_process(x, stock=stock, seed=5, output=output, grain=grain, precision="f32")
+    out = _run(gpu, x, stock=stock, seed=5, output=output, grain=grain)
+    err = np.abs(out - ref)
+    assert np.isfinite(out).all()
+    assert err.max() < TOL, f"max {err.max():.3g} rms {np.sqrt((err**2).mean()):.3g}"
+
+
+@pytest.mark.parametrize("stock", OTHER_STOCKS)
+def test_other_stocks_small_frame(oracle_lib, gpu, stock):
+    x = _abs_scene(48, 64, seed=20 + stock)
+    ref = oracle_lib.film_process(x, stock=stock, seed=3, grain=True, precision="f32")
+    out = _run(gpu, x, stock=stock, seed=3, grain=True)
+    assert np.abs(out - ref).max() < TOL

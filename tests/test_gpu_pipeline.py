@@ -124,6 +124,24 @@ def test_pipeline_colorneg_film_matches_oracle(gpu, oracle_lib):
     assert np.abs(got - ref).max() < 1e-4
 
 
+@pytest.mark.parametrize("name,sid", [("Portra400", 2), ("Ektar100", 3), ("FujiPro400H", 4),
+                                      ("EktachromeE100", 5), ("TriX400", 6)])
+def test_pipeline_stock_names(gpu, oracle_lib, name, sid):
+    """modules.rs:846-853: the config's stock string selects the StockId."""
+    from imops_b200.pipeline import Image, parse_config, run_pixel_pipeline
+    rng = np.random.default_rng(40 + sid)
+    rel = (rng.random((32, 512, 3)) ** 2).astype(np.float32)
+    cfg = ('[[pipeline_modules]]\nname = "BaselineExposureCompensation"\n'
+           f'[[pipeline_modules]]\nname = "Film"\nstock = "{name}"\nfilm_format = "Film35mm"\nseed = 7\n'
+           'output = "PositiveLinear"\n')
+    img = Image.from_rgb(rel, 3, _meta(shutter=1 / 125, f_number=5.6, iso=400.0))
+    run_pixel_pipeline(img, parse_config(cfg))
+    got = img.rgb_f32()
+    x, _ = oracle_lib.baseline_exposure(rel, 0.0, 1 / 125, 5.6, 400.0)
+    ref = oracle_lib.film_process(x, stock=sid, seed=7, output=1, shutter=1 / 125)
+    assert np.abs(got - ref).max() < 1e-4
+
+
 def test_pipeline_u8_export(gpu):
     from imops_b200.pipeline import Image
     x = np.array([[[-0.5, 0.0, 0.25], [0.5, 0.999, 1.7]]], np.float32)

@@ -184,3 +184,40 @@ def test_baseline_preset_oracle_sane(oracle_lib):
     assert (hi < lo).all()
     x, y, z = oracle_lib.cmf81()
     assert abs(y.max() - 1.0) < 0.02 and 550 <= 380 + 5 * int(np.argmax(y)) <= 560
+
+
+# emulsion layers per StockId (film/stock/*: BwStub, ColorNeg200, Portra400,
+# Ektar100, FujiPro400H, EktachromeE100, TriX400)
+STOCK_EMULSIONS = {0: 1, 1: 3, 2: 6, 3: 6, 4: 7, 5: 3, 6: 2}
+
+
+def test_all_stocks_load_and_validate(oracle_lib):
+    # film/mod.rs:221-233: every stock loads; its emulsions have a finite
+    # grain kappa and a monotone capture LUT (capture.rs:113-130), and the
+    # normalised Dmin peaks at 1 (film/mod.rs:526-535)
+    for sid, ne in STOCK_EMULSIONS.items():
+        ks = [oracle_lib.layer_kappa(sid, e) for e in range(ne)]
+        assert all(np.isfinite(k) and k > 0 for k in ks), (sid, ks)
+        assert np.isnan(oracle_lib.layer_kappa(sid, ne))
+        for e in range(ne):
+            fs = [oracle_lib.lut_sample(sid, e, 10.0 ** lp) for lp in np.linspace(-4, 8, 25)]
+            assert all(b >= a - 1e-12 for a, b in zip(fs, fs[1:])), (sid, e)
+        d = oracle_lib.normalized_dmin(sid)
+        assert np.isfinite(d).all() and abs(d.max() - 1.0) < 1e-5, (sid, d)
+
+
+def test_colour_negatives_have_orange_dmin(oracle_lib):
+    # the orange mask of the masked negatives: R > G > B on the film base
+    for sid in (1, 2, 3, 4):
+        d = oracle_lib.normalized_dmin(sid)
+        assert d[0] > d[1] > d[2], (sid, d)
+
+
+def test_reversal_ektachrome_positive_slide(oracle_lib):
+    # film/mod.rs:509-521: the reversal stock on mid grey gives a finite
+    # positive (the output mode is ignored for reversal stocks)
+    g = 0.185 * 12.5 * 64.0
+    a = oracle_lib.film_process(np.full((16, 16, 3), g, np.float32), stock=5, seed=1, output=1)
+    b = oracle_lib.film_process(np.full((16, 16, 3), g, np.float32), stock=5, seed=1, output=0)
+    assert np.isfinite(a.reshape(-1, 3).mean(0)).all()
+    assert np.array_equal(a, b)
