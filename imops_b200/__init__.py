@@ -20,7 +20,7 @@ ERRORS = {
     6: "wrong color space", 7: "invalid dimensions", 8: "invalid stock", 9: "config error", 10: "not implemented",
     11: "timeout",
 }
-CS_CAMERA, CS_XYZD65, CS_LINEAR_SRGB, CS_SRGB, CS_ACESCG = -1, 0, 1, 2, 3
+CS_CAMERA, CS_XYZD65, CS_LINEAR_SRGB, CS_SRGB, CS_ACESCG, CS_OKLCH = -1, 0, 1, 2, 3, 4
 DEMOSAIC_AMAZE, DEMOSAIC_MARKESTEIJN, DEMOSAIC_FAST, DEMOSAIC_SUPERFAST, DEMOSAIC_SUPERSUPERFAST = range(5)
 
 
@@ -179,6 +179,43 @@ def camera_cst(rgb, calib, target: int, stream=None):
     f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
     check(f(_ptr(rgb), rgb.numel() // 3, c, target, _stream(stream)))
     return rgb
+
+
+# ---- display stages (one launch each; the pipeline fuses consecutive ones) ---
+
+def _pixel_call(name, rgb, argtypes, *args, stream=None):
+    _require_cuda_f32(rgb, "rgb")
+    f = getattr(lib(), name)
+    f.argtypes = [ctypes.c_void_p, ctypes.c_size_t] + argtypes + [ctypes.c_void_p]
+    check(f(_ptr(rgb), rgb.numel() // 3, *args, _stream(stream)))
+    return rgb
+
+
+def cst(rgb, source: int, target: int, stream=None):
+    """cst (cst.rs:6-10) between CS_XYZD65, CS_LINEAR_SRGB, CS_SRGB, CS_ACESCG and CS_OKLCH."""
+    return _pixel_call("imops_cst", rgb, [ctypes.c_int, ctypes.c_int], source, target, stream=stream)
+
+
+def highlight_reconstruction(rgb, wb, stream=None):
+    c = (ctypes.c_float * 4)(*(list(wb) + [0.0] * (4 - len(wb))))
+    return _pixel_call("imops_highlight_reconstruction", rgb, [ctypes.c_void_p], c, stream=stream)
+
+
+def contrast(rgb, value: float, stream=None):
+    return _pixel_call("imops_contrast", rgb, [ctypes.c_float], value, stream=stream)
+
+
+def gamma(rgb, g: float, stream=None):
+    return _pixel_call("imops_gamma", rgb, [ctypes.c_float], g, stream=stream)
+
+
+def lch(rgb, color_space: int, lc: float, cc: float, hc: float, stream=None):
+    return _pixel_call("imops_lch", rgb, [ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float],
+                       color_space, lc, cc, hc, stream=stream)
+
+
+def sigmoid_tone_map(rgb, stream=None):
+    return _pixel_call("imops_sigmoid_tone_map", rgb, [], stream=stream)
 
 
 # ---- film -------------------------------------------------------------------

@@ -5,12 +5,13 @@
 //
 // Module semantics follow modules.rs: Demosaic :629-668, CFACoeffs :529-557,
 // Exp :295-329, BaselineExposureCompensation :335-373, CST :576-592,
-// Film :841-876.  Where the reference panics (expect / panic!), the call
-// returns NULL / an error code and the same message is kept for
-// get_last_error_c.  Modules of the reference that are not part of this
-// path (BM3D, ChromaDenoise, LumaGuidedChromaDenoise, Vignette, LCH,
-// SigmoidToneMap, Gamma, Contrast, HighlightReconstruction) parse with the
-// reference's field rules and return IMOPS_ERR_NOT_IMPLEMENTED when run.
+// Film :841-876, LCH :221-261, HighlightReconstruction :265-293,
+// SigmoidToneMap :392-415, Gamma :417-453, Contrast :455-489.  Where the
+// reference panics (expect / panic!), the call returns NULL / an error code
+// and the same message is kept for get_last_error_c.  Modules of the
+// reference that are not part of this path (BM3D, ChromaDenoise,
+// LumaGuidedChromaDenoise, Vignette) parse with the reference's field rules
+// and return IMOPS_ERR_NOT_IMPLEMENTED when run.
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -23,6 +24,7 @@
 #include "amaze.cuh"
 #include "color.cuh"
 #include "config.hpp"
+#include "display.cuh"
 
 namespace imops {
 namespace pipe {
@@ -170,8 +172,9 @@ int cs_from_name(const std::string& name, int* cs, bool* known_elsewhere) {
     else if (name == "LinearSrgb") *cs = IMOPS_CS_LINEAR_SRGB;
     else if (name == "AcesCg") *cs = IMOPS_CS_ACESCG;
     else if (name == "XyzD65") *cs = IMOPS_CS_XYZD65;
+    else if (name == "Oklch") *cs = IMOPS_CS_OKLCH;
     else {
-        static const char* others[] = {"Lab", "Lch", "Hsl", "Hwb", "Oklab", "Oklch", "DisplayP3", "A98Rgb",
+        static const char* others[] = {"Lab", "Lch", "Hsl", "Hwb", "Oklab", "DisplayP3", "A98Rgb",
                                        "ProphotoRgb", "Rec2020", "Aces2065_1", "XyzD50"};
         for (const char* o : others)
             if (name == o) *known_elsewhere = true;
@@ -187,6 +190,7 @@ const char* cs_debug(const ImopsImage& img) {
         case IMOPS_CS_LINEAR_SRGB: return "Some(LinearSrgb)";
         case IMOPS_CS_ACESCG: return "Some(AcesCg)";
         case IMOPS_CS_XYZD65: return "Some(XyzD65)";
+        case IMOPS_CS_OKLCH: return "Some(Oklch)";
     }
     return "Some(?)";
 }
@@ -264,44 +268,65 @@ int need_rgb(const ImopsImage& img, const char* mod) {
     return IMOPS_OK;
 }
 
-struct CFACoeffs : Module {
+// A per-pixel module: appends its ops to a chain (display.cuh) and updates
+// the image's colour space.  run_pixel_pipeline_c runs each run of
+// consecutive per-pixel modules as one chain, one pass over the image; the
+// ops are each module's own f32 arithmetic in order, so the result is the
+// same as one pass per module.
+struct PixelModule : Module {
+    // most ops this module appends
+    virtual int max_ops() const { return 1; }
+    virtual int add_ops(ImopsImage& img, display::Chain& c) = 0;
     int process(ImopsImage& img) override {
+        display::Chain c{};
+        int rc = add_ops(img, c);
+        if (rc) return rc;
+        return display::run(static_cast<float*>(img.rgb.p), img.width * img.height, c, img.stream, "pixel modules");
+    }
+};
+
+struct CFACoeffs : PixelModule {
+    int add_ops(ImopsImage& img, display::Chain& c) override {
         int rc = need_rgb(img, "CFACoeffs");
         if (rc) return rc;
         if (!img.meta.has_wb)
             return fail(IMOPS_ERR_INVALID_ARGUMENT, "wb_coeffs needs to be set to perform highlight_reconstruction");
-        return imops_cfa_coeffs(static_cast<float*>(img.rgb.p), img.width * img.height, img.meta.wb_coeffs,
-                                img.stream);
+        return display::add_gain(c, img.meta.wb_coeffs[0], img.meta.wb_coeffs[1], img.meta.wb_coeffs[2]);
     }
 };
 
-struct Exp : Module {
+struct Exp : PixelModule {
     float ev = 0.0f;
-    int process(ImopsImage& img) override {
+    int add_ops(ImopsImage& img, display::Chain& c) override {
         int rc = need_rgb(img, "Exp");
         if (rc) return rc;
-        return imops_exp(static_cast<float*>(img.rgb.p), img.width * img.height, ev, img.stream);
+        float v = color::exp_value(ev);
+        return display::add_gain(c, v, v, v);
     }
 };
 
-struct BaselineExposureCompensation : Module {
-    int process(ImopsImage& img) override {
+struct BaselineExposureCompensation : PixelModule {
+    int max_ops() const override { return 2; }
+    int add_ops(ImopsImage& img, display::Chain& c) override {
         int rc = need_rgb(img, "BaselineExposureCompensation");
         if (rc) return rc;
         const ImopsImageMeta& m = img.meta;
         float ev = m.has_baseline_exposure ? m.baseline_exposure : 0.0f;
-        float t = m.has_shutter ? m.shutter_seconds : 0.0f;
-        float n = m.has_f_number ? m.f_number : 0.0f;
-        float iso = m.has_iso ? m.iso : 0.0f;
-        int applied = 0;
-        return imops_baseline_exposure(static_cast<float*>(img.rgb.p), img.width * img.height, ev, t, n, iso,
-                                       &applied, img.stream);
+        if (fabsf(ev) > 1e-6f) {
+            float v = color::exp_value(ev);
+            if ((rc = display::add_gain(c, v, v, v))) return rc;
+        }
+        bool ok = m.has_shutter && m.has_f_number && m.has_iso && m.shutter_seconds > 0.0f && m.f_number > 0.0f &&
+                  m.iso > 0.0f;
+        if (!ok) return IMOPS_OK;
+        float g = color::luminance_gain(m.shutter_seconds, m.f_number, m.iso);
+        return display::add_gain(c, g, g, g);
     }
 };
 
-struct CST : Module {
+struct CST : PixelModule {
     std::string target;
-    int process(ImopsImage& img) override {
+    int add_ops(ImopsImage& img, display::Chain& c) override {
         int rc = need_rgb(img, "CST");
         if (rc) return rc;
         std::string name = target;
@@ -311,30 +336,73 @@ struct CST : Module {
         bool elsewhere;
         if (!cs_from_name(name, &cs, &elsewhere)) {
             if (elsewhere)
-                return fail(IMOPS_ERR_NOT_IMPLEMENTED,
-                            "CST to " + name + " is not on the GPU path (Srgb, LinearSrgb, AcesCg, XyzD65 are)");
+                return fail(IMOPS_ERR_NOT_IMPLEMENTED, "CST to " + name +
+                                                           " is not on the GPU path (Srgb, LinearSrgb, AcesCg, "
+                                                           "XyzD65, Oklch are)");
             return fail(IMOPS_ERR_CONFIG, "Color space not recognized: " + target);
         }
-        float* rgb = static_cast<float*>(img.rgb.p);
-        size_t n = img.width * img.height;
         if (!img.has_cs) {
             if (!img.meta.has_calibration)
                 return fail(IMOPS_ERR_INVALID_ARGUMENT,
                             "A calibration matrix must be set to perform a camera cst transform");
-            rc = imops_camera_cst(rgb, n, img.meta.calibration_matrix_d65, cs, img.stream);
-        } else if (img.color_space != cs) {
-            color::Epilogue e = color::identity_epilogue();
-            color::to_xyz(img.color_space, e.fwd);
-            color::xyz_to_target(cs, e.tgt);
-            e.do_cst = 1;
-            e.src_srgb = img.color_space == IMOPS_CS_SRGB;
-            e.srgb = cs == IMOPS_CS_SRGB;
-            rc = color::run_epilogue(rgb, n, e, img.stream, "cst");
+            float fwd[9];
+            color::camera_forward_matrix(img.meta.calibration_matrix_d65, fwd);
+            rc = display::add_cst(c, IMOPS_CS_CAMERA, cs, fwd);
+        } else {
+            rc = display::add_cst(c, img.color_space, cs, nullptr);
         }
         if (rc) return rc;
         img.has_cs = true;
         img.color_space = cs;
         return IMOPS_OK;
+    }
+};
+
+struct HighlightReconstruction : PixelModule {
+    int add_ops(ImopsImage& img, display::Chain& c) override {
+        int rc = need_rgb(img, "HighlightReconstruction");
+        if (rc) return rc;
+        if (!img.meta.has_wb)
+            return fail(IMOPS_ERR_INVALID_ARGUMENT, "wb_coeffs needs to be set to perform highlight_reconstruction");
+        return display::add_highlight(c, img.meta.wb_coeffs[1]);
+    }
+};
+
+struct Contrast : PixelModule {
+    float value = 1.0f;
+    int add_ops(ImopsImage& img, display::Chain& c) override {
+        int rc = need_rgb(img, "Contrast");
+        if (rc) return rc;
+        return display::add_contrast(c, value);
+    }
+};
+
+struct LCH : PixelModule {
+    float lc = 1.0f, cc = 1.0f, hc = 1.0f;
+    int max_ops() const override { return 3; }
+    int add_ops(ImopsImage& img, display::Chain& c) override {
+        int rc = need_rgb(img, "LCH");
+        if (rc) return rc;
+        // Image::lch unwraps metadata.color_space (pixel.rs:60-68)
+        if (!img.has_cs) return fail(IMOPS_ERR_INVALID_ARGUMENT, "called `Option::unwrap()` on a `None` value");
+        return display::add_lch(c, img.color_space, lc, cc, hc);
+    }
+};
+
+struct SigmoidToneMap : PixelModule {
+    int add_ops(ImopsImage& img, display::Chain& c) override {
+        int rc = need_rgb(img, "SigmoidToneMap");
+        if (rc) return rc;
+        return display::add_sigmoid(c);
+    }
+};
+
+struct Gamma : PixelModule {
+    float gamma = 2.2f;
+    int add_ops(ImopsImage& img, display::Chain& c) override {
+        int rc = need_rgb(img, "Gamma");
+        if (rc) return rc;
+        return display::add_gamma(c, gamma);
     }
 };
 
@@ -454,7 +522,7 @@ const std::vector<ModDef>& registry() {
         {"Vignette", "Apply radial vignette correction.",
          {{"strength", "float", nullptr, 1.0, "Correction strength modifier.", {}}}, false},
         {"HighlightReconstruction", "Reconstruct clipped highlight details using white balance coefficients.", {},
-         false},
+         true},
         {"BaselineExposureCompensation",
          "Apply DNG BaselineExposure EV, then convert camera-relative linear values to absolute luminance using "
          "EXIF shutter/f-number/ISO (L = K\xc2\xb7v\xc2\xb7N\xc2\xb2/(t\xc2\xb7S)).",
@@ -462,7 +530,7 @@ const std::vector<ModDef>& registry() {
          true},
         {"Exp", "Apply manual exposure compensation in EV.",
          {{"ev", "float", nullptr, 0.0, "Exposure compensation value in EV.", {}}}, true},
-        {"Contrast", "Adjust image contrast.", {{"c", "float", nullptr, 1.0, "Contrast adjustment factor.", {}}}, false},
+        {"Contrast", "Adjust image contrast.", {{"c", "float", nullptr, 1.0, "Contrast adjustment factor.", {}}}, true},
         {"CST", "Perform Color Space Transform.",
          {{"target_color_space", "string", "", 0, "Target color space to convert to.",
            {"Srgb", "AcesCg", "Oklch", "XyzD65"}}},
@@ -485,12 +553,12 @@ const std::vector<ModDef>& registry() {
          {{"cc", "float", nullptr, 1.0, "Chroma (saturation) coefficient multiplier.", {}},
           {"hc", "float", nullptr, 1.0, "Hue coefficient multiplier.", {}},
           {"lc", "float", nullptr, 1.0, "Lightness coefficient multiplier.", {}}},
-         false},
-        {"SigmoidToneMap", "Sigmoid display tone map with ACES reference gamut compression (ACEScg).", {}, false},
+         true},
+        {"SigmoidToneMap", "Sigmoid display tone map with ACES reference gamut compression (ACEScg).", {}, true},
         {"Gamma",
          "Power-law display encode: out = linear^(1/\xce\xb3). Use \xce\xb3=2.2 for sRGB-like, \xce\xb3=2.4 for "
          "BT.1886. Apply after CST to a linear display space.",
-         {{"gamma", "float", nullptr, 2.2, "Display gamma (2.2 \xe2\x89\x88 sRGB, 2.4 = BT.1886).", {}}}, false},
+         {{"gamma", "float", nullptr, 2.2, "Display gamma (2.2 \xe2\x89\x88 sRGB, 2.4 = BT.1886).", {}}}, true},
         {"BM3D", "Apply BM3D image denoising.", {{"intensity", "float", nullptr, 0.0, "Denoising intensity factor.", {}}},
          false},
     };
@@ -553,6 +621,25 @@ std::unique_ptr<Module> create(const ModDef& d, const Value& table) {
         m->p.seed = (uint64_t)get_int(table, n, "seed", true);
         m->p.grain = 1;
         m->p.shutter_seconds = -1.0f;
+        return m;
+    }
+    if (n == "HighlightReconstruction") return std::make_unique<HighlightReconstruction>();
+    if (n == "SigmoidToneMap") return std::make_unique<SigmoidToneMap>();
+    if (n == "Contrast") {
+        auto m = std::make_unique<Contrast>();
+        m->value = get_f32(table, n, "c");
+        return m;
+    }
+    if (n == "Gamma") {
+        auto m = std::make_unique<Gamma>();
+        m->gamma = get_f32(table, n, "gamma");
+        return m;
+    }
+    if (n == "LCH") {
+        auto m = std::make_unique<LCH>();
+        m->lc = get_f32(table, n, "lc");
+        m->cc = get_f32(table, n, "cc");
+        m->hc = get_f32(table, n, "hc");
         return m;
     }
     auto m = std::make_unique<OffPath>();
@@ -729,6 +816,32 @@ extern "C" ImopsImage* run_pixel_pipeline_c(ImopsImage* image, ImopsPipeline* pi
     if (dev != image->dev) cudaSetDevice(image->dev);
     auto& mods = pipeline->modules;
     for (size_t k = 0; k < mods.size(); k++) {
+        if (dynamic_cast<pipe::PixelModule*>(mods[k].get())) {
+            // a run of per-pixel modules: one pass per display::MAX_OPS ops
+            display::Chain c{};
+            auto flush = [&]() {
+                int rc = display::run(static_cast<float*>(image->rgb.p), image->width * image->height, c,
+                                      image->stream, "pixel modules");
+                c.n = 0;
+                return rc;
+            };
+            size_t j = k;
+            for (; j < mods.size(); j++) {
+                auto* q = dynamic_cast<pipe::PixelModule*>(mods[j].get());
+                if (!q) break;
+                if (c.n + q->max_ops() > display::MAX_OPS && flush() != IMOPS_OK) return nullptr;
+                if (int rc = q->add_ops(*image, c)) {
+                    // the modules before this one have run, as in the reference
+                    std::string msg = last_error();
+                    flush();
+                    fail(rc, msg);
+                    return nullptr;
+                }
+            }
+            if (flush() != IMOPS_OK) return nullptr;
+            k = j - 1;
+            continue;
+        }
         auto* dem = dynamic_cast<pipe::Demosaic*>(mods[k].get());
         size_t fused_until = k;
         if (dem && dem->algorithm == IMOPS_DEMOSAIC_AMAZE && image->raw_kind != 0 && !image->cfa.empty())
@@ -867,7 +980,7 @@ extern "C" char* get_image_metadata_c(const ImopsImage* image) {
     Value cs;
     if (image->has_cs) {
         cs.kind = Value::STRING;
-        const char* names[] = {"XyzD65", "LinearSrgb", "Srgb", "AcesCg"};
+        const char* names[] = {"XyzD65", "LinearSrgb", "Srgb", "AcesCg", "Oklch"};
         cs.s = names[image->color_space];
     }
     root.t.emplace_back("color_space", cs);

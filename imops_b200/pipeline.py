@@ -13,10 +13,10 @@ import json
 
 import numpy as np
 
-from . import CS_ACESCG, CS_CAMERA, CS_LINEAR_SRGB, CS_SRGB, CS_XYZD65, ImopsError, last_error, lib
+from . import CS_ACESCG, CS_CAMERA, CS_LINEAR_SRGB, CS_OKLCH, CS_SRGB, CS_XYZD65, ImopsError, last_error, lib
 
 CS_NAMES = {CS_XYZD65: "XyzD65", CS_LINEAR_SRGB: "LinearSrgb", CS_SRGB: "Srgb", CS_ACESCG: "AcesCg",
-            CS_CAMERA: None}
+            CS_OKLCH: "Oklch", CS_CAMERA: None}
 
 
 class ImageMeta(ctypes.Structure):

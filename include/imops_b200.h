@@ -52,6 +52,7 @@ typedef void *imops_stream_t;
 #define IMOPS_CS_LINEAR_SRGB 1
 #define IMOPS_CS_SRGB 2
 #define IMOPS_CS_ACESCG 3
+#define IMOPS_CS_OKLCH 4                /* CSS Color 4 Oklch: L, C, hue in degrees [0, 360) */
 
 /* Demosaic algorithms: DemosaicAlgorithmType (pichromatic-pipeline/src/modules.rs:72-104). */
 #define IMOPS_DEMOSAIC_AMAZE 0
@@ -136,6 +137,35 @@ int imops_camera_forward_matrix(const float calib_d65[9], float forward[9]);
 /* camera_cst (cst.rs:12-48): xyz = forward * rgb, then XYZ(D65) -> target
  * (IMOPS_CS_*).  calib_d65: the 3x3 row-major calibration matrix. */
 int imops_camera_cst(float *rgb, size_t n_pixels, const float calib_d65[9], int target, imops_stream_t stream);
+
+/* ---- display stages and colour-space conversion ---------------------------
+ * Each runs in place over interleaved RGB.  The pipeline C-ABI fuses a run of
+ * consecutive per-pixel modules into one pass of the same ops.  Conversions
+ * involving Oklch restate the `color` crate 0.3.3 ColorSpaceTag::convert:
+ * Oklab (Ottosson 2020, linear-sRGB matrices), LCh per CSS Color 4. */
+
+/* cst (cst.rs:6-10): source -> target between IMOPS_CS_XYZD65, _LINEAR_SRGB,
+ * _SRGB, _ACESCG and _OKLCH (camera RGB goes through imops_camera_cst). */
+int imops_cst(float *rgb, size_t n_pixels, int source, int target, imops_stream_t stream);
+
+/* highlight_reconstruction (highlight_reconstruction.rs:5-13):
+ * f = g / wb[1]; g = (1 - f) g + f (r + b) / 2. */
+int imops_highlight_reconstruction(float *rgb, size_t n_pixels, const float wb[4], imops_stream_t stream);
+
+/* contrast (contrast.rs:4-8): x = 0.185 (x / 0.185)^value per channel. */
+int imops_contrast(float *rgb, size_t n_pixels, float value, imops_stream_t stream);
+
+/* gamma_encode (tone_map.rs:38-49): x <= 0 ? 0 : x^(1 / max(gamma, 1e-6)). */
+int imops_gamma(float *rgb, size_t n_pixels, float gamma, imops_stream_t stream);
+
+/* lch (lch.rs:5-18): to Oklch from color_space, (L, C, h) *= (lc, cc, hc),
+ * back.  IMOPS_CS_CAMERA is rejected (the reference unwraps None). */
+int imops_lch(float *rgb, size_t n_pixels, int color_space, float lc, float cc, float hc, imops_stream_t stream);
+
+/* sigmoid (tone_map.rs:18-33) on ACEScg: ACES reference gamut compression
+ * (default RgcParams, :59-69), square_sigmoid per channel, chroma scaled by
+ * 1 - Y^5 in Oklch with the hue of the compressed pixel. */
+int imops_sigmoid_tone_map(float *rgb, size_t n_pixels, imops_stream_t stream);
 
 /* ---- spectral film simulation ------------------------------------------- */
 

@@ -27,7 +27,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 _lib = None
 
-CS_XYZD65, CS_LINEAR_SRGB, CS_SRGB, CS_ACESCG = 0, 1, 2, 3
+CS_XYZD65, CS_LINEAR_SRGB, CS_SRGB, CS_ACESCG, CS_OKLCH = 0, 1, 2, 3, 4
 STOCK_BWSTUB, STOCK_COLORNEG200 = 0, 1
 ERR_NAMES = {0: "ok", 1: "invalid argument", 2: "unsupported CFA", 3: "unsupported size"}
 
@@ -216,6 +216,55 @@ def camera_cst(rgb: np.ndarray, calib, target: int, precision: str = "f32"):
     fn.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int]
     _check(fn(_ptr(out), out.size // 3, _ptr(c), target), "camera_cst")
     return out
+
+
+def _rgb_op(name, rgb, precision, argtypes, *args, check=False):
+    dt = _dt(precision)
+    out = np.ascontiguousarray(rgb, dtype=dt).copy()
+    fn = _f(name, precision)
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_size_t] + argtypes
+    rc = fn(_ptr(out), out.size // 3, *args)
+    if check:
+        _check(rc, name)
+    return out
+
+
+def _real(precision):
+    return ctypes.c_float if precision == "f32" else ctypes.c_double
+
+
+def cst_space(rgb: np.ndarray, src: int, dst: int, precision: str = "f32"):
+    """cst (cst.rs:6-10) between XyzD65, LinearSrgb, Srgb, AcesCg and Oklch."""
+    return _rgb_op("oracle_cst_space", rgb, precision, [ctypes.c_int, ctypes.c_int], src, dst, check=True)
+
+
+def highlight(rgb: np.ndarray, wb, precision: str = "f32"):
+    """highlight_reconstruction (highlight_reconstruction.rs:5-13); clip_g = wb[1]."""
+    return _rgb_op("oracle_highlight", rgb, precision, [_real(precision)], float(wb[1]))
+
+
+def contrast(rgb: np.ndarray, c: float, precision: str = "f32"):
+    return _rgb_op("oracle_contrast", rgb, precision, [_real(precision)], c)
+
+
+def gamma(rgb: np.ndarray, g: float, precision: str = "f32"):
+    return _rgb_op("oracle_gamma", rgb, precision, [_real(precision)], g)
+
+
+def lch(rgb: np.ndarray, cs: int, lc: float, cc: float, hc: float, precision: str = "f32"):
+    r = _real(precision)
+    return _rgb_op("oracle_lch", rgb, precision, [ctypes.c_int, r, r, r], cs, lc, cc, hc, check=True)
+
+
+def sigmoid(rgb: np.ndarray, precision: str = "f32"):
+    return _rgb_op("oracle_sigmoid", rgb, precision, [])
+
+
+def square_sigmoid(x: float, precision: str = "f32") -> float:
+    fn = _f("oracle_square_sigmoid", precision)
+    fn.argtypes = [_real(precision)]
+    fn.restype = _real(precision)
+    return fn(x)
 
 
 def blur(plane: np.ndarray, sigma: float, precision: str = "f32"):

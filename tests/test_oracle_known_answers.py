@@ -221,3 +221,60 @@ def test_reversal_ektachrome_positive_slide(oracle_lib):
     b = oracle_lib.film_process(np.full((16, 16, 3), g, np.float32), stock=5, seed=1, output=0)
     assert np.isfinite(a.reshape(-1, 3).mean(0)).all()
     assert np.array_equal(a, b)
+
+
+# ---- display stages -----------------------------------------------------------
+
+def test_highlight_reconstruction_known_answer(oracle_lib):
+    # highlight_reconstruction.rs:19-31
+    out = oracle_lib.highlight(np.array([[0.6, 0.4, 0.8]], np.float32), [1.0, 1.0, 1.0, 1.0])
+    assert abs(out[0, 0] - 0.6) < 1e-6 and abs(out[0, 1] - 0.52) < 1e-6 and abs(out[0, 2] - 0.8) < 1e-6
+
+
+def test_square_sigmoid_gray_preservation(oracle_lib):
+    # tone_map.rs:176-186
+    assert abs(oracle_lib.square_sigmoid(0.18) - 0.18) < 1e-5
+
+
+def test_gamma_22_roundtrip_mid(oracle_lib):
+    # tone_map.rs:188-195
+    e = oracle_lib.gamma(np.full((1, 3), 0.18, np.float32), 2.2)[0, 0]
+    assert abs(np.float32(e) ** np.float32(2.2) - 0.18) < 1e-5
+
+
+def test_lch_roundtrip_identity(oracle_lib):
+    # lch.rs:24-36
+    out = oracle_lib.lch(np.array([[0.4, 0.7, 0.2]], np.float32), oracle_lib.CS_SRGB, 1.0, 1.0, 1.0)
+    assert np.abs(out - [0.4, 0.7, 0.2]).max() < 1e-4
+
+
+def test_oklab_published_values(oracle_lib):
+    # Ottosson (2020), "A perceptual color space for image processing": XYZ
+    # (D65) -> Oklab table, three decimals
+    xyz = np.array([[0.950, 1.000, 1.089], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float64)
+    lab = np.array([[1.000, 0.000, 0.000], [0.450, 1.236, -0.019], [0.922, -0.671, 0.263],
+                    [0.153, -1.415, -0.449]])
+    lch = oracle_lib.cst_space(xyz, oracle_lib.CS_XYZD65, oracle_lib.CS_OKLCH, precision="f64")
+    h = np.radians(lch[:, 2])
+    got = np.stack([lch[:, 0], lch[:, 1] * np.cos(h), lch[:, 1] * np.sin(h)], axis=1)
+    assert np.abs(got - lab).max() < 1.5e-3
+    assert ((lch[:, 2] >= 0) & (lch[:, 2] < 360)).all()
+
+
+def test_oklch_roundtrips(oracle_lib):
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-0.2, 2.0, (2000, 3))
+    for cs in (oracle_lib.CS_ACESCG, oracle_lib.CS_SRGB, oracle_lib.CS_LINEAR_SRGB, oracle_lib.CS_XYZD65):
+        back = oracle_lib.cst_space(oracle_lib.cst_space(x, cs, oracle_lib.CS_OKLCH, "f64"),
+                                    oracle_lib.CS_OKLCH, cs, "f64")
+        # the Oklab matrices are the published 10-digit values, rounded to f32
+        assert np.abs(back - x).max() < 1e-4, cs
+
+
+def test_sigmoid_keeps_mid_gray_and_zero(oracle_lib):
+    # tone_map.rs:6-33: grays are not gamut-compressed and at mid grey the
+    # chroma factor 1 - Y^5 is ~1, so 18% grey maps to 18% grey (the square
+    # sigmoid's fixed point, tone_map.rs:176-186); black stays black
+    out = oracle_lib.sigmoid(np.array([[0.18, 0.18, 0.18], [0.0, 0.0, 0.0]], np.float32), "f64")
+    assert np.abs(out[0] - 0.18).max() < 1e-5
+    assert np.abs(out[1]).max() < 1e-12
