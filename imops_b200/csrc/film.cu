@@ -535,20 +535,42 @@ __global__ void mean_rgb_kernel(const float* __restrict__ rgb, int n, float* __r
 // 81-bin scan.  Each block owns a 32x64 pixel tile and stages the rows of
 // the halation row-pass output it needs (64 + 2*64) in shared memory.
 
-struct Base81 {
-    BaselineSpec B;
-    ScanSpec81 S;
-    float taps[2 * HAL_R + 1];
+// The 81-bin tables as pairs of adjacent bins (2l, 2l+1) for the packed f32x2
+// FMA of sm_100 (FFMA2: two lanes per instruction), plus the last bin:
+//   ne[e][l]  = -(eps_e(2l), eps_e(2l+1))   (negated: the sum is -d directly)
+//   C2[c][l]  = (C(2l)[c], C(2l+1)[c])
+// tap2[k] = (taps[k], taps[k-1]) with zero outside [0, 2R] feeds the column
+// pass two outputs (rows j, j+1) per instruction; each output still sums its
+// taps in ascending order.
+constexpr int NP81 = NB81 / 2;  // 40 pairs + bin 80
+struct Pairs81 {
+    float2 ne[3][NP81];
+    float2 C2[3][NP81];
+    float ne_last[3], C_last[3];
 };
 
+struct Base81 {
+    BaselineSpec B;
+    Pairs81 P;
+    float2 tap2[2 * HAL_R + 2];
+};
+
+// -d of bins 2l, 2l+1 for the negated densities (nD0, nD1, nD2) broadcast.
+__device__ __forceinline__ float2 neg_density2(const Pairs81& P, int l, float2 d0, float2 d1, float2 d2) {
+    float2 x = __fmul2_rn(d0, P.ne[0][l]);
+    x = __ffma2_rn(d1, P.ne[1][l], x);
+    return __ffma2_rn(d2, P.ne[2][l], x);
+}
+
 // One thread per 16 consecutive rows of a column: the halation column pass
-// (register sliding window, taps as parameter-bank operands, ascending tap
-// order as in blur_cols), then per pixel the logistic curves, grain and the
-// 81-bin scan with its tables as parameter-bank operands.
+// (register sliding window, tap pairs as parameter-bank operands, ascending
+// tap order as in blur_cols), then per pixel the logistic curves, grain and
+// the 81-bin scan with its tables as parameter-bank operands.
 __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kernel(
     const float* __restrict__ a, const float* __restrict__ hr, const float* __restrict__ noise,
     const double* __restrict__ sumsq, int W, int H, const __grid_constant__ Base81 c, float* __restrict__ rgb) {
     static_assert(HAL_R == R64, "the fused scan's column pass is the radius-64 window");
+    static_assert(R64_COL_OUT % 2 == 0, "column outputs go in pairs");
     __shared__ float s[(R64_COL_TH + 2 * HAL_R) * R64_COL_TW];
     const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
     const int tx = threadIdx.x, ty = threadIdx.y, x = x0 + tx;
@@ -565,16 +587,31 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
             norm[e] = var > 1e-12 ? (float)(1.0 / sqrt(var)) : 1.0f;
         }
     const int rb = ty * R64_COL_OUT;
-    float bs[R64_COL_OUT];
+    // bs[q] = (output row 2q, output row 2q+1); at window row m the pair takes
+    // taps m-2q and m-2q-1
+    float2 bs[R64_COL_OUT / 2];
 #pragma unroll
-    for (int j = 0; j < R64_COL_OUT; j++) bs[j] = 0.0f;
+    for (int q = 0; q < R64_COL_OUT / 2; q++) bs[q] = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int m = 0; m < R64_COL_OUT + 2 * HAL_R; m++) {
         const float v = s[(rb + m) * R64_COL_TW + tx];
+        const float2 vv = make_float2(v, v);
 #pragma unroll
-        for (int j = 0; j < R64_COL_OUT; j++) {
-            const int k = m - j;
-            if (k >= 0 && k <= 2 * HAL_R) bs[j] = fmaf(v, c.taps[k], bs[j]);
+        for (int q = 0; q < R64_COL_OUT / 2; q++) {
+            const int k = m - 2 * q;
+            if (k >= 0 && k <= 2 * HAL_R + 1) bs[q] = __ffma2_rn(vv, c.tap2[k], bs[q]);
+        }
+    }
+    // the exposure and noise of the next pixel are loaded while this one is
+    // scanned, so the global-load latency hides behind the 81-bin loop
+    const bool grain = c.B.grain_sigma > 0.0f;
+    float na[3], nz[3] = {0.f, 0.f, 0.f};
+    {
+        const size_t p0 = (size_t)min(y0 + rb, H - 1) * W + x;
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            na[e] = a[e * n + p0];
+            if (grain) nz[e] = noise[e * n + p0];
         }
     }
 #pragma unroll 1
@@ -582,32 +619,62 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
         const int y = y0 + rb + j;
         if (y >= H) break;
         const size_t p = (size_t)y * W + x;
-        float bsum = bs[0];
+        const float ca[3] = {na[0], na[1], na[2]}, cz[3] = {nz[0], nz[1], nz[2]};
+        if (j + 1 < R64_COL_OUT && y + 1 < H) {
 #pragma unroll
-        for (int q = 1; q < R64_COL_OUT; q++)
-            if (q == j) bsum = bs[q];
+            for (int e = 0; e < 3; e++) {
+                na[e] = a[e * n + p + W];
+                if (grain) nz[e] = noise[e * n + p + W];
+            }
+        }
+        float bsum = bs[0].x;
+#pragma unroll
+        for (int q = 0; q < R64_COL_OUT / 2; q++) {
+            if (2 * q == j) bsum = bs[q].x;
+            if (2 * q + 1 == j) bsum = bs[q].y;
+        }
         float D[3];
+#pragma unroll
         for (int e = 0; e < 3; e++) {
-            float E = a[e * n + p] + c.B.hal_strength * c.B.bleed[e] * bsum;
+            float E = ca[e] + c.B.hal_strength * c.B.bleed[e] * bsum;
             float le = log10f(fmaxf(E, 1e-6f));
             D[e] = c.B.dmax[e] / (1.0f + expf(-c.B.k[e] * (le - c.B.x0[e])));
-            if (c.B.grain_sigma > 0.0f) D[e] += c.B.grain_sigma * noise[e * n + p] * norm[e];
+            if (grain) D[e] += c.B.grain_sigma * cz[e] * norm[e];
         }
-        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+        const float2 d0 = make_float2(D[0], D[0]), d1 = make_float2(D[1], D[1]), d2 = make_float2(D[2], D[2]);
+        float2 o0 = make_float2(0.f, 0.f), o1 = o0, o2 = o0;
 #pragma unroll
-        for (int l = 0; l < NB81; l++) {
-            float d = D[0] * c.S.eps[0][l];
-            d = fmaf(D[1], c.S.eps[1][l], d);
-            d = fmaf(D[2], c.S.eps[2][l], d);
-            float t = ex2_fast(-d);
-            o0 = fmaf(c.S.C[l][0], t, o0);
-            o1 = fmaf(c.S.C[l][1], t, o1);
-            o2 = fmaf(c.S.C[l][2], t, o2);
+        for (int l = 0; l < NP81; l++) {
+            const float2 xd = neg_density2(c.P, l, d0, d1, d2);
+            const float2 t = make_float2(ex2_fast(xd.x), ex2_fast(xd.y));
+            o0 = __ffma2_rn(c.P.C2[0][l], t, o0);
+            o1 = __ffma2_rn(c.P.C2[1][l], t, o1);
+            o2 = __ffma2_rn(c.P.C2[2][l], t, o2);
         }
-        rgb[3 * p] = o0;
-        rgb[3 * p + 1] = o1;
-        rgb[3 * p + 2] = o2;
+        float xl = D[0] * c.P.ne_last[0];
+        xl = fmaf(D[1], c.P.ne_last[1], xl);
+        xl = fmaf(D[2], c.P.ne_last[2], xl);
+        const float tl = ex2_fast(xl);
+        rgb[3 * p] = fmaf(c.P.C_last[0], tl, o0.x + o0.y);
+        rgb[3 * p + 1] = fmaf(c.P.C_last[1], tl, o1.x + o1.y);
+        rgb[3 * p + 2] = fmaf(c.P.C_last[2], tl, o2.x + o2.y);
     }
+}
+
+// Host: the pair tables of the 81-bin scan and halation taps.
+static void build_base81(const Stock& st, Base81* hp) {
+    hp->B = st.base;
+    const ScanSpec81& S = st.scan81;
+    for (int e = 0; e < 3; e++) {
+        for (int l = 0; l < NP81; l++) hp->P.ne[e][l] = make_float2(-S.eps[e][2 * l], -S.eps[e][2 * l + 1]);
+        hp->P.ne_last[e] = -S.eps[e][NB81 - 1];
+    }
+    for (int ch = 0; ch < 3; ch++) {
+        for (int l = 0; l < NP81; l++) hp->P.C2[ch][l] = make_float2(S.C[2 * l][ch], S.C[2 * l + 1][ch]);
+        hp->P.C_last[ch] = S.C[NB81 - 1][ch];
+    }
+    for (int k = 0; k <= 2 * HAL_R + 1; k++)
+        hp->tap2[k] = make_float2(k <= 2 * HAL_R ? st.hal_taps[k] : 0.0f, k >= 1 ? st.hal_taps[k - 1] : 0.0f);
 }
 
 // ---------------------------------------------------------------------------
@@ -806,9 +873,7 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
     float* noise = A.take<float>(3 * n);
     double* gpart = A.take<double>(grain_partials(W, H, 3));
     Base81 hp;
-    hp.B = st.base;
-    hp.S = st.scan81;
-    for (int i = 0; i < 2 * HAL_R + 1; i++) hp.taps[i] = st.hal_taps[i];
+    build_base81(st, &hp);
     int g = grid_for(n);
     expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
     note_launch();

@@ -3,6 +3,7 @@
   python -m imops_b200.profile_cases amaze --width 4096 --height 3072
   python -m imops_b200.profile_cases film81 --width 4096 --height 3072
   python -m imops_b200.profile_cases fwdbwd --width 6048 --height 4024
+  python -m imops_b200.profile_cases display --width 6048 --height 4024
 
 Each case builds a seeded synthetic input, runs the stage once and
 synchronises, so `ncu -k regex:<kernel> -c 1` captures exactly one launch.
@@ -16,7 +17,7 @@ import numpy as np
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["amaze", "film81", "develop", "fwdbwd"])
+    ap.add_argument("case", choices=["amaze", "film81", "develop", "fwdbwd", "display"])
     ap.add_argument("--width", type=int, default=4096)
     ap.add_argument("--height", type=int, default=3072)
     a = ap.parse_args()
@@ -51,13 +52,24 @@ def main() -> None:
     p.target = im.CS_ACESCG
     for i in range(9):
         p.calib_d65[i] = synthetic.CALIB_D65[i]
-    p.film = 1 if a.case == "develop" else 0
+    p.film = 1 if a.case in ("develop", "display") else 0
     p.film_params = im.FilmParams(im.STOCK_BASELINE81, 0, 1, 0, -1.0, 1)
     p.baseline = im.baseline_film_defaults()
     out = im.develop_u16(raw, (0, 0, W, H), synthetic.BLACK, synthetic.WHITE, p)
     if a.case == "film81":
         torch.cuda.synchronize()
         im.film_process(out, stock=im.STOCK_BASELINE81)
+    if a.case == "display":
+        # the display modules after the scan, one chain launch through the
+        # pipeline C-ABI: Exp -> SigmoidToneMap -> CST LinearSrgb -> Gamma
+        from imops_b200.pipeline import Image, make_meta, parse_config, run_pixel_pipeline
+        img = Image.from_rgb(out.cpu().numpy().reshape(H, W, 3), im.CS_ACESCG, make_meta())
+        cfg = parse_config('[[pipeline_modules]]\nname = "Exp"\nev = 0.5\n'
+                           '[[pipeline_modules]]\nname = "SigmoidToneMap"\n'
+                           '[[pipeline_modules]]\nname = "CST"\ntarget_color_space = "LinearSrgb"\n'
+                           '[[pipeline_modules]]\nname = "Gamma"\ngamma = 2.2\n')
+        run_pixel_pipeline(img, cfg)
+        out = torch.from_numpy(img.rgb_f32())
     torch.cuda.synchronize()
     print(f"{a.case} {W}x{H} ok, mean {float(out.mean()):.6f}")
 
