@@ -34,6 +34,8 @@ using film::NB81;
 constexpr int NPAR = 24;  // wb3 C9 ev1 dmax3 k3 x03 s1 sigma1
 constexpr int BLK = 256;
 
+constexpr int NP = NB81 / 2;  // 40 bin pairs + bin 80
+
 struct Const {
     float wb[3], C[9], ev2, ev;
     float dmax[3], k[3], x0[3], s, thr;
@@ -45,6 +47,14 @@ struct Const {
     // Q[l][e][c] = -ln2 eps[e][l] Cs[l][c]: dL/dD_e = sum_c go_c sum_l Q[l][e][c] T_l,
     // so the backward needs only the forward's T_l, weighted before go is known
     float Q[NB81][3][3];
+    // the forward's tables as pairs of bins (2l, 2l+1) for the packed f32x2
+    // FMA, bin 80 alone: ne2 = -eps (the sum is -d), Cs2 per channel.  (The
+    // backward keeps scalar bins: reading single lanes of a float2 parameter
+    // costs the constant-bank operands, and packed 3x3 accumulators cost
+    // occupancy.)
+    float2 ne2[3][NP];
+    float2 Cs2[3][NP];
+    float ne_l[3], Cs_l[3];
 };
 
 __device__ __forceinline__ void color_fwd(const Const& c, const float* x, float y[3], float a[3]) {
@@ -74,12 +84,40 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
     // partials: dmax0-2 (0..2), k0-2 (3..5), x00-2 (6..8), s (9), sigma (10), loss (11)
     float acc[12];
     for (int i = 0; i < 12; i++) acc[i] = 0.0f;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    // the next pixel's inputs are loaded while this one is scanned, so the
+    // global-load latency hides behind the 81-bin loop
+    float nx[3] = {0.f, 0.f, 0.f}, nb = 0.f;
+    size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (p < n) {
+        nx[0] = x[3 * p];
+        nx[1] = x[3 * p + 1];
+        nx[2] = x[3 * p + 2];
+        nb = B[p];
+    }
+    for (; p < n; p += stride) {
+        const float xp[3] = {nx[0], nx[1], nx[2]};
+        const float b = nb;
+        if (p + stride < n) {
+            nx[0] = x[3 * (p + stride)];
+            nx[1] = x[3 * (p + stride) + 1];
+            nx[2] = x[3 * (p + stride) + 2];
+            nb = B[p + stride];
+        }
+        // the backward's per-pixel inputs, loaded before the scan that hides
+        // their latency
+        float gin[3] = {0.f, 0.f, 0.f}, bsp = 0.f;
+        if (MODE == 1) {
+            const float* src = g_out ? g_out : target;
+            gin[0] = src[3 * p];
+            gin[1] = src[3 * p + 1];
+            gin[2] = src[3 * p + 2];
+            bsp = Bs[p];
+        }
         float y[3], a[3];
-        color_fwd(c, x + 3 * p, y, a);
+        color_fwd(c, xp, y, a);
         float w[3];
         for (int k = 0; k < 3; k++) w[k] = c.minv[3 * k] * a[0] + c.minv[3 * k + 1] * a[1] + c.minv[3 * k + 2] * a[2];
-        float b = B[p];
         float E[3], le[3], sg[3], D[3];
         for (int l = 0; l < 3; l++) {
             float e = fmaxf(w[0], 0.0f) * c.A[0][l] + fmaxf(w[1], 0.0f) * c.A[1][l] + fmaxf(w[2], 0.0f) * c.A[2][l];
@@ -88,18 +126,43 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
             sg[l] = 1.0f / (1.0f + expf(-c.k[l] * (le[l] - c.x0[l])));
             D[l] = c.dmax[l] * sg[l];
         }
-        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
-        float M[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        float o0, o1, o2v;
+        float M[3][3];
+        if (MODE == 0) {
+            // forward: bins in pairs on the packed f32x2 FMA
+            const float2 d0 = make_float2(D[0], D[0]), d1 = make_float2(D[1], D[1]), d2 = make_float2(D[2], D[2]);
+            float2 oo[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
 #pragma unroll
-        for (int l = 0; l < NB81; l++) {
-            float d = D[0] * c.eps[0][l];
-            d = fmaf(D[1], c.eps[1][l], d);
-            d = fmaf(D[2], c.eps[2][l], d);
-            float t = exp2f(-d);
-            o0 = fmaf(c.Cs[l][0], t, o0);
-            o1 = fmaf(c.Cs[l][1], t, o1);
-            o2 = fmaf(c.Cs[l][2], t, o2);
-            if (MODE == 1) {
+            for (int l = 0; l < NP; l++) {
+                float2 xd = __fmul2_rn(d0, c.ne2[0][l]);
+                xd = __ffma2_rn(d1, c.ne2[1][l], xd);
+                xd = __ffma2_rn(d2, c.ne2[2][l], xd);
+                const float2 t = make_float2(exp2f(xd.x), exp2f(xd.y));
+#pragma unroll
+                for (int j = 0; j < 3; j++) oo[j] = __ffma2_rn(c.Cs2[j][l], t, oo[j]);
+            }
+            float xl = D[0] * c.ne_l[0];
+            xl = fmaf(D[1], c.ne_l[1], xl);
+            xl = fmaf(D[2], c.ne_l[2], xl);
+            const float tl = exp2f(xl);
+            o0 = fmaf(c.Cs_l[0], tl, oo[0].x + oo[0].y);
+            o1 = fmaf(c.Cs_l[1], tl, oo[1].x + oo[1].y);
+            o2v = fmaf(c.Cs_l[2], tl, oo[2].x + oo[2].y);
+        } else {
+            o0 = o1 = o2v = 0.0f;
+#pragma unroll
+            for (int e = 0; e < 3; e++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) M[e][j] = 0.0f;
+#pragma unroll
+            for (int l = 0; l < NB81; l++) {
+                float d = D[0] * c.eps[0][l];
+                d = fmaf(D[1], c.eps[1][l], d);
+                d = fmaf(D[2], c.eps[2][l], d);
+                const float t = exp2f(-d);
+                o0 = fmaf(c.Cs[l][0], t, o0);
+                o1 = fmaf(c.Cs[l][1], t, o1);
+                o2v = fmaf(c.Cs[l][2], t, o2v);
 #pragma unroll
                 for (int e = 0; e < 3; e++)
 #pragma unroll
@@ -109,16 +172,16 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
         if (MODE == 0) {
             out[3 * p] = o0;
             out[3 * p + 1] = o1;
-            out[3 * p + 2] = o2;
+            out[3 * p + 2] = o2v;
             continue;
         }
         float go[3];
         if (g_out) {
-            go[0] = g_out[3 * p];
-            go[1] = g_out[3 * p + 1];
-            go[2] = g_out[3 * p + 2];
+            go[0] = gin[0];
+            go[1] = gin[1];
+            go[2] = gin[2];
         } else {
-            float r0 = o0 - target[3 * p], r1 = o1 - target[3 * p + 1], r2 = o2 - target[3 * p + 2];
+            float r0 = o0 - gin[0], r1 = o1 - gin[1], r2 = o2v - gin[2];
             acc[11] += loss_scale * (r0 * r0 + r1 * r1 + r2 * r2);
             go[0] = 2.0f * loss_scale * r0;
             go[1] = 2.0f * loss_scale * r1;
@@ -139,7 +202,7 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
         }
         float gb = c.s * (c.bleed[0] * gE[0] + c.bleed[1] * gE[1] + c.bleed[2] * gE[2]);
         acc[9] += (c.bleed[0] * gE[0] + c.bleed[1] * gE[1] + c.bleed[2] * gE[2]) * b;
-        acc[10] += gb * Bs[p];
+        acc[10] += gb * bsp;
         gB[p] = gb;
         float gw[3];
         for (int k = 0; k < 3; k++)
@@ -354,14 +417,26 @@ int build_const(const ImopsFilmGradParams& P, const ImopsBaselineFilm& F, Const*
     for (int i = 0; i < 9; i++) c->minv[i] = st.expose.minv[i];
     for (int k = 0; k < 3; k++)
         for (int l = 0; l < 3; l++) c->A[k][l] = st.expose.A[k][l];
-    for (int l = 0; l < 3; l++)
-        for (int i = 0; i < NB81; i++) c->eps[l][i] = st.scan81.eps[l][i];
+    const film::ScanSpec81& S = st.scan81;
+    auto q = [&](int e, int j, int i) {
+        return (float)(-0.69314718055994531 * (double)S.eps[e][i] * (double)S.C[i][j]);
+    };
+    for (int e = 0; e < 3; e++)
+        for (int i = 0; i < NB81; i++) c->eps[e][i] = S.eps[e][i];
     for (int i = 0; i < NB81; i++)
-        for (int j = 0; j < 3; j++) c->Cs[i][j] = st.scan81.C[i][j];
-    for (int i = 0; i < NB81; i++)
-        for (int e = 0; e < 3; e++)
-            for (int j = 0; j < 3; j++)
-                c->Q[i][e][j] = (float)(-0.69314718055994531 * (double)st.scan81.eps[e][i] * (double)st.scan81.C[i][j]);
+        for (int e = 0; e < 3; e++) {
+            c->Cs[i][e] = S.C[i][e];
+            for (int j = 0; j < 3; j++) c->Q[i][e][j] = q(e, j, i);
+        }
+    for (int l = 0; l < NP; l++)
+        for (int e = 0; e < 3; e++) {
+            c->ne2[e][l] = make_float2(-S.eps[e][2 * l], -S.eps[e][2 * l + 1]);
+            c->Cs2[e][l] = make_float2(S.C[2 * l][e], S.C[2 * l + 1][e]);
+        }
+    for (int e = 0; e < 3; e++) {
+        c->ne_l[e] = -S.eps[e][NB81 - 1];
+        c->Cs_l[e] = S.C[NB81 - 1][e];
+    }
     if (F.hal_radius < 1 || F.hal_radius > HAL_R) return fail(IMOPS_ERR_INVALID_ARGUMENT, "hal_radius must be 1..64");
     if (!(P.hal_sigma > 0.0f)) return fail(IMOPS_ERR_INVALID_ARGUMENT, "hal_sigma must be > 0");
     halation_taps(P.hal_sigma, F.hal_radius, taps, dtaps);
