@@ -27,6 +27,21 @@ struct Taps {
     float t[2 * MAXR + 1];
 };
 
+// Radius-64 taps as pairs t2[k] = (t[k], t[k-1]), zero outside [0, 128]:
+// the radius-64 kernels accumulate two adjacent outputs per packed f32x2 FMA
+// (output j takes tap k, output j+1 tap k-1 of the same input sample), each
+// output still summing its taps in ascending order.
+struct Taps2 {
+    float2 t2[2 * MAXR + 2];
+};
+
+static Taps2 pair_taps(const Taps& tp) {
+    Taps2 p;
+    for (int k = 0; k <= 2 * MAXR + 1; k++)
+        p.t2[k] = make_float2(k <= 2 * MAXR ? tp.t[k] : 0.0f, k >= 1 ? tp.t[k - 1] : 0.0f);
+    return p;
+}
+
 __device__ __forceinline__ int reflect(int i, int n) {
     // blur.rs:70-89: mirror without repeating the edge sample
     if (n == 1) return 0;
@@ -109,7 +124,9 @@ constexpr int R64_ROW_THREADS = 256;
 constexpr int R64_ROW_TILE = R64_ROW_OUT * R64_ROW_THREADS;  // 1024 outputs per block
 
 __global__ void __launch_bounds__(R64_ROW_THREADS) blur_rows_r64_kernel(const float* __restrict__ in,
-                                                                       float* __restrict__ out, int W, int H, Taps tp) {
+                                                                       float* __restrict__ out, int W, int H,
+                                                                       const __grid_constant__ Taps2 tp) {
+    static_assert(R64_ROW_OUT % 2 == 0, "outputs go in pairs");
     __shared__ __align__(16) float s[R64_ROW_TILE + 2 * R64];
     const int y = blockIdx.y, x0 = blockIdx.x * R64_ROW_TILE;
     const float* row = in + (size_t)y * W;
@@ -117,25 +134,29 @@ __global__ void __launch_bounds__(R64_ROW_THREADS) blur_rows_r64_kernel(const fl
         s[j] = __ldg(row + reflect(x0 - R64 + j, W));
     __syncthreads();
     const int xb = R64_ROW_OUT * threadIdx.x;
-    float acc[R64_ROW_OUT];
+    float2 acc[R64_ROW_OUT / 2];
 #pragma unroll
-    for (int j = 0; j < R64_ROW_OUT; j++) acc[j] = 0.0f;
+    for (int j = 0; j < R64_ROW_OUT / 2; j++) acc[j] = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int q = 0; q < (R64_ROW_OUT + 2 * R64) / 4; q++) {
         const float4 v4 = *reinterpret_cast<const float4*>(s + xb + 4 * q);
         const float v[4] = {v4.x, v4.y, v4.z, v4.w};
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+        for (int u = 0; u < 4; u++) {
+            const float2 vv = make_float2(v[u], v[u]);
 #pragma unroll
-            for (int j = 0; j < R64_ROW_OUT; j++) {
-                const int k = 4 * q + u - j;
-                if (k >= 0 && k <= 2 * R64) acc[j] = fmaf(v[u], tp.t[k], acc[j]);
+            for (int j = 0; j < R64_ROW_OUT / 2; j++) {
+                const int k = 4 * q + u - 2 * j;
+                if (k >= 0 && k <= 2 * R64 + 1) acc[j] = __ffma2_rn(vv, tp.t2[k], acc[j]);
             }
+        }
     }
     float* o = out + (size_t)y * W;
 #pragma unroll
-    for (int j = 0; j < R64_ROW_OUT; j++)
-        if (x0 + xb + j < W) o[x0 + xb + j] = acc[j];
+    for (int j = 0; j < R64_ROW_OUT / 2; j++) {
+        if (x0 + xb + 2 * j < W) o[x0 + xb + 2 * j] = acc[j].x;
+        if (x0 + xb + 2 * j + 1 < W) o[x0 + xb + 2 * j + 1] = acc[j].y;
+    }
 }
 
 constexpr int R64_COL_TW = 32, R64_COL_GROUPS = 8, R64_COL_OUT = 16;  // 32x8 threads, 16 rows each
@@ -143,7 +164,10 @@ constexpr int R64_COL_TH = R64_COL_GROUPS * R64_COL_OUT;              // 128 out
 
 template <class Epi>
 __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) blur_cols_r64_kernel(const float* __restrict__ in,
-                                                                                     int W, int H, Taps tp, Epi epi) {
+                                                                                     int W, int H,
+                                                                                     const __grid_constant__ Taps2 tp,
+                                                                                     Epi epi) {
+    static_assert(R64_COL_OUT % 2 == 0, "outputs go in pairs");
     __shared__ float s[(R64_COL_TH + 2 * R64) * R64_COL_TW];
     const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -154,22 +178,24 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) blur_cols_r64_ker
     __syncthreads();
     if (x >= W) return;
     const int rb = ty * R64_COL_OUT;
-    float acc[R64_COL_OUT];
+    float2 acc[R64_COL_OUT / 2];
 #pragma unroll
-    for (int j = 0; j < R64_COL_OUT; j++) acc[j] = 0.0f;
+    for (int j = 0; j < R64_COL_OUT / 2; j++) acc[j] = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int m = 0; m < R64_COL_OUT + 2 * R64; m++) {
         const float v = s[(rb + m) * R64_COL_TW + tx];
+        const float2 vv = make_float2(v, v);
 #pragma unroll
-        for (int j = 0; j < R64_COL_OUT; j++) {
-            const int k = m - j;
-            if (k >= 0 && k <= 2 * R64) acc[j] = fmaf(v, tp.t[k], acc[j]);
+        for (int j = 0; j < R64_COL_OUT / 2; j++) {
+            const int k = m - 2 * j;
+            if (k >= 0 && k <= 2 * R64 + 1) acc[j] = __ffma2_rn(vv, tp.t2[k], acc[j]);
         }
     }
 #pragma unroll
-    for (int j = 0; j < R64_COL_OUT; j++) {
-        const int yy = y0 + rb + j;
-        if (yy < H) epi((size_t)yy * W + x, acc[j]);
+    for (int j = 0; j < R64_COL_OUT / 2; j++) {
+        const int yy = y0 + rb + 2 * j;
+        if (yy < H) epi((size_t)yy * W + x, acc[j].x);
+        if (yy + 1 < H) epi((size_t)(yy + 1) * W + x, acc[j].y);
     }
 }
 
@@ -216,7 +242,7 @@ int blur_rows(const float* in, float* out, int W, int H, const float* taps, int 
     for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
     if (R == R64) {
         dim3 rg((W + R64_ROW_TILE - 1) / R64_ROW_TILE, H);
-        blur_rows_r64_kernel<<<rg, R64_ROW_THREADS, 0, s>>>(in, out, W, H, tp);
+        blur_rows_r64_kernel<<<rg, R64_ROW_THREADS, 0, s>>>(in, out, W, H, pair_taps(tp));
     } else {
         dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
         blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(in, out, W, H, tp);
@@ -233,8 +259,9 @@ int blur_cols(const float* in, float* out, int W, int H, const float* taps, int 
     for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
     if (R == R64) {
         dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + R64_COL_TH - 1) / R64_COL_TH);
-        if (add) blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiAdd{out});
-        else blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiStore{out});
+        const Taps2 t2 = pair_taps(tp);
+        if (add) blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, t2, EpiAdd{out});
+        else blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, t2, EpiStore{out});
     } else {
         dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
         if (add) blur_cols_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiAdd{out});
