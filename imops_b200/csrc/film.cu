@@ -358,7 +358,8 @@ __global__ void dir_apply_kernel(float* __restrict__ planes, const float* __rest
 // bit); the field written, and the block's sum of squares (f64) stored in
 // partial[plane][block] for the variance.  Plane z holds RNG layer
 // layer0 + z.  Radius <= GR_MAXR.
-constexpr int GR_TW = 64, GR_TH = 64, GR_MAXR = 16;
+constexpr int GR_TW = 128, GR_TH = 64, GR_MAXR = 16;
+constexpr int GR_THREADS = 512, GR_TY = GR_THREADS / 32;
 
 // Noise of pixel (y, x) of a layer (grain.rs:20-45, 53-66): the sum of 12
 // uniforms minus 6, the uniforms being draws 12x+1 .. 12x+12 of the row's
@@ -378,10 +379,10 @@ __device__ __forceinline__ float grain_noise_at(uint64_t seed, int layer, int y,
     return acc - 6.0f;
 }
 
-__global__ void __launch_bounds__(256) grain_field_kernel(float* __restrict__ noise, int W, int H, uint64_t seed,
+__global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restrict__ noise, int W, int H, uint64_t seed,
                                                           int layer0, Taps tp, double* __restrict__ partial) {
     extern __shared__ float gsm[];
-    __shared__ double red[8];
+    __shared__ double red[GR_TY];
     const int layer = layer0 + (int)blockIdx.z, R = tp.R;
     const int x0 = blockIdx.x * GR_TW, y0 = blockIdx.y * GR_TH;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
@@ -391,12 +392,21 @@ __global__ void __launch_bounds__(256) grain_field_kernel(float* __restrict__ no
     float* sr = gsm + NH * NW;   // row-blurred: NH x GR_TW
     // flat over the tile + halo so every lane draws (the halo row is not a
     // multiple of the warp width)
-    for (int idx = tid; idx < NH * NW; idx += 256) {
-        const int r = idx / NW, c = idx - r * NW;
+    // (row, column) of idx stepped without a division: idx advances by
+    // GR_THREADS = dq rows + dr columns
+    const int dq = GR_THREADS / NW, dr = GR_THREADS - dq * NW;
+    int r = tid / NW, c = tid - (tid / NW) * NW;
+    for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
         sn[idx] = grain_noise_at(seed, layer, reflect(y0 - R + r, H), reflect(x0 - R + c, W));
+        r += dq;
+        c += dr;
+        if (c >= NW) {
+            c -= NW;
+            r++;
+        }
     }
     __syncthreads();
-    for (int r = ty; r < NH; r += 8)
+    for (int r = ty; r < NH; r += GR_TY)
         for (int c = tx; c < GR_TW; c += 32) {
             float acc = 0.0f;
             for (int k = 0; k <= 2 * R; k++) acc = fmaf(sn[r * GR_SW + c + k], tp.t[k], acc);
@@ -405,7 +415,7 @@ __global__ void __launch_bounds__(256) grain_field_kernel(float* __restrict__ no
     __syncthreads();
     const size_t n = (size_t)W * H;
     double sq = 0.0;
-    for (int r = ty; r < GR_TH; r += 8)
+    for (int r = ty; r < GR_TH; r += GR_TY)
         for (int c = tx; c < GR_TW; c += 32) {
             const int y = y0 + r, x = x0 + c;
             if (y >= H || x >= W) continue;
@@ -419,7 +429,7 @@ __global__ void __launch_bounds__(256) grain_field_kernel(float* __restrict__ no
     __syncthreads();
     if (tid == 0) {
         double t = 0.0;
-        for (int w = 0; w < 8; w++) t += red[w];
+        for (int w = 0; w < GR_TY; w++) t += red[w];
         partial[(size_t)blockIdx.z * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x] = t;
     }
 }
@@ -451,7 +461,7 @@ size_t grain_partials(int W, int H, int layers) {
 int grain_fields(float* noise, int W, int H, uint64_t seed, int layer0, int layers, const Taps& tp, double* partial,
                  double* sums, cudaStream_t s) {
     if (tp.R > GR_MAXR) return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "film: grain blur radius above 16 px");
-    dim3 b(32, 8), g((W + GR_TW - 1) / GR_TW, (H + GR_TH - 1) / GR_TH, layers);
+    dim3 b(32, GR_TY), g((W + GR_TW - 1) / GR_TW, (H + GR_TH - 1) / GR_TH, layers);
     const int NW = GR_TW + 2 * tp.R, NH = GR_TH + 2 * tp.R;
     const size_t smem = (size_t)NH * (NW + GR_TW) * sizeof(float);
     IMOPS_CUDA_TRY(cudaFuncSetAttribute(grain_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
