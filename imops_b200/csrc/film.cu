@@ -396,20 +396,40 @@ __global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restri
     // GR_THREADS = dq rows + dr columns
     const int dq = GR_THREADS / NW, dr = GR_THREADS - dq * NW;
     int r = tid / NW, c = tid - (tid / NW) * NW;
-    for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
-        sn[idx] = grain_noise_at(seed, layer, reflect(y0 - R + r, H), reflect(x0 - R + c, W));
-        r += dq;
-        c += dr;
-        if (c >= NW) {
-            c -= NW;
-            r++;
+    // blocks whose tile + halo lies inside the image need no mirroring
+    const bool inner = x0 - R >= 0 && y0 - R >= 0 && x0 + GR_TW + R <= W && y0 + GR_TH + R <= H;
+    if (inner) {
+        for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
+            sn[idx] = grain_noise_at(seed, layer, y0 - R + r, x0 - R + c);
+            r += dq;
+            c += dr;
+            if (c >= NW) {
+                c -= NW;
+                r++;
+            }
+        }
+    } else {
+        for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
+            sn[idx] = grain_noise_at(seed, layer, reflect(y0 - R + r, H), reflect(x0 - R + c, W));
+            r += dq;
+            c += dr;
+            if (c >= NW) {
+                c -= NW;
+                r++;
+            }
         }
     }
     __syncthreads();
     for (int r = ty; r < NH; r += GR_TY)
         for (int c = tx; c < GR_TW; c += 32) {
             float acc = 0.0f;
-            for (int k = 0; k <= 2 * R; k++) acc = fmaf(sn[r * GR_SW + c + k], tp.t[k], acc);
+            // radius 3 (a 1 px grain blur, every stock here) unrolled
+            if (R == 3) {
+#pragma unroll
+                for (int k = 0; k <= 6; k++) acc = fmaf(sn[r * GR_SW + c + k], tp.t[k], acc);
+            } else {
+                for (int k = 0; k <= 2 * R; k++) acc = fmaf(sn[r * GR_SW + c + k], tp.t[k], acc);
+            }
             sr[r * GR_TW + c] = acc;
         }
     __syncthreads();
@@ -420,7 +440,12 @@ __global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restri
             const int y = y0 + r, x = x0 + c;
             if (y >= H || x >= W) continue;
             float acc = 0.0f;
-            for (int k = 0; k <= 2 * R; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
+            if (R == 3) {
+#pragma unroll
+                for (int k = 0; k <= 6; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
+            } else {
+                for (int k = 0; k <= 2 * R; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
+            }
             noise[blockIdx.z * n + (size_t)y * W + x] = acc;
             sq += (double)acc * (double)acc;
         }
