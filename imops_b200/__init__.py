@@ -107,6 +107,19 @@ def demosaic_markesteijn(mosaic, cfa: str, shift=(0, 0), out=None, stream=None):
     return out
 
 
+def demosaic_markesteijn3(mosaic, cfa: str, shift=(0, 0), out=None, stream=None):
+    """3-pass directional X-Trans demosaic (imops_demosaic_markesteijn3); (H, W, 3)."""
+    import torch
+    _require_cuda_f32(mosaic, "mosaic")
+    H, W = mosaic.shape
+    out = out if out is not None else torch.empty((H, W, 3), device=mosaic.device, dtype=torch.float32)
+    f = lib().imops_demosaic_markesteijn3
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_void_p, ctypes.c_void_p]
+    check(f(_ptr(mosaic), W, H, _cfa(cfa), shift[0], shift[1], _ptr(out), _stream(stream)))
+    return out
+
+
 def demosaic_quad(mosaic, cfa: str, factor: int, shift=(0, 0), stream=None):
     import torch
     _require_cuda_f32(mosaic, "mosaic")

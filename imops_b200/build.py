@@ -26,7 +26,7 @@ LIB = os.path.join(HERE, "libimops_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
           "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
-EXACT = {"amaze.cu", "demosaic_simple.cu", "color.cu", "common.cu", "display.cu"}
+EXACT = {"amaze.cu", "demosaic_simple.cu", "color.cu", "common.cu", "display.cu", "markesteijn.cu"}
 
 
 def nvcc() -> str:

@@ -42,6 +42,33 @@ struct CfaDev {
     }
 };
 
+// A CFA whose period is known at compile time, for non-negative
+// coordinates, for kernels that look colours up many times per pixel: the
+// modulo is by a constant (a multiply-high) instead of a runtime integer
+// division, and the colours are 3-bit codes packed into two 64-bit words
+// (cells 0..20 and 21..41), read with shifts: no array is indexed at run
+// time, so nothing goes through local or parameter-space loads.  Same
+// colours as CfaDev::at.
+template <int PW, int PH>
+struct CfaFixed {
+    static_assert(PW * PH <= 42, "at most 42 cells in two 64-bit words");
+    unsigned long long lo, hi;
+    __device__ __forceinline__ int at(int r, int c) const {
+        const int k = (int)(((unsigned)r % PH) * PW + (unsigned)c % PW);
+        return (int)((k < 21 ? lo >> (3 * k) : hi >> (3 * (k - 21))) & 7ull);
+    }
+    static CfaFixed from(const CfaDev& d) {
+        CfaFixed f;
+        f.lo = f.hi = 0ull;
+        for (int i = 0; i < PW * PH; i++) {
+            const unsigned long long v = (unsigned long long)(d.col[i] & 7);
+            if (i < 21) f.lo |= v << (3 * i);
+            else f.hi |= v << (3 * (i - 21));
+        }
+        return f;
+    }
+};
+
 // Parses a CFA pattern string the way CFA::new does (cfa.rs:98-129) and
 // applies CFA::shift (cfa.rs:204-233).  Returns IMOPS_OK or an error code.
 int parse_cfa(const char* pattern, int shift_x, int shift_y, CfaDev* out);

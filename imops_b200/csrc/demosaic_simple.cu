@@ -12,30 +12,67 @@
 namespace imops {
 namespace simple {
 
-__global__ void mean3x3_kernel(const float* __restrict__ in, int W, int H, CfaDev cfa, float* __restrict__ out) {
+// Cfa: CfaFixed<2, 2> / CfaFixed<6, 6> (modulo by a constant) for Bayer and
+// X-Trans, CfaDev for other periods; coordinates here are never negative.
+template <class Cfa>
+__global__ void mean3x3_kernel(const float* __restrict__ in, int W, int H, const __grid_constant__ Cfa cfa,
+                               float* __restrict__ out) {
     int col = blockIdx.x * blockDim.x + threadIdx.x;
     int row = blockIdx.y * blockDim.y + threadIdx.y;
     if (col >= W || row >= H) return;
+    int centre = cfa.at(row, col);
+    if (row >= 1 && row + 1 < H && col >= 1 && col + 1 < W) {
+        // interior: the whole 3x3 window, unrolled and branch-free; each
+        // colour's sum takes its sites in row-major order (predicated adds)
+        const float* p = in + (size_t)(row - 1) * W + (col - 1);
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                if (a == 1 && b == 1) continue;
+                const int k = cfa.at(row + a - 1, col + b - 1);
+                const float v = __ldg(p + (size_t)a * W + b);
+                s0 = k == 0 ? s0 + v : s0;
+                n0 = k == 0 ? n0 + 1.0f : n0;
+                s1 = k == 1 ? s1 + v : s1;
+                n1 = k == 1 ? n1 + 1.0f : n1;
+                s2 = k == 2 ? s2 + v : s2;
+                n2 = k == 2 ? n2 + 1.0f : n2;
+            }
+        const float self = __ldg(in + (size_t)row * W + col);
+        float* o = out + ((size_t)row * W + col) * 3;
+        o[0] = centre == 0 ? self : (n0 > 0.0f ? s0 / n0 : 0.0f);
+        o[1] = centre == 1 ? self : (n1 > 0.0f ? s1 / n1 : 0.0f);
+        o[2] = centre == 2 ? self : (n2 > 0.0f ? s2 / n2 : 0.0f);
+        return;
+    }
     int y0 = row > 0 ? row - 1 : 0, y1 = row + 1 < H - 1 ? row + 1 : H - 1;
     int x0 = col > 0 ? col - 1 : 0, x1 = col + 1 < W - 1 ? col + 1 : W - 1;
-    int centre = cfa.at(row, col);
-    float v[3];
-    for (int ch = 0; ch < 3; ch++) {
-        if (ch == centre) {
-            v[ch] = __ldg(in + (size_t)row * W + col);
-            continue;
-        }
-        float sum = 0.0f, cnt = 0.0f;
-        for (int ny = y0; ny <= y1; ny++)
-            for (int nx = x0; nx <= x1; nx++) {
-                if (ny == row && nx == col) continue;
-                if (cfa.at(ny, nx) == ch) {
-                    sum += __ldg(in + (size_t)ny * W + nx);
-                    cnt += 1.0f;
-                }
+    // one row-major pass over the window: each colour's sum takes its sites
+    // in the order of the reference's per-colour loops
+    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
+    for (int ny = y0; ny <= y1; ny++)
+        for (int nx = x0; nx <= x1; nx++) {
+            if (ny == row && nx == col) continue;
+            const int k = cfa.at(ny, nx);
+            const float v = __ldg(in + (size_t)ny * W + nx);
+            if (k == 0) {
+                s0 += v;
+                n0 += 1.0f;
+            } else if (k == 1) {
+                s1 += v;
+                n1 += 1.0f;
+            } else if (k == 2) {
+                s2 += v;
+                n2 += 1.0f;
             }
-        v[ch] = cnt > 0.0f ? sum / cnt : 0.0f;
-    }
+        }
+    const float self = __ldg(in + (size_t)row * W + col);
+    float v[3];
+    v[0] = centre == 0 ? self : (n0 > 0.0f ? s0 / n0 : 0.0f);
+    v[1] = centre == 1 ? self : (n1 > 0.0f ? s1 / n1 : 0.0f);
+    v[2] = centre == 2 ? self : (n2 > 0.0f ? s2 / n2 : 0.0f);
     float* o = out + ((size_t)row * W + col) * 3;
     o[0] = v[0];
     o[1] = v[1];
@@ -73,7 +110,13 @@ extern "C" int imops_demosaic_markesteijn(const float* mosaic, int w, int h, con
     if (w <= 0 || h <= 0) return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: empty image");
     if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, "injected launch failure (markesteijn)");
     dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
-    simple::mean3x3_kernel<<<grid, block, 0, as_stream(stream)>>>(mosaic, w, h, c, rgb);
+    cudaStream_t s = as_stream(stream);
+    if (c.pw == 2 && c.ph == 2)
+        simple::mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, CfaFixed<2, 2>::from(c), rgb);
+    else if (c.pw == 6 && c.ph == 6)
+        simple::mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, CfaFixed<6, 6>::from(c), rgb);
+    else
+        simple::mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, c, rgb);
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "markesteijn launch");
     return IMOPS_OK;

@@ -4,6 +4,7 @@
   python -m imops_b200.profile_cases film81 --width 4096 --height 3072
   python -m imops_b200.profile_cases fwdbwd --width 6048 --height 4024
   python -m imops_b200.profile_cases display --width 6048 --height 4024
+  python -m imops_b200.profile_cases xtrans --width 6032 --height 4032
 
 Each case builds a seeded synthetic input, runs the stage once and
 synchronises, so `ncu -k regex:<kernel> -c 1` captures exactly one launch.
@@ -17,7 +18,7 @@ import numpy as np
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["amaze", "film81", "develop", "fwdbwd", "display"])
+    ap.add_argument("case", choices=["amaze", "film81", "develop", "fwdbwd", "display", "xtrans"])
     ap.add_argument("--width", type=int, default=4096)
     ap.add_argument("--height", type=int, default=3072)
     a = ap.parse_args()
@@ -28,6 +29,15 @@ def main() -> None:
     from imops_b200 import synthetic
 
     W, H = a.width, a.height
+    if a.case == "xtrans":
+        # the 24 MP X-Trans frame: the reference's 3x3 mean, then the 3-pass
+        # directional demosaic
+        m = torch.from_numpy(synthetic.mosaic_f32(H, W, seed=1001, pattern=synthetic.XTRANS)).cuda()
+        mean = im.demosaic_markesteijn(m, synthetic.XTRANS)
+        out = im.demosaic_markesteijn3(m, synthetic.XTRANS)
+        torch.cuda.synchronize()
+        print(f"{a.case} {W}x{H} ok, mean {float(mean.mean()):.6f} {float(out.mean()):.6f}")
+        return
     raw = torch.from_numpy(synthetic.mosaic_u16(H, W, seed=5).view(np.int16)).cuda()
     if a.case == "fwdbwd":
         # the differentiable model: AMaZE to camera RGB, forward, adjoint

@@ -110,6 +110,16 @@ int imops_amaze_size_supported(int w, int h);
 int imops_demosaic_markesteijn(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y,
                                float *rgb, imops_stream_t stream);
 
+/* 3-pass directional X-Trans demosaic after Markesteijn's method (no
+ * counterpart in the reference, whose "markesteijn" is the 3x3 mean above):
+ * green along four directions bounded by the orthogonal greens, red / blue
+ * from colour differences, two green refinement passes, and a CIELab
+ * homogeneity vote between the directions; pixels within 10 of an edge take
+ * the 3x3 mean.  6x6 CFAs only (IMOPS_ERR_UNSUPPORTED_CFA otherwise).
+ * Keeps a per-(device, stream) working set of 128 bytes per pixel. */
+int imops_demosaic_markesteijn3(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y,
+                                float *rgb, imops_stream_t stream);
+
 /* Quad-sampling previews Fast / SuperFast / SuperSuperFast (demosaic.rs:189-356):
  * factor 2, 4 or 8; rgb holds (w/factor)*(h/factor)*3 floats. */
 int imops_demosaic_quad(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y, int factor,

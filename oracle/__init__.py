@@ -138,6 +138,19 @@ def mean3x3(mosaic: np.ndarray, cfa: str, shift=(0, 0), precision: str = "f32", 
     return out
 
 
+def markesteijn3(mosaic: np.ndarray, cfa: str, shift=(0, 0), precision: str = "f32"):
+    """The library's 3-pass directional X-Trans demosaic (oracle/xtrans.c)."""
+    dt = _dt(precision)
+    m = np.ascontiguousarray(mosaic, dtype=dt)
+    H, W = m.shape
+    out = np.zeros((H, W, 3), dtype=dt)
+    c = parse_cfa(cfa, *shift)
+    fn = _f("oracle_markesteijn3", precision)
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OracleCfa), ctypes.c_void_p]
+    _check(fn(_ptr(m), W, H, ctypes.byref(c), _ptr(out)), "markesteijn3")
+    return out
+
+
 def quad(mosaic: np.ndarray, cfa: str, factor: int, shift=(0, 0), precision: str = "f32"):
     dt = _dt(precision)
     m = np.ascontiguousarray(mosaic, dtype=dt)

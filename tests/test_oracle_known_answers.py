@@ -278,3 +278,32 @@ def test_sigmoid_keeps_mid_gray_and_zero(oracle_lib):
     out = oracle_lib.sigmoid(np.array([[0.18, 0.18, 0.18], [0.0, 0.0, 0.0]], np.float32), "f64")
     assert np.abs(out[0] - 0.18).max() < 1e-5
     assert np.abs(out[1]).max() < 1e-12
+
+
+# ---- 3-pass directional X-Trans demosaic (the library's own method) -----------
+
+def _xtrans_scene(H, W, seed):
+    from imops_b200 import synthetic
+    sc = synthetic.scene(H, W, seed=seed)
+    cols = synthetic.cfa_colors(synthetic.XTRANS, H, W)
+    m = np.take_along_axis(sc, cols[..., None].astype(np.int64), axis=2)[..., 0].astype(np.float32)
+    return sc, cols, m
+
+
+def test_markesteijn3_properties(oracle_lib):
+    from imops_b200 import synthetic
+    sc, cols, m = _xtrans_scene(180, 210, 4)
+    out = oracle_lib.markesteijn3(m, synthetic.XTRANS)
+    own = np.take_along_axis(out, cols[..., None].astype(np.int64), axis=2)[..., 0]
+    assert np.array_equal(own, m)  # CFA samples kept
+    flat = oracle_lib.markesteijn3(np.full((60, 66), 0.3, np.float32), synthetic.XTRANS)
+    assert np.abs(flat[10:-10, 10:-10] - 0.3).max() == 0.0
+    mean = oracle_lib.mean3x3(m, synthetic.XTRANS)
+    band = np.ones(m.shape, bool)
+    band[10:-10, 10:-10] = False
+    assert np.array_equal(out[band], mean[band])  # edge band = the reference's 3x3 mean
+    psnr = lambda x: 10 * np.log10(1.0 / np.mean((x[12:-12, 12:-12] - sc[12:-12, 12:-12]) ** 2))
+    assert psnr(out) > psnr(mean) + 5.0
+    # f32 specification close to its FP64 instantiation
+    f64 = oracle_lib.markesteijn3(m, synthetic.XTRANS, precision="f64")
+    assert np.abs(out - f64)[10:-10, 10:-10].mean() < 1e-5
