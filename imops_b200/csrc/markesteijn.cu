@@ -79,19 +79,17 @@ __global__ void green1_kernel(const __grid_constant__ Img im, float* __restrict_
     float lo, hi, sum;
     int cnt;
     gbounds(im, r, c, lo, hi, sum, cnt);
+#pragma unroll
     for (int d = 0; d < 4; d++) {
-        int kp = 0, km = 0;
-        float a = 0.0f, b = 0.0f;
-        for (int k = 1; k <= 2 && !kp; k++)
-            if (im.col(r + k * DY[d], c + k * DX[d]) == 1) {
-                kp = k;
-                a = im.m[im.at(r + k * DY[d], c + k * DX[d])];
-            }
-        for (int k = 1; k <= 2 && !km; k++)
-            if (im.col(r - k * DY[d], c - k * DX[d]) == 1) {
-                km = k;
-                b = im.m[im.at(r - k * DY[d], c - k * DX[d])];
-            }
+        // nearest green at distance 1 or 2 on each side, both candidates read
+        // (clamped, so in bounds) and chosen by selects, no divergent loop
+        const int dy = DY[d], dx = DX[d];
+        const bool p1 = im.col(r + dy, c + dx) == 1, p2 = im.col(r + 2 * dy, c + 2 * dx) == 1;
+        const bool m1 = im.col(r - dy, c - dx) == 1, m2 = im.col(r - 2 * dy, c - 2 * dx) == 1;
+        const float vp1 = im.m[im.at(r + dy, c + dx)], vp2 = im.m[im.at(r + 2 * dy, c + 2 * dx)];
+        const float vm1 = im.m[im.at(r - dy, c - dx)], vm2 = im.m[im.at(r - 2 * dy, c - 2 * dx)];
+        const int kp = p1 ? 1 : (p2 ? 2 : 0), km = m1 ? 1 : (m2 ? 2 : 0);
+        const float a = p1 ? vp1 : (p2 ? vp2 : 0.0f), b = m1 ? vm1 : (m2 ? vm2 : 0.0f);
         float g;
         if (kp && km) g = (a * (float)km + b * (float)kp) / (float)(kp + km);
         else if (kp) g = a;
@@ -101,9 +99,6 @@ __global__ void green1_kernel(const __grid_constant__ Img im, float* __restrict_
     }
 }
 
-// Step 2 for all four directions: the 3x3 window's colours are looked up
-// once; each direction's red and blue sums take their sites in row-major
-// order, as the oracle's per-colour loops do.
 __global__ void rb_kernel(const __grid_constant__ Img im, const float* __restrict__ G, float* __restrict__ R, float* __restrict__ B) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y * blockDim.y + threadIdx.y;
     if (c >= im.W || r >= im.H) return;
@@ -169,6 +164,7 @@ __global__ void refine_kernel(const __grid_constant__ Img im, const float* __res
     float lo, hi, sum;
     int cnt;
     gbounds(im, r, c, lo, hi, sum, cnt);
+#pragma unroll
     for (int d = 0; d < 4; d++) {
         const float* C = (ch == 0 ? R : B) + d * n;
         const float* Gd = G + d * n;
@@ -182,7 +178,7 @@ __global__ void refine_kernel(const __grid_constant__ Img im, const float* __res
 __device__ __forceinline__ float cbrt_nt(float t) {
     float y = __uint_as_float(__float_as_uint(t) / 3u + 0x2A555555u);
 #pragma unroll
-    for (int it = 0; it < 4; it++) y = (y + y + t / (y * y)) / 3.0f;
+    for (int it = 0; it < 3; it++) y = (y + y + t / (y * y)) * (1.0f / 3.0f);
     return y;
 }
 

@@ -163,9 +163,10 @@ static real xt_cbrt(real t)
     float yf;
     memcpy(&yf, &u, 4);
     real y = (real)yf;
-    for (int it = 0; it < 4; it++) y = (y + y + t / (y * y)) / K(3.0);
+    /* three steps take the 6% first guess to f32 accuracy (1.6e-7) */
+    for (int it = 0; it < 3; it++) y = (y + y + t / (y * y)) * (K(1.0) / K(3.0));
 #ifndef ORACLE_F32
-    y = (y + y + t / (y * y)) / 3.0;
+    for (int it = 0; it < 2; it++) y = (y + y + t / (y * y)) * (1.0 / 3.0);
 #endif
     return y;
 }
