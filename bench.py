@@ -66,18 +66,39 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+def ncu_figure(key):
+    """A per-launch figure of the dominant kernel (`traffic_bytes_per_launch`,
+    `warp_instructions_per_launch`) from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "amaze_develop_6048x4024_ncu.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith(key + ":"):
             try:
                 return int(line.split(":")[1].strip().split()[0])
             except ValueError:
                 return None
     return None
+
+
+def ncu_traffic():
+    return ncu_figure("traffic_bytes_per_launch")
+
+
+def issue_fraction(t_ms, clk):
+    """The dominant kernel against the SM issue rate: its warp instructions
+    per launch (ncu count, scaled to the frame) over its CUDA-event time,
+    divided by SMs x 4 schedulers x the SM clock (the sampled maximum, else
+    1965 MHz)."""
+    import torch
+    inst = ncu_figure("warp_instructions_per_launch")
+    if not inst or not t_ms:
+        return None
+    mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+    peak = torch.cuda.get_device_properties(0).multi_processor_count * 4 * mhz * 1e6
+    achieved = inst / (t_ms / 1e3)
+    return {"achieved": round(achieved / 1e9, 1), "peak": round(peak / 1e9, 1), "unit": "G warp-instr/s",
+            "frac": round(achieved / peak, 4), "instructions_per_launch": inst}
 
 
 class Clocks:
@@ -357,6 +378,7 @@ def main():
     dom_bytes = H * W * 14  # u16 mosaic in (2 B) + f32 RGB out (12 B) per pixel
     achieved = dom_bytes / (t_dem / 1e3) / 1e9
     if rank == 0:
+        clk_summary = clk.summary()
         cpu_v, cpu_sample_desc = cpu_sample(os.cpu_count() or 1)
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "MP/s", "n_gpus": world, "steps": args.steps,
@@ -376,7 +398,8 @@ def main():
                          "frac": round(achieved / bw, 5), "traffic": ncu_traffic(), "peak_kind": peak_kind,
                          "bytes_per_launch": dom_bytes,
                          "note": "AMaZE is FP32-issue bound (~25 IEEE divides/px on 1.78x overlapping tiles); "
-                                 "the HBM fraction is reported against 14 B/px compulsory traffic"},
+                                 "the HBM fraction is reported against 14 B/px compulsory traffic",
+                         "issue": issue_fraction(t_dem, clk_summary)},
             "cpu_baseline": {"value": round(cpu_v, 3), "unit": "MP/s", "cores": os.cpu_count(), "kind": "port",
                              "sample": cpu_sample_desc},
             "e2e": {"value": round(e2e, 2), "unit": "MP/s", "h2d_bytes_per_step": H * W * 2,
@@ -384,7 +407,7 @@ def main():
                     "get_image_rgb_f32_c per frame, frame k submitted before frame k-1 is read back (pinned host "
                     "buffers, host clock)"},
             "gpu_launches": int(launches),
-            "clocks": clk.summary(),
+            "clocks": clk_summary,
         }
         print(json.dumps(line), flush=True)
     if dist:
