@@ -162,6 +162,23 @@ __global__ void __launch_bounds__(R64_ROW_THREADS) blur_rows_r64_kernel(const fl
 constexpr int R64_COL_TW = 32, R64_COL_GROUPS = 8, R64_COL_OUT = 16;  // 32x8 threads, 16 rows each
 constexpr int R64_COL_TH = R64_COL_GROUPS * R64_COL_OUT;              // 128 output rows per block
 
+// Stages rows y0 - 64 .. y0 + R64_COL_TH + 63 of column x into the block's
+// window s (mirrored at the image edges).  Blocks whose rows all lie inside
+// the image read them directly, the loop unrolled so a thread's 32 loads are
+// in flight together; edge blocks mirror each row.
+__device__ __forceinline__ void stage_col_window(float* s, const float* __restrict__ in, int W, int H, int x, int y0,
+                                                 int tx, int ty) {
+    constexpr int ROWS = R64_COL_TH + 2 * R64;
+    if (y0 - R64 >= 0 && y0 + R64_COL_TH + R64 <= H) {
+        const float* src = in + (size_t)(y0 - R64) * W + x;
+#pragma unroll
+        for (int j = ty; j < ROWS; j += R64_COL_GROUPS) s[j * R64_COL_TW + tx] = __ldg(src + (size_t)j * W);
+    } else {
+        for (int j = ty; j < ROWS; j += R64_COL_GROUPS)
+            s[j * R64_COL_TW + tx] = __ldg(in + (size_t)reflect(y0 - R64 + j, H) * W + x);
+    }
+}
+
 template <class Epi>
 __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) blur_cols_r64_kernel(const float* __restrict__ in,
                                                                                      int W, int H,
@@ -172,9 +189,7 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) blur_cols_r64_ker
     const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x = x0 + tx;
-    if (x < W)
-        for (int j = ty; j < R64_COL_TH + 2 * R64; j += R64_COL_GROUPS)
-            s[j * R64_COL_TW + tx] = __ldg(in + (size_t)reflect(y0 - R64 + j, H) * W + x);
+    if (x < W) stage_col_window(s, in, W, H, x, y0, tx, ty);
     __syncthreads();
     if (x >= W) return;
     const int rb = ty * R64_COL_OUT;
@@ -636,9 +651,7 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
     __shared__ float s[(R64_COL_TH + 2 * HAL_R) * R64_COL_TW];
     const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
     const int tx = threadIdx.x, ty = threadIdx.y, x = x0 + tx;
-    if (x < W)
-        for (int j = ty; j < R64_COL_TH + 2 * HAL_R; j += R64_COL_GROUPS)
-            s[j * R64_COL_TW + tx] = __ldg(hr + (size_t)reflect(y0 - HAL_R + j, H) * W + x);
+    if (x < W) stage_col_window(s, hr, W, H, x, y0, tx, ty);
     __syncthreads();
     if (x >= W) return;
     const size_t n = (size_t)W * H;
