@@ -186,6 +186,14 @@ def cpu_sample(threads: int):
     return h * w / 1e6 / dt, f"{w}x{h} crop of the 6048x4024 frame: AMaZE + WB + CST + 81-bin film (f32 oracle)"
 
 
+def workload_config(world):
+    """The workload both arms report (the reference arm times a bounded sample
+    of it, described in its cpu_baseline.sample)."""
+    return {"workload": "24MP Bayer forward: 6048x4024 RGGB u16 14-bit -> AMaZE -> WB+CST(ACEScg) -> "
+                        "81-bin film (halation, grain)", "global_batch": world, "frames_per_gpu": 1,
+            "parallelism": f"replicas x{world}", "l2": "256 MB buffer written between timed steps"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -199,8 +207,7 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": round(value, 3), "unit": "MP/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1536 * 1024 / 1e3 / value, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "24MP Bayer forward (6048x4024 RGGB u16) sampled on a 1536x1024 crop",
-                       "l2": "n/a (CPU)"},
+            "config": workload_config(world),
             "impl": "reference",
             "cpu_baseline": {"value": round(value, 3), "unit": "MP/s", "cores": threads, "kind": "port",
                              "sample": sample},
@@ -412,9 +419,7 @@ def main():
             "metric": METRIC, "value": round(value, 2), "unit": "MP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_total / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "24MP Bayer forward: 6048x4024 RGGB u16 14-bit -> AMaZE -> WB+CST(ACEScg) -> "
-                                   "81-bin film (halation, grain)", "global_batch": world, "frames_per_gpu": 1,
-                       "parallelism": f"replicas x{world}", "l2": "256 MB buffer written between timed steps"},
+            "config": workload_config(world),
             "stages_ms": {"amaze_colour": round(t_dem, 4), "film": round(t_film, 4)},
             "fwd_bwd": {"value": round(fwd_bwd, 2), "unit": "MP/s", "ms_per_step": round(t_fb / args.steps, 4),
                         "stages_ms": {"amaze_cam_plus_model_fwd": round(t_fb_fwd, 4),
