@@ -161,15 +161,18 @@ __global__ void __launch_bounds__(R64_ROW_THREADS) blur_rows_r64_kernel(const fl
 
 constexpr int R64_COL_TW = 32, R64_COL_GROUPS = 8, R64_COL_OUT = 16;  // 32x8 threads, 16 rows each
 constexpr int R64_COL_TH = R64_COL_GROUPS * R64_COL_OUT;              // 128 output rows per block
+// the plain column blur: output rows per thread and per block
+constexpr int BLUR_COL_OUT = 16, BLUR_COL_TH = R64_COL_GROUPS * BLUR_COL_OUT;
 
-// Stages rows y0 - 64 .. y0 + R64_COL_TH + 63 of column x into the block's
-// window s (mirrored at the image edges).  Blocks whose rows all lie inside
+// Stages rows y0 - 64 .. y0 + TH + 63 of column x into the block's window s
+// (mirrored at the image edges).  Blocks whose rows all lie inside
 // the image read them directly, the loop unrolled so a thread's 32 loads are
 // in flight together; edge blocks mirror each row.
+template <int TH>
 __device__ __forceinline__ void stage_col_window(float* s, const float* __restrict__ in, int W, int H, int x, int y0,
                                                  int tx, int ty) {
-    constexpr int ROWS = R64_COL_TH + 2 * R64;
-    if (y0 - R64 >= 0 && y0 + R64_COL_TH + R64 <= H) {
+    constexpr int ROWS = TH + 2 * R64;
+    if (y0 - R64 >= 0 && y0 + TH + R64 <= H) {
         const float* src = in + (size_t)(y0 - R64) * W + x;
 #pragma unroll
         for (int j = ty; j < ROWS; j += R64_COL_GROUPS) s[j * R64_COL_TW + tx] = __ldg(src + (size_t)j * W);
@@ -184,30 +187,30 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) blur_cols_r64_ker
                                                                                      int W, int H,
                                                                                      const __grid_constant__ Taps2 tp,
                                                                                      Epi epi) {
-    static_assert(R64_COL_OUT % 2 == 0, "outputs go in pairs");
-    __shared__ float s[(R64_COL_TH + 2 * R64) * R64_COL_TW];
-    const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
+    static_assert(BLUR_COL_OUT % 2 == 0, "outputs go in pairs");
+    __shared__ float s[(BLUR_COL_TH + 2 * R64) * R64_COL_TW];
+    const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * BLUR_COL_TH;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x = x0 + tx;
-    if (x < W) stage_col_window(s, in, W, H, x, y0, tx, ty);
+    if (x < W) stage_col_window<BLUR_COL_TH>(s, in, W, H, x, y0, tx, ty);
     __syncthreads();
     if (x >= W) return;
-    const int rb = ty * R64_COL_OUT;
-    float2 acc[R64_COL_OUT / 2];
+    const int rb = ty * BLUR_COL_OUT;
+    float2 acc[BLUR_COL_OUT / 2];
 #pragma unroll
-    for (int j = 0; j < R64_COL_OUT / 2; j++) acc[j] = make_float2(0.0f, 0.0f);
+    for (int j = 0; j < BLUR_COL_OUT / 2; j++) acc[j] = make_float2(0.0f, 0.0f);
 #pragma unroll
-    for (int m = 0; m < R64_COL_OUT + 2 * R64; m++) {
+    for (int m = 0; m < BLUR_COL_OUT + 2 * R64; m++) {
         const float v = s[(rb + m) * R64_COL_TW + tx];
         const float2 vv = make_float2(v, v);
 #pragma unroll
-        for (int j = 0; j < R64_COL_OUT / 2; j++) {
+        for (int j = 0; j < BLUR_COL_OUT / 2; j++) {
             const int k = m - 2 * j;
             if (k >= 0 && k <= 2 * R64 + 1) acc[j] = __ffma2_rn(vv, tp.t2[k], acc[j]);
         }
     }
 #pragma unroll
-    for (int j = 0; j < R64_COL_OUT / 2; j++) {
+    for (int j = 0; j < BLUR_COL_OUT / 2; j++) {
         const int yy = y0 + rb + 2 * j;
         if (yy < H) epi((size_t)yy * W + x, acc[j].x);
         if (yy + 1 < H) epi((size_t)(yy + 1) * W + x, acc[j].y);
@@ -273,7 +276,7 @@ int blur_cols(const float* in, float* out, int W, int H, const float* taps, int 
     tp.R = R;
     for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
     if (R == R64) {
-        dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + R64_COL_TH - 1) / R64_COL_TH);
+        dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + BLUR_COL_TH - 1) / BLUR_COL_TH);
         const Taps2 t2 = pair_taps(tp);
         if (add) blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, t2, EpiAdd{out});
         else blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, t2, EpiStore{out});
@@ -651,7 +654,7 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
     __shared__ float s[(R64_COL_TH + 2 * HAL_R) * R64_COL_TW];
     const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
     const int tx = threadIdx.x, ty = threadIdx.y, x = x0 + tx;
-    if (x < W) stage_col_window(s, hr, W, H, x, y0, tx, ty);
+    if (x < W) stage_col_window<R64_COL_TH>(s, hr, W, H, x, y0, tx, ty);
     __syncthreads();
     if (x >= W) return;
     const size_t n = (size_t)W * H;
