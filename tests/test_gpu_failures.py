@@ -75,3 +75,31 @@ def test_pipeline_c_abi_returns_null_and_last_error(gpu, monkeypatch):
     monkeypatch.delenv("IMOPS_FAULT_INJECT")
     got = run_pixel_pipeline(Image.from_u16(raw, meta), cfg).rgb_f32()
     assert np.array_equal(got, ref)
+
+
+def test_injected_failures_in_xtrans_and_display(gpu, monkeypatch):
+    """The 3-pass X-Trans demosaic (working planes) and the display chain fail
+    with a status and recover the same way."""
+    import torch
+
+    import imops_b200 as im
+    from imops_b200 import synthetic
+    m = torch.from_numpy(synthetic.mosaic_f32(96, 120, seed=4, pattern=synthetic.XTRANS)).to(gpu)
+    ref = im.demosaic_markesteijn3(m, synthetic.XTRANS)
+    monkeypatch.setenv("IMOPS_FAULT_INJECT", "alloc")
+    with pytest.raises(im.ImopsError) as e:
+        im.demosaic_markesteijn3(m, synthetic.XTRANS)
+    assert e.value.code == 5 and "injected allocation failure" in e.value.message
+    monkeypatch.setenv("IMOPS_FAULT_INJECT", "launch")
+    x = _rgb(gpu)
+    with pytest.raises(im.ImopsError) as e:
+        im.sigmoid_tone_map(x.clone())
+    assert e.value.code == 4 and "injected launch failure" in e.value.message
+    monkeypatch.delenv("IMOPS_FAULT_INJECT")
+    got = im.demosaic_markesteijn3(m, synthetic.XTRANS)
+    torch.cuda.synchronize()
+    assert torch.equal(got, ref)
+    a = im.sigmoid_tone_map(x.clone())
+    b = im.sigmoid_tone_map(x.clone())
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
