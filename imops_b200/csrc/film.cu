@@ -161,8 +161,8 @@ __global__ void __launch_bounds__(R64_ROW_THREADS) blur_rows_r64_kernel(const fl
 
 constexpr int R64_COL_TW = 32, R64_COL_GROUPS = 8, R64_COL_OUT = 16;  // 32x8 threads, 16 rows each
 constexpr int R64_COL_TH = R64_COL_GROUPS * R64_COL_OUT;              // 128 output rows per block
-// the plain column blur: output rows per thread and per block
-constexpr int BLUR_COL_OUT = 16, BLUR_COL_TH = R64_COL_GROUPS * BLUR_COL_OUT;
+// the plain column blur: output rows per thread
+constexpr int BLUR_COL_OUT = 16;
 
 // Stages rows y0 - 64 .. y0 + TH + 63 of column x into the block's window s
 // (mirrored at the image edges).  Blocks whose rows all lie inside
@@ -182,38 +182,84 @@ __device__ __forceinline__ void stage_col_window(float* s, const float* __restri
     }
 }
 
+// Streaming radius-64 column pass.  A CTA walks a 32-column strip down a
+// segment of SC_CHUNKS chunks of 128 output rows.  Its shared window is a
+// ring of three 128-row slabs: chunk j reads slabs j and j+1 while the rows
+// of slab j+2 are loaded into registers (issued before the chunk's FMAs, so
+// their latency hides behind them) and stored into the slot of slab j-1
+// afterwards.  A segment reads (chunks + 2) slabs for its chunks' rows
+// (1.5x for four chunks, against 2x for a block that stages the 256 rows of
+// one chunk).  Each output sums its taps in ascending order with the pair
+// taps (t[k], t[k-1]): the same value as the generic column blur.
+constexpr int SC_SLAB = R64_COL_GROUPS * BLUR_COL_OUT;  // 128 rows: one chunk of outputs, one slab of inputs
+constexpr int SC_CHUNKS = 4;
+constexpr int SC_PER = SC_SLAB / R64_COL_GROUPS;  // slab rows loaded per thread
+
 template <class Epi>
-__global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) blur_cols_r64_kernel(const float* __restrict__ in,
-                                                                                     int W, int H,
-                                                                                     const __grid_constant__ Taps2 tp,
-                                                                                     Epi epi) {
-    static_assert(BLUR_COL_OUT % 2 == 0, "outputs go in pairs");
-    __shared__ float s[(BLUR_COL_TH + 2 * R64) * R64_COL_TW];
-    const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * BLUR_COL_TH;
+__global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) blur_cols_r64_stream_kernel(
+    const float* __restrict__ in, int W, int H, const __grid_constant__ Taps2 tp, Epi epi) {
+    static_assert(SC_SLAB == 2 * R64, "a chunk's 256-row window is two slabs");
+    __shared__ float ring[3 * SC_SLAB * R64_COL_TW];
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x = x0 + tx;
-    if (x < W) stage_col_window<BLUR_COL_TH>(s, in, W, H, x, y0, tx, ty);
-    __syncthreads();
-    if (x >= W) return;
-    const int rb = ty * BLUR_COL_OUT;
-    float2 acc[BLUR_COL_OUT / 2];
+    const int x = blockIdx.x * R64_COL_TW + tx;
+    const bool xin = x < W;
+    const int ybase = blockIdx.y * SC_CHUNKS * SC_SLAB;
+    const int left = (H - ybase + SC_SLAB - 1) / SC_SLAB;
+    const int nch = left < SC_CHUNKS ? left : SC_CHUNKS;
+    float v[SC_PER];
+    // slab s: rows ybase - 64 + 128 s .. + 127 of column x (mirrored at the edges)
+    auto load = [&](int sl) {
+        const int r0 = ybase - R64 + SC_SLAB * sl;
+        if (r0 >= 0 && r0 + SC_SLAB <= H) {
+            const float* src = in + (size_t)(r0 + ty) * W + x;
 #pragma unroll
-    for (int j = 0; j < BLUR_COL_OUT / 2; j++) acc[j] = make_float2(0.0f, 0.0f);
+            for (int q = 0; q < SC_PER; q++) v[q] = xin ? __ldg(src + (size_t)q * R64_COL_GROUPS * W) : 0.0f;
+        } else {
 #pragma unroll
-    for (int m = 0; m < BLUR_COL_OUT + 2 * R64; m++) {
-        const float v = s[(rb + m) * R64_COL_TW + tx];
-        const float2 vv = make_float2(v, v);
-#pragma unroll
-        for (int j = 0; j < BLUR_COL_OUT / 2; j++) {
-            const int k = m - 2 * j;
-            if (k >= 0 && k <= 2 * R64 + 1) acc[j] = __ffma2_rn(vv, tp.t2[k], acc[j]);
+            for (int q = 0; q < SC_PER; q++)
+                v[q] = xin ? __ldg(in + (size_t)reflect(r0 + ty + q * R64_COL_GROUPS, H) * W + x) : 0.0f;
         }
-    }
+    };
+    auto store = [&](int sl) {
+        float* slab = ring + (sl % 3) * SC_SLAB * R64_COL_TW;
 #pragma unroll
-    for (int j = 0; j < BLUR_COL_OUT / 2; j++) {
-        const int yy = y0 + rb + 2 * j;
-        if (yy < H) epi((size_t)yy * W + x, acc[j].x);
-        if (yy + 1 < H) epi((size_t)(yy + 1) * W + x, acc[j].y);
+        for (int q = 0; q < SC_PER; q++) slab[(ty + q * R64_COL_GROUPS) * R64_COL_TW + tx] = v[q];
+    };
+    load(0);
+    store(0);
+    load(1);
+    store(1);
+    __syncthreads();
+    const int rb = ty * BLUR_COL_OUT;
+    for (int j = 0; j < nch; j++) {
+        if (j + 1 < nch) load(j + 2);  // in flight during this chunk
+        const float* A = ring + (j % 3) * SC_SLAB * R64_COL_TW;
+        const float* B = ring + ((j + 1) % 3) * SC_SLAB * R64_COL_TW;
+        float2 acc[BLUR_COL_OUT / 2];
+#pragma unroll
+        for (int q = 0; q < BLUR_COL_OUT / 2; q++) acc[q] = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int m = 0; m < BLUR_COL_OUT + 2 * R64; m++) {
+            const int row = rb + m;
+            const float val = row < SC_SLAB ? A[row * R64_COL_TW + tx] : B[(row - SC_SLAB) * R64_COL_TW + tx];
+            const float2 vv = make_float2(val, val);
+#pragma unroll
+            for (int q = 0; q < BLUR_COL_OUT / 2; q++) {
+                const int k = m - 2 * q;
+                if (k >= 0 && k <= 2 * R64 + 1) acc[q] = __ffma2_rn(vv, tp.t2[k], acc[q]);
+            }
+        }
+        if (xin) {
+            const int y0 = ybase + j * SC_SLAB + rb;
+#pragma unroll
+            for (int q = 0; q < BLUR_COL_OUT / 2; q++) {
+                const int yy = y0 + 2 * q;
+                if (yy < H) epi((size_t)yy * W + x, acc[q].x);
+                if (yy + 1 < H) epi((size_t)(yy + 1) * W + x, acc[q].y);
+            }
+        }
+        if (j + 1 < nch) store(j + 2);  // into the slot of slab j-1, read last in chunk j-1
+        __syncthreads();
     }
 }
 
@@ -276,10 +322,11 @@ int blur_cols(const float* in, float* out, int W, int H, const float* taps, int 
     tp.R = R;
     for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
     if (R == R64) {
-        dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + BLUR_COL_TH - 1) / BLUR_COL_TH);
+        dim3 cb(R64_COL_TW, R64_COL_GROUPS),
+            cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + SC_CHUNKS * SC_SLAB - 1) / (SC_CHUNKS * SC_SLAB));
         const Taps2 t2 = pair_taps(tp);
-        if (add) blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, t2, EpiAdd{out});
-        else blur_cols_r64_kernel<<<cg, cb, 0, s>>>(in, W, H, t2, EpiStore{out});
+        if (add) blur_cols_r64_stream_kernel<<<cg, cb, 0, s>>>(in, W, H, t2, EpiAdd{out});
+        else blur_cols_r64_stream_kernel<<<cg, cb, 0, s>>>(in, W, H, t2, EpiStore{out});
     } else {
         dim3 cb(COL_TW, COL_TH / COL_RPT), cg((W + COL_TW - 1) / COL_TW, (H + COL_TH - 1) / COL_TH);
         if (add) blur_cols_kernel<<<cg, cb, 0, s>>>(in, W, H, tp, EpiAdd{out});
