@@ -12,8 +12,11 @@ error reporting).
 Parity status: the reference (Rust) cannot be built or run here, so the
 restatements are pinned by the reference's own known-answer tests (ported in
 ``tests/test_oracle_known_answers.py``); the black/white scaling formula
-(rawler) and the XYZ->target conversion (``color`` crate) are restated from
-their published definitions and are "parity unpinned".
+(rawler) and the colour-space conversions (``color`` crate: XYZ->target, and
+Oklab / Oklch, the latter checked against Ottosson's published XYZ->Oklab
+table) are restated from their published definitions and are "parity
+unpinned".  ``markesteijn3`` (``xtrans.c``) is the specification of the
+library's own X-Trans method, which has no counterpart in the reference.
 """
 from __future__ import annotations
 
