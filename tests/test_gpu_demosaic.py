@@ -139,3 +139,22 @@ def test_quad_previews(oracle_lib, gpu, factor):
     # demosaic.rs:1388-1408: flat 0.5 stays 0.5
     flat = torch.full((16, 16), 0.5, device=gpu)
     assert torch.all((im.demosaic_quad(flat, "RGGB", 2) - 0.5).abs() < 1e-4)
+
+
+def test_amaze_largest_frame_45mp(oracle_lib, gpu):
+    """8256x5504 (45 MP, the largest frame of the uneven-size batch): the
+    oracle on tile-aligned corner crops.  A tile's output depends only on its
+    own window, so a crop whose origin is a multiple of 96 holds the same
+    tiles; their cores match where the window lies inside the crop or at an
+    edge the crop shares with the frame."""
+    import torch
+    import imops_b200 as im
+    H, W = 5504, 8256
+    m = synthetic.mosaic_f32(H, W, seed=45)
+    out = im.demosaic_amaze(torch.from_numpy(m).to(gpu)).cpu().numpy()
+    assert np.isfinite(out).all()
+    tl = oracle_lib.amaze(m[:384, :384])
+    assert np.array_equal(out[:288, :288], tl[:288, :288])
+    y, x = 96 * 53, 96 * 82
+    br = oracle_lib.amaze(m[y:, x:], shift=(x, y))
+    assert np.array_equal(out[y + 96:, x + 96:], br[96:, 96:])

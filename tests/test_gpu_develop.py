@@ -90,3 +90,27 @@ def test_develop_film_requires_acescg(gpu):
     with pytest.raises(im.ImopsError) as e:
         im.develop_u16(raw, (0, 0, 64, 64), synthetic.BLACK, synthetic.WHITE, p)
     assert e.value.code == 6
+
+
+def test_develop_largest_frame_45mp(gpu):
+    """The fused forward (AMaZE + colour + 81-bin film, grain on) on an
+    8256x5504 frame: runs within the working sets and stays finite."""
+    import torch
+    import imops_b200 as im
+    from imops_b200 import synthetic
+    H, W = 5504, 8256
+    raw = torch.from_numpy(synthetic.mosaic_u16(H, W, seed=46).view(np.int16)).to(gpu)
+    p = im.DevelopParams()
+    p.demosaic, p.cfa, p.clip_pt = im.DEMOSAIC_AMAZE, b"RGGB", 1.0
+    for i in range(4):
+        p.wb[i] = synthetic.WB[i]
+    p.target = im.CS_ACESCG
+    for i in range(9):
+        p.calib_d65[i] = synthetic.CALIB_D65[i]
+    p.film = 1
+    p.film_params = im.FilmParams(im.STOCK_BASELINE81, 0, 1, 0, -1.0, 1)
+    p.baseline = im.baseline_film_defaults()
+    out = im.develop_u16(raw, (0, 0, W, H), synthetic.BLACK, synthetic.WHITE, p)
+    torch.cuda.synchronize()
+    assert out.shape == (H, W, 3)
+    assert bool(torch.isfinite(out).all())
