@@ -284,6 +284,78 @@ def film_process(rgb, stock: int = STOCK_COLORNEG200, film_format: int = FORMAT_
     return rgb
 
 
+class FilmStages:
+    """The reference model's film sub-stages (imops_film_expose .. _invert),
+    one call each, on an (H, W, 3) float32 ACEScg CUDA image.  Chained in
+    order they give film_process's result; the planes are (E, H, W)."""
+
+    def __init__(self, stock: int = STOCK_COLORNEG200, film_format: int = FORMAT_35MM, seed: int = 1,
+                 output: int = FILM_NEGATIVE_LINEAR, shutter: float = -1.0, grain: bool = True):
+        self.p = FilmParams(stock, film_format, seed, output, shutter, int(grain))
+        n = ctypes.c_int(0)
+        f = lib().imops_film_layers
+        f.argtypes = [ctypes.POINTER(FilmParams), ctypes.POINTER(ctypes.c_int)]
+        check(f(ctypes.byref(self.p), ctypes.byref(n)))
+        self.layers = n.value
+
+    def _call(self, name, argtypes, *args, stream=None):
+        f = getattr(lib(), name)
+        f.argtypes = argtypes + [ctypes.c_void_p]
+        check(f(*args, _stream(stream)))
+
+    def expose(self, rgb, stream=None):
+        import torch
+        _require_cuda_f32(rgb, "rgb")
+        H, W = rgb.shape[:2]
+        planes = torch.empty((self.layers, H, W), device=rgb.device, dtype=torch.float32)
+        self._call("imops_film_expose", [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(FilmParams),
+                                         ctypes.c_void_p], _ptr(rgb), W, H, ctypes.byref(self.p), _ptr(planes),
+                   stream=stream)
+        return planes
+
+    def halation(self, planes, stream=None):
+        _, H, W = planes.shape
+        self._call("imops_film_halation", [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(FilmParams)],
+                   _ptr(planes), W, H, ctypes.byref(self.p), stream=stream)
+        return planes
+
+    def develop(self, planes, stream=None):
+        import torch
+        _, H, W = planes.shape
+        mask = torch.empty_like(planes)
+        self._call("imops_film_develop", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(FilmParams)],
+                   _ptr(planes), _ptr(mask), W, H, ctypes.byref(self.p), stream=stream)
+        return planes, mask
+
+    def grain(self, planes, stream=None):
+        _, H, W = planes.shape
+        self._call("imops_film_grain", [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(FilmParams)],
+                   _ptr(planes), W, H, ctypes.byref(self.p), stream=stream)
+        return planes
+
+    def scan(self, planes, mask, stream=None):
+        import torch
+        _, H, W = planes.shape
+        rgb = torch.empty((H, W, 3), device=planes.device, dtype=torch.float32)
+        self._call("imops_film_scan", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(FilmParams), ctypes.c_void_p],
+                   _ptr(planes), _ptr(mask), W, H, ctypes.byref(self.p), _ptr(rgb), stream=stream)
+        return rgb
+
+    def invert(self, rgb, stream=None):
+        H, W = rgb.shape[:2]
+        self._call("imops_film_invert", [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(FilmParams)],
+                   _ptr(rgb), W, H, ctypes.byref(self.p), stream=stream)
+        return rgb
+
+    def run(self, rgb, stream=None):
+        """All stages in film::process's order; returns the film RGB."""
+        planes = self.halation(self.expose(rgb, stream), stream)
+        planes, mask = self.develop(planes, stream)
+        return self.invert(self.scan(self.grain(planes, stream), mask, stream), stream)
+
+
 class DevelopParams(ctypes.Structure):
     """ImopsDevelopParams (include/imops_b200.h)."""
 

@@ -867,21 +867,24 @@ size_t ref_workspace_bytes(size_t n, int E) {
     return (size_t)(3 * E + 2) * n * 4 + sizeof(RefSpec) + sizeof(ScanSpec16) + 64 * 1024;
 }
 
-// expose -> develop -> scan for the reference model; rgb in, rgb out.
-int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int grain, Arena& A, const RefSpec* dR,
-                  const ScanSpec16* dC, cudaStream_t s) {
+// The reference model's stages (film/mod.rs:77-129), each on the stock's E
+// planar layers; run_reference chains them, and the imops_film_* entry
+// points expose them one by one.
+//   expose: ACEScg RGB -> absorbed exposure per layer (exposure/mod.rs:45-137,
+//     absorption.rs:24-108)
+int stage_expose(const float* rgb, int W, int H, const Stock& st, float* planes, cudaStream_t s) {
+    const size_t n = (size_t)W * H;
+    expose_kernel<<<grid_for(n), 256, 0, s>>>(rgb, n, st.expose, planes, nullptr);
+    note_launch();
+    return IMOPS_OK;
+}
+
+//   halation: local scatter and the wide bounce of the deepest layer
+//     (halation.rs:24-93); tmp, bounce: one plane each
+int stage_halation(float* planes, int W, int H, const Stock& st, float* tmp, float* bounce, cudaStream_t s) {
     const RefSpec& R = st.ref;
     const int E = R.E;
     const size_t n = (size_t)W * H;
-    float* planes = A.take<float>(E * n);
-    float* mask = A.take<float>(E * n);
-    float* inh = A.take<float>(E * n);
-    float* tmp = A.take<float>(n);
-    float* noise = A.take<float>(n);
-    double* sums = A.take<double>(MAXE);
-    int g = grid_for(n);
-    expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, planes, nullptr);
-    note_launch();
     Taps tp;
     int rc;
     if (R.sigma_local >= 1e-3f && R.local_mix > 0.0f) {
@@ -898,9 +901,23 @@ int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int 
         eb.E = E;
         for (int e = 0; e < MAXE; e++) eb.gain[e] = R.hal_gain[e];
         // the bounce source is the deepest plane before the bounce is added
-        IMOPS_CUDA_TRY(cudaMemcpyAsync(noise, planes + (E - 1) * n, n * 4, cudaMemcpyDeviceToDevice, s), "copy");
-        if ((rc = blur(noise, tmp, W, H, tp, eb, s))) return rc;
+        IMOPS_CUDA_TRY(cudaMemcpyAsync(bounce, planes + (E - 1) * n, n * 4, cudaMemcpyDeviceToDevice, s), "copy");
+        if ((rc = blur(bounce, tmp, W, H, tp, eb, s))) return rc;
     }
+    return IMOPS_OK;
+}
+
+//   develop: capture LUT + reciprocity + reduction to image-dye and mask
+//     densities, DIR inhibition, adjacency (capture.rs:61-88,
+//     reduction.rs:16-68, diffusion.rs:11-84); inh: E planes, tmp: one
+int stage_develop(float* planes, float* mask, int W, int H, const Stock& st, const RefSpec* dR, float* inh,
+                  float* tmp, cudaStream_t s) {
+    const RefSpec& R = st.ref;
+    const int E = R.E;
+    const size_t n = (size_t)W * H;
+    const int g = grid_for(n);
+    Taps tp;
+    int rc;
     lut_reduce_kernel<<<g, 256, 0, s>>>(planes, mask, n, E, dR);
     note_launch();
     if (R.dir_any && R.sigma_dir >= 1e-3f) {
@@ -915,21 +932,79 @@ int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int 
         for (int e = 0; e < E; e++)
             if ((rc = blur(planes + e * n, tmp, W, H, tp, EpiAdjacency{planes + e * n, R.beta}, s))) return rc;
     }
-    if (grain) {
-        if ((rc = taps_for(fmaxf(R.sigma_grain, 1.0f), &tp))) return rc;
-        IMOPS_CUDA_TRY(cudaMemsetAsync(sums, 0, MAXE * sizeof(double), s), "memset");
-        for (int e = 0; e < E; e++) {
-            if (R.kappa[e] <= 0.0f || R.dmax[e] <= 0.0f) continue;
-            // the inhibition planes are free here: they hold the block sums
-            if ((rc = grain_fields(noise, W, H, seed, e, 1, tp, reinterpret_cast<double*>(inh), sums + e, s)))
-                return rc;
-            grain_apply_kernel<<<g, 256, 0, s>>>(planes + e * n, noise, n, sums + e, R.kappa[e], R.dmax[e]);
-            note_launch();
-        }
+    return IMOPS_OK;
+}
+
+//   grain: seeded SplitMix64 fields, normalised and scaled per layer
+//     (grain.rs:53-100); noise: one plane, partial: grain_partials(W, H, 1)
+//     doubles, sums: MAXE doubles
+int stage_grain(float* planes, int W, int H, const Stock& st, uint64_t seed, float* noise, double* partial,
+                double* sums, cudaStream_t s) {
+    const RefSpec& R = st.ref;
+    const size_t n = (size_t)W * H;
+    Taps tp;
+    int rc;
+    if ((rc = taps_for(fmaxf(R.sigma_grain, 1.0f), &tp))) return rc;
+    IMOPS_CUDA_TRY(cudaMemsetAsync(sums, 0, MAXE * sizeof(double), s), "memset");
+    for (int e = 0; e < R.E; e++) {
+        if (R.kappa[e] <= 0.0f || R.dmax[e] <= 0.0f) continue;
+        if ((rc = grain_fields(noise, W, H, seed, e, 1, tp, partial, sums + e, s))) return rc;
+        grain_apply_kernel<<<grid_for(n), 256, 0, s>>>(planes + e * n, noise, n, sums + e, R.kappa[e], R.dmax[e]);
+        note_launch();
     }
-    scan16_kernel<<<g, 256, 0, s>>>(planes, mask, n, dC, rgb);
+    return IMOPS_OK;
+}
+
+//   scan: densities -> ACEScg RGB of the scanned negative (scan/mod.rs:24-30,
+//     densitometry.rs:13-73)
+int stage_scan(const float* planes, const float* mask, int W, int H, const ScanSpec16* dC, float* rgb,
+               cudaStream_t s) {
+    const size_t n = (size_t)W * H;
+    scan16_kernel<<<grid_for(n), 256, 0, s>>>(planes, mask, n, dC, rgb);
     note_launch();
+    return IMOPS_OK;
+}
+
+// expose -> halation -> develop -> grain -> scan for the reference model;
+// rgb in, rgb out.
+int run_reference(float* rgb, int W, int H, const Stock& st, uint64_t seed, int grain, Arena& A, const RefSpec* dR,
+                  const ScanSpec16* dC, cudaStream_t s) {
+    const int E = st.ref.E;
+    const size_t n = (size_t)W * H;
+    float* planes = A.take<float>(E * n);
+    float* mask = A.take<float>(E * n);
+    float* inh = A.take<float>(E * n);
+    float* tmp = A.take<float>(n);
+    float* noise = A.take<float>(n);
+    double* sums = A.take<double>(MAXE);
+    int rc;
+    if ((rc = stage_expose(rgb, W, H, st, planes, s))) return rc;
+    if ((rc = stage_halation(planes, W, H, st, tmp, noise, s))) return rc;
+    if ((rc = stage_develop(planes, mask, W, H, st, dR, inh, tmp, s))) return rc;
+    // the inhibition planes are free after develop: they hold the grain's block sums
+    if (grain && (rc = stage_grain(planes, W, H, st, seed, noise, reinterpret_cast<double*>(inh), sums, s)))
+        return rc;
+    if ((rc = stage_scan(planes, mask, W, H, dC, rgb, s))) return rc;
     IMOPS_CUDA_TRY(cudaGetLastError(), "film kernels");
+    return IMOPS_OK;
+}
+
+// PositiveLinear's reference points (film/mod.rs:136-151): the mean RGB of
+// a 32x32 mid-grey patch through the same path (seed 0) into mid_dmin[0..2]
+// and the stock's normalised Dmin into mid_dmin[3..5].  Takes
+// ref_workspace_bytes(1024, E) + 1024 * 12 bytes of A.
+int mid_gray_negative(const Stock& st, int grain, Arena& A, const RefSpec* dR, const ScanSpec16* dC, float* mid_dmin,
+                      cudaStream_t s) {
+    const size_t nm = 32 * 32;
+    float g = relative_to_absolute_y(0.185f, st.ref.box_iso);
+    std::vector<float> patch(nm * 3, g);
+    float* dpatch = A.take<float>(nm * 3);
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(dpatch, patch.data(), nm * 12, cudaMemcpyHostToDevice, s), "copy patch");
+    int rc;
+    if ((rc = run_reference(dpatch, 32, 32, st, 0, grain, A, dR, dC, s))) return rc;
+    mean_rgb_kernel<<<1, 256, 0, s>>>(dpatch, (int)nm, mid_dmin);
+    note_launch();
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(mid_dmin + 3, st.ref.dmin_norm, 12, cudaMemcpyHostToDevice, s), "copy dmin");
     return IMOPS_OK;
 }
 
@@ -950,24 +1025,41 @@ int process_reference(float* rgb, int W, int H, const ImopsFilmParams& P, cudaSt
     IMOPS_CUDA_TRY(cudaMemcpyAsync(dR, &st.ref, sizeof(RefSpec), cudaMemcpyHostToDevice, s), "copy spec");
     IMOPS_CUDA_TRY(cudaMemcpyAsync(dC, &st.scan16, sizeof(ScanSpec16), cudaMemcpyHostToDevice, s), "copy spec");
     bool positive = P.output == IMOPS_FILM_POSITIVE_LINEAR && !st.ref.any_reversal;
-    if (positive) {
-        // mid-gray negative: a 32x32 flat patch through the same path, seed 0
-        // (film/mod.rs:136-151)
-        float g = relative_to_absolute_y(0.185f, st.ref.box_iso);
-        std::vector<float> patch(nm * 3, g);
-        float* dpatch = A.take<float>(nm * 3);
-        IMOPS_CUDA_TRY(cudaMemcpyAsync(dpatch, patch.data(), nm * 12, cudaMemcpyHostToDevice, s), "copy patch");
-        Arena B{A.base, A.off};
-        B.off = A.off + ref_workspace_bytes(n, st.ref.E);
-        if ((rc = run_reference(dpatch, 32, 32, st, 0, P.grain, B, dR, dC, s))) return rc;
-        mean_rgb_kernel<<<1, 256, 0, s>>>(dpatch, (int)nm, mid_dmin);
-        note_launch();
-        IMOPS_CUDA_TRY(cudaMemcpyAsync(mid_dmin + 3, st.ref.dmin_norm, 12, cudaMemcpyHostToDevice, s), "copy dmin");
-    }
+    if (positive && (rc = mid_gray_negative(st, P.grain, A, dR, dC, mid_dmin, s))) return rc;
     if ((rc = run_reference(rgb, W, H, st, P.seed, P.grain, A, dR, dC, s))) return rc;
-    if (positive) invert_kernel<<<grid_for(n), 256, 0, s>>>(rgb, n, mid_dmin);
-    note_launch();
+    if (positive) {
+        invert_kernel<<<grid_for(n), 256, 0, s>>>(rgb, n, mid_dmin);
+        note_launch();
+    }
     IMOPS_CUDA_TRY(cudaGetLastError(), "film invert");
+    return IMOPS_OK;
+}
+
+// One sub-stage call: the stock (reference model only), device copies of its
+// specs and an arena of `extra` bytes in the film workspace.
+struct StageCtx {
+    Stock st;
+    Arena A;
+    RefSpec* dR;
+    ScanSpec16* dC;
+};
+
+int stage_ctx(const ImopsFilmParams* P, int W, int H, size_t extra, cudaStream_t s, StageCtx* c) {
+    if (!P) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film stage: NULL params");
+    if (W <= 0 || H <= 0) return fail(IMOPS_ERR_INVALID_DIMENSIONS, "invalid image dimensions");
+    float pitch = 0;
+    int rc = build_stock(P->stock, P->film_format, W, P->shutter_seconds, nullptr, &c->st, &pitch);
+    if (rc) return rc;
+    if (c->st.model != MODEL_REFERENCE)
+        return fail(IMOPS_ERR_INVALID_STOCK, "film stages: the baseline preset runs only whole (imops_film_process)");
+    void* ws = nullptr;
+    if ((rc = workspace(s, sizeof(RefSpec) + sizeof(ScanSpec16) + extra + 4096, &ws))) return rc;
+    c->A = Arena{static_cast<char*>(ws), 0};
+    c->dR = c->A.take<RefSpec>(1);
+    c->dC = c->A.take<ScanSpec16>(1);
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(c->dR, &c->st.ref, sizeof(RefSpec), cudaMemcpyHostToDevice, s), "copy spec");
+    IMOPS_CUDA_TRY(cudaMemcpyAsync(c->dC, &c->st.scan16, sizeof(ScanSpec16), cudaMemcpyHostToDevice, s),
+                   "copy spec");
     return IMOPS_OK;
 }
 
@@ -1020,6 +1112,118 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
 
 
 using namespace imops;
+
+// ---- the reference model's sub-stages ----------------------------------------
+
+extern "C" int imops_film_layers(const ImopsFilmParams* params, int* layers) {
+    clear_error();
+    if (!layers) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film_layers: NULL output");
+    film::StageCtx c;
+    if (!params) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film stage: NULL params");
+    float pitch = 0;
+    int rc = film::build_stock(params->stock, params->film_format, 1024, params->shutter_seconds, nullptr, &c.st,
+                               &pitch);
+    if (rc) return rc;
+    if (c.st.model != film::MODEL_REFERENCE)
+        return fail(IMOPS_ERR_INVALID_STOCK, "film stages: the baseline preset runs only whole (imops_film_process)");
+    *layers = c.st.ref.E;
+    return IMOPS_OK;
+}
+
+extern "C" int imops_film_expose(const float* rgb, int w, int h, const ImopsFilmParams* params, float* planes,
+                                 imops_stream_t stream) {
+    clear_error();
+    cudaStream_t s = as_stream(stream);
+    film::StageCtx c;
+    int rc = film::stage_ctx(params, w, h, 0, s, &c);
+    if (rc) return rc;
+    if (!rgb || !planes) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film_expose: NULL buffer");
+    if ((rc = film::stage_expose(rgb, w, h, c.st, planes, s))) return rc;
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film_expose");
+    return IMOPS_OK;
+}
+
+extern "C" int imops_film_halation(float* planes, int w, int h, const ImopsFilmParams* params,
+                                   imops_stream_t stream) {
+    clear_error();
+    cudaStream_t s = as_stream(stream);
+    const size_t n = (size_t)(w > 0 ? w : 0) * (h > 0 ? h : 0);
+    film::StageCtx c;
+    int rc = film::stage_ctx(params, w, h, 2 * n * 4 + 512, s, &c);
+    if (rc) return rc;
+    if (!planes) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film_halation: NULL buffer");
+    float* tmp = c.A.take<float>(n);
+    float* bounce = c.A.take<float>(n);
+    if ((rc = film::stage_halation(planes, w, h, c.st, tmp, bounce, s))) return rc;
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film_halation");
+    return IMOPS_OK;
+}
+
+extern "C" int imops_film_develop(float* planes, float* mask, int w, int h, const ImopsFilmParams* params,
+                                  imops_stream_t stream) {
+    clear_error();
+    cudaStream_t s = as_stream(stream);
+    const size_t n = (size_t)(w > 0 ? w : 0) * (h > 0 ? h : 0);
+    film::StageCtx c;
+    int rc = film::stage_ctx(params, w, h, (size_t)(film::MAXE + 1) * n * 4 + 512, s, &c);
+    if (rc) return rc;
+    if (!planes || !mask) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film_develop: NULL buffer");
+    float* inh = c.A.take<float>((size_t)c.st.ref.E * n);
+    float* tmp = c.A.take<float>(n);
+    if ((rc = film::stage_develop(planes, mask, w, h, c.st, c.dR, inh, tmp, s))) return rc;
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film_develop");
+    return IMOPS_OK;
+}
+
+extern "C" int imops_film_grain(float* planes, int w, int h, const ImopsFilmParams* params, imops_stream_t stream) {
+    clear_error();
+    cudaStream_t s = as_stream(stream);
+    const size_t n = (size_t)(w > 0 ? w : 0) * (h > 0 ? h : 0);
+    const size_t np = w > 0 && h > 0 ? film::grain_partials(w, h, 1) : 0;
+    film::StageCtx c;
+    int rc = film::stage_ctx(params, w, h, n * 4 + np * 8 + film::MAXE * 8 + 768, s, &c);
+    if (rc) return rc;
+    if (!planes) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film_grain: NULL buffer");
+    if (!params->grain) return IMOPS_OK;
+    float* noise = c.A.take<float>(n);
+    double* partial = c.A.take<double>(np);
+    double* sums = c.A.take<double>(film::MAXE);
+    if ((rc = film::stage_grain(planes, w, h, c.st, params->seed, noise, partial, sums, s))) return rc;
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film_grain");
+    return IMOPS_OK;
+}
+
+extern "C" int imops_film_scan(const float* planes, const float* mask, int w, int h, const ImopsFilmParams* params,
+                               float* rgb, imops_stream_t stream) {
+    clear_error();
+    cudaStream_t s = as_stream(stream);
+    film::StageCtx c;
+    int rc = film::stage_ctx(params, w, h, 0, s, &c);
+    if (rc) return rc;
+    if (!planes || !mask || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film_scan: NULL buffer");
+    if ((rc = film::stage_scan(planes, mask, w, h, c.dC, rgb, s))) return rc;
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film_scan");
+    return IMOPS_OK;
+}
+
+extern "C" int imops_film_invert(float* rgb, int w, int h, const ImopsFilmParams* params, imops_stream_t stream) {
+    clear_error();
+    cudaStream_t s = as_stream(stream);
+    // the mid-grey patch's path and its reference points come from the same arena
+    const size_t nm = 32 * 32;
+    film::StageCtx c;
+    int rc = film::stage_ctx(params, w, h, film::ref_workspace_bytes(nm, film::MAXE) + nm * 12 + 1024, s, &c);
+    if (rc) return rc;
+    if (!rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film_invert: NULL buffer");
+    if (!(params->output == IMOPS_FILM_POSITIVE_LINEAR && !c.st.ref.any_reversal)) return IMOPS_OK;
+    float* mid_dmin = c.A.take<float>(8);
+    if ((rc = film::mid_gray_negative(c.st, params->grain, c.A, c.dR, c.dC, mid_dmin, s))) return rc;
+    const size_t n = (size_t)w * h;
+    film::invert_kernel<<<film::grid_for(n), 256, 0, s>>>(rgb, n, mid_dmin);
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "film_invert");
+    return IMOPS_OK;
+}
 
 extern "C" int imops_film_process(float* rgb, int w, int h, int color_space, const ImopsFilmParams* params,
                                   const ImopsBaselineFilm* baseline, imops_stream_t stream) {

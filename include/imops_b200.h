@@ -242,6 +242,48 @@ void imops_baseline_film_defaults(ImopsBaselineFilm *out);
 int imops_film_process(float *rgb, int w, int h, int color_space, const ImopsFilmParams *params,
                        const ImopsBaselineFilm *baseline, imops_stream_t stream);
 
+/* ---- the reference model's film sub-stages -----------------------------------
+ * The stages that film::process (film/mod.rs:77-129) chains, one call each,
+ * for a host that runs them separately.  imops_film_process is the same
+ * chain: expose -> halation -> develop -> grain -> scan -> invert gives its
+ * result bit for bit.  Planes are planar f32 (w*h each) of the stock's E
+ * emulsion layers (imops_film_layers); rgb is interleaved ACEScg.  The
+ * baseline preset runs only whole (IMOPS_ERR_INVALID_STOCK here).  params
+ * supply stock, film format (pixel pitch), shutter, seed, grain and output as
+ * for imops_film_process.  Each call keeps its scratch in the per-(device,
+ * stream) film working set. */
+
+/* E, the stock's emulsion layers (film/stock/mod.rs:152-214). */
+int imops_film_layers(const ImopsFilmParams *params, int *layers);
+
+/* Absorbed exposure per layer from absolute-luminance ACEScg
+ * (exposure/mod.rs:45-137 with absorption.rs:24-108): rgb -> E planes. */
+int imops_film_expose(const float *rgb, int w, int h, const ImopsFilmParams *params, float *planes,
+                      imops_stream_t stream);
+
+/* Local scatter and the wide halation bounce, in place (halation.rs:24-93). */
+int imops_film_halation(float *planes, int w, int h, const ImopsFilmParams *params, imops_stream_t stream);
+
+/* Development, in place: capture LUT with reciprocity, reduction to image-dye
+ * densities (planes) and mask densities (mask, E planes), DIR inhibition and
+ * adjacency (capture.rs:61-88, reduction.rs:16-68, diffusion.rs:11-84). */
+int imops_film_develop(float *planes, float *mask, int w, int h, const ImopsFilmParams *params,
+                       imops_stream_t stream);
+
+/* Seeded grain on the image-dye planes, in place (grain.rs:53-100); nothing
+ * when params->grain is 0. */
+int imops_film_grain(float *planes, int w, int h, const ImopsFilmParams *params, imops_stream_t stream);
+
+/* Scan of the densities to ACEScg RGB (scan/mod.rs:24-30,
+ * densitometry.rs:13-73): planes + mask -> rgb. */
+int imops_film_scan(const float *planes, const float *mask, int w, int h, const ImopsFilmParams *params,
+                    float *rgb, imops_stream_t stream);
+
+/* PositiveLinear inversion in place (invert.rs:36-108, with the mid-grey
+ * negative of film/mod.rs:136-151); nothing for NegativeLinear or a
+ * reversal stock. */
+int imops_film_invert(float *rgb, int w, int h, const ImopsFilmParams *params, imops_stream_t stream);
+
 /* ---- fused forward -------------------------------------------------------
  * The path Demosaic -> CFACoeffs -> Exp -> CST -> Film (the module chain of
  * run_pixel_pipeline, pichromatic-pipeline/src/pipeline.rs:4-13, with the

@@ -119,3 +119,31 @@ def test_other_stocks_small_frame(oracle_lib, gpu, stock):
     ref = oracle_lib.film_process(x, stock=stock, seed=3, grain=True, precision="f32")
     out = _run(gpu, x, stock=stock, seed=3, grain=True)
     assert np.abs(out - ref).max() < TOL
+
+
+@pytest.mark.parametrize("stock", [0, 1, 2, 5, 6])
+@pytest.mark.parametrize("output", [0, 1])
+def test_film_sub_stages_chain_to_film_process(gpu, stock, output):
+    """expose -> halation -> develop -> grain -> scan -> invert as separate
+    C-ABI calls equals film_process bit for bit (film/mod.rs:77-129)."""
+    import torch
+    import imops_b200 as im
+    x = torch.from_numpy(_abs_scene(96, 160, seed=30 + stock)).to(gpu)
+    ref = im.film_process(x.clone(), stock=stock, seed=9, output=output, grain=True)
+    st = im.FilmStages(stock=stock, seed=9, output=output, grain=True)
+    assert st.layers >= 1
+    got = st.run(x.clone())
+    torch.cuda.synchronize()
+    assert torch.equal(got, ref)
+
+
+def test_film_sub_stages_shapes_and_errors(gpu):
+    import torch
+    import imops_b200 as im
+    st = im.FilmStages(stock=im.STOCK_PORTRA400)
+    x = torch.from_numpy(_abs_scene(32, 48, seed=3)).to(gpu)
+    planes = st.expose(x)
+    assert planes.shape == (st.layers, 32, 48) and st.layers == 6
+    with pytest.raises(im.ImopsError) as e:
+        im.FilmStages(stock=im.STOCK_BASELINE81)
+    assert e.value.code == 8
