@@ -395,6 +395,13 @@ def develop_f32(mosaic, params: DevelopParams, shift=(0, 0), out=None, stream=No
     return out
 
 
+def release_working_sets():
+    """Frees the cached per-(device, stream) working sets on the current device."""
+    f = lib().imops_release_working_sets
+    f.argtypes = []
+    check(f())
+
+
 def launch_count() -> int:
     f = lib().imops_launch_count
     f.restype = ctypes.c_uint64

@@ -324,42 +324,9 @@ __global__ void blurT_edges_kernel(const float* __restrict__ g, float* __restric
 
 // ---- host ---------------------------------------------------------------------
 
-struct Workspace {
-    std::mutex mu;
-    struct E {
-        int dev;
-        cudaStream_t s;
-        void* p;
-        size_t bytes;
-    };
-    std::vector<E> v;
-};
-Workspace g_ws;
+StreamCache g_ws("adjoint workspace");
 
-int workspace(cudaStream_t s, size_t bytes, void** out) {
-    if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, "injected allocation failure (adjoint workspace)");
-    int dev = 0;
-    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
-    std::lock_guard<std::mutex> lock(g_ws.mu);
-    for (auto& e : g_ws.v)
-        if (e.dev == dev && e.s == s) {
-            if (e.bytes < bytes) {
-                IMOPS_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-                IMOPS_CUDA_TRY(cudaFree(e.p), "cudaFree");
-                e.p = nullptr;
-                e.bytes = 0;
-                IMOPS_CUDA_TRY(cudaMalloc(&e.p, bytes), "cudaMalloc(adjoint workspace)");
-                e.bytes = bytes;
-            }
-            *out = e.p;
-            return IMOPS_OK;
-        }
-    void* p = nullptr;
-    IMOPS_CUDA_TRY(cudaMalloc(&p, bytes), "cudaMalloc(adjoint workspace)");
-    g_ws.v.push_back({dev, s, p, bytes});
-    *out = p;
-    return IMOPS_OK;
-}
+int workspace(cudaStream_t s, size_t bytes, void** out) { return g_ws.get(s, bytes, out); }
 
 struct Arena {
     char* base;

@@ -92,6 +92,64 @@ int sm_count() {
     return cached[dev];
 }
 
+namespace {
+std::mutex g_caches_mu;
+std::vector<StreamCache*>& caches() {
+    static std::vector<StreamCache*> v;
+    return v;
+}
+}  // namespace
+
+StreamCache::StreamCache(const char* what) : what_(what) {
+    std::lock_guard<std::mutex> lock(g_caches_mu);
+    caches().push_back(this);
+}
+
+int StreamCache::get(cudaStream_t s, size_t bytes, void** out) {
+    if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, std::string("injected allocation failure (") + what_ + ")");
+    int dev = 0;
+    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    const std::string m = std::string("cudaMalloc(") + what_ + ")";
+    std::lock_guard<std::mutex> lock(mu_);
+    for (auto& e : v_)
+        if (e.dev == dev && e.s == s) {
+            if (e.bytes < bytes) {
+                IMOPS_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+                IMOPS_CUDA_TRY(cudaFree(e.p), "cudaFree");
+                e.p = nullptr;
+                e.bytes = 0;
+                IMOPS_CUDA_TRY(cudaMalloc(&e.p, bytes), m.c_str());
+                e.bytes = bytes;
+            }
+            *out = e.p;
+            return IMOPS_OK;
+        }
+    void* p = nullptr;
+    IMOPS_CUDA_TRY(cudaMalloc(&p, bytes), m.c_str());
+    v_.push_back({dev, s, p, bytes});
+    *out = p;
+    return IMOPS_OK;
+}
+
+void StreamCache::release_device(int dev) {
+    std::lock_guard<std::mutex> lock(mu_);
+    for (size_t k = 0; k < v_.size();) {
+        if (v_[k].dev == dev) {
+            if (v_[k].p) cudaFree(v_[k].p);
+            v_.erase(v_.begin() + k);
+        } else {
+            k++;
+        }
+    }
+}
+
+int release_working_sets(int dev) {
+    IMOPS_CUDA_TRY(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    std::lock_guard<std::mutex> lock(g_caches_mu);
+    for (StreamCache* c : caches()) c->release_device(dev);
+    return IMOPS_OK;
+}
+
 static std::atomic<uint64_t> g_launches{0};
 
 void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
@@ -109,3 +167,10 @@ extern "C" const char* imops_last_error(void) { return imops::last_error(); }
 extern "C" uint64_t imops_launch_count(void) { return imops::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" const char* imops_version(void) { return "imops_b200 0.1.0 (sm_100a)"; }
+
+extern "C" int imops_release_working_sets(void) {
+    imops::clear_error();
+    int dev = 0;
+    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    return imops::release_working_sets(dev);
+}

@@ -5,7 +5,10 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "imops_b200.h"
 
@@ -89,5 +92,33 @@ void note_launch(int n = 1);
 // variable IMOPS_FAULT_INJECT names `site` ("alloc", "launch"), the call
 // reports a failure instead of touching the GPU.
 bool fault_injected(const char* site);
+
+// A device buffer per (device, stream), grown on demand: the working sets of
+// the film, adjoint, X-Trans and fused-develop paths.  Growing waits for the
+// stream, frees the old buffer and allocates the new one.  Every cache
+// registers itself, so imops_release_working_sets can free them all.
+class StreamCache {
+   public:
+    explicit StreamCache(const char* what);
+    // The buffer of the current device and stream s, at least `bytes` long
+    // (fault site "alloc").
+    int get(cudaStream_t s, size_t bytes, void** out);
+    // Frees every buffer of device `dev`; its work must have finished.
+    void release_device(int dev);
+
+   private:
+    struct E {
+        int dev;
+        cudaStream_t s;
+        void* p;
+        size_t bytes;
+    };
+    const char* what_;
+    std::mutex mu_;
+    std::vector<E> v_;
+};
+
+// Frees the working sets of every cache on device `dev` (after waiting for it).
+int release_working_sets(int dev);
 
 }  // namespace imops

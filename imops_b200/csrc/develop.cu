@@ -12,41 +12,13 @@ namespace imops {
 namespace develop {
 
 // small per-stream buffer for the Markesteijn path's scaled mosaic
-struct Buf {
-    std::mutex mu;
-    struct E {
-        int dev;
-        cudaStream_t s;
-        void* p;
-        size_t bytes;
-    };
-    std::vector<E> v;
-};
-Buf g_buf;
+StreamCache g_buf("mosaic buffer");
 
 int mosaic_buffer(cudaStream_t s, size_t bytes, float** out) {
-    if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, "injected allocation failure (mosaic buffer)");
-    int dev = 0;
-    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
-    std::lock_guard<std::mutex> lock(g_buf.mu);
-    for (auto& e : g_buf.v)
-        if (e.dev == dev && e.s == s) {
-            if (e.bytes < bytes) {
-                IMOPS_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-                IMOPS_CUDA_TRY(cudaFree(e.p), "cudaFree");
-                e.p = nullptr;
-                e.bytes = 0;
-                IMOPS_CUDA_TRY(cudaMalloc(&e.p, bytes), "cudaMalloc(mosaic buffer)");
-                e.bytes = bytes;
-            }
-            *out = static_cast<float*>(e.p);
-            return IMOPS_OK;
-        }
     void* p = nullptr;
-    IMOPS_CUDA_TRY(cudaMalloc(&p, bytes), "cudaMalloc(mosaic buffer)");
-    g_buf.v.push_back({dev, s, p, bytes});
+    int rc = g_buf.get(s, bytes, &p);
     *out = static_cast<float*>(p);
-    return IMOPS_OK;
+    return rc;
 }
 
 int make_epilogue(const ImopsDevelopParams& P, color::Epilogue* e) {

@@ -805,42 +805,9 @@ static void build_base81(const Stock& st, Base81* hp) {
 // ---------------------------------------------------------------------------
 // workspace (per device+stream, grows on demand)
 
-struct Workspace {
-    std::mutex mu;
-    struct Entry {
-        int dev;
-        cudaStream_t s;
-        void* p;
-        size_t bytes;
-    };
-    std::vector<Entry> v;
-};
-Workspace g_ws;
+StreamCache g_ws("film workspace");
 
-int workspace(cudaStream_t s, size_t bytes, void** out) {
-    if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, "injected allocation failure (film workspace)");
-    int dev = 0;
-    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
-    std::lock_guard<std::mutex> lock(g_ws.mu);
-    for (auto& e : g_ws.v)
-        if (e.dev == dev && e.s == s) {
-            if (e.bytes < bytes) {
-                IMOPS_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-                IMOPS_CUDA_TRY(cudaFree(e.p), "cudaFree(film workspace)");
-                e.p = nullptr;
-                e.bytes = 0;
-                IMOPS_CUDA_TRY(cudaMalloc(&e.p, bytes), "cudaMalloc(film workspace)");
-                e.bytes = bytes;
-            }
-            *out = e.p;
-            return IMOPS_OK;
-        }
-    void* p = nullptr;
-    IMOPS_CUDA_TRY(cudaMalloc(&p, bytes), "cudaMalloc(film workspace)");
-    g_ws.v.push_back({dev, s, p, bytes});
-    *out = p;
-    return IMOPS_OK;
-}
+int workspace(cudaStream_t s, size_t bytes, void** out) { return g_ws.get(s, bytes, out); }
 
 int grid_for(size_t n) {
     size_t g = (n + 255) / 256, cap = (size_t)sm_count() * 8;

@@ -20,9 +20,6 @@
 // re-read their neighbours from L1/L2.  Built with --fmad=false: the same
 // IEEE f32 operations in the same order as the oracle, including its cube
 // root (Newton's method from an exponent-divided-by-3 first guess).
-#include <mutex>
-#include <vector>
-
 #include "common.cuh"
 
 namespace imops {
@@ -292,38 +289,13 @@ __global__ void vote_kernel(const __grid_constant__ Img im, const float* __restr
 }
 
 // per (device, stream) working planes, grown on demand
-struct Ws {
-    int dev;
-    cudaStream_t s;
-    float* p;
-    size_t bytes;
-};
-std::mutex g_mu;
-std::vector<Ws> g_ws;
+StreamCache g_ws("X-Trans planes");
 
 int workspace(cudaStream_t s, size_t bytes, float** out) {
-    if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, "injected allocation failure (X-Trans planes)");
-    int dev = 0;
-    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
-    std::lock_guard<std::mutex> lock(g_mu);
-    for (auto& e : g_ws)
-        if (e.dev == dev && e.s == s) {
-            if (e.bytes < bytes) {
-                IMOPS_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-                IMOPS_CUDA_TRY(cudaFree(e.p), "cudaFree(X-Trans planes)");
-                e.p = nullptr;
-                e.bytes = 0;
-                IMOPS_CUDA_TRY(cudaMalloc(&e.p, bytes), "cudaMalloc(X-Trans planes)");
-                e.bytes = bytes;
-            }
-            *out = e.p;
-            return IMOPS_OK;
-        }
-    float* p = nullptr;
-    IMOPS_CUDA_TRY(cudaMalloc(&p, bytes), "cudaMalloc(X-Trans planes)");
-    g_ws.push_back({dev, s, p, bytes});
-    *out = p;
-    return IMOPS_OK;
+    void* p = nullptr;
+    int rc = g_ws.get(s, bytes, &p);
+    *out = static_cast<float*>(p);
+    return rc;
 }
 
 }  // namespace xtrans

@@ -69,6 +69,14 @@ const char *imops_last_error(void);
 /* Library version string. */
 const char *imops_version(void);
 
+/* Frees the working sets the stage entry points cache per (device, stream)
+ * on the current device (film, adjoint, X-Trans planes, the fused develop's
+ * mosaic buffer), after waiting for the device; the next call allocates
+ * again.  No counterpart in the reference (its buffers are Rust Vecs freed
+ * with each module).  Call it when no work of this library is in flight on
+ * the device from another thread. */
+int imops_release_working_sets(void);
+
 /* ---- decode-side normalisation ------------------------------------------
  * Black/white scaling of a u16 sensor frame plus the crop copy.  Replaces
  * RawImage::apply_scaling (rawler 0.7, called at extern_pipeline.rs:263) and

@@ -103,3 +103,22 @@ def test_injected_failures_in_xtrans_and_display(gpu, monkeypatch):
     b = im.sigmoid_tone_map(x.clone())
     torch.cuda.synchronize()
     assert torch.equal(a, b)
+
+
+def test_release_working_sets_then_reuse(gpu):
+    """Freeing the cached working sets between calls changes no result."""
+    import torch
+
+    import imops_b200 as im
+    from imops_b200 import synthetic
+    x = _rgb(gpu)
+    a = im.film_process(x.clone(), stock=im.STOCK_BASELINE81)
+    m = torch.from_numpy(synthetic.mosaic_f32(96, 120, seed=4, pattern=synthetic.XTRANS)).to(gpu)
+    xa = im.demosaic_markesteijn3(m, synthetic.XTRANS)
+    torch.cuda.synchronize()
+    im.release_working_sets()
+    b = im.film_process(x.clone(), stock=im.STOCK_BASELINE81)
+    xb = im.demosaic_markesteijn3(m, synthetic.XTRANS)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b) and torch.equal(xa, xb)
+    im.release_working_sets()
