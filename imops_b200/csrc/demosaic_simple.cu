@@ -2,25 +2,27 @@
 // pichromatic/src/demosaic.rs:108-186) and the quad-sampling previews
 // (Fast / SuperFast / SuperSuperFast, demosaic.rs:189-356).
 //
-// The mean is HBM-bound (4 B in, 12 B out per pixel): one thread per
-// output pixel, a 32x8 block so each warp reads 34 consecutive floats of the
-// three rows it needs (coalesced, re-read from L1), CFA colours from a
-// kernel-parameter period table.  Built with --fmad=false: sums and the
-// final division round exactly as the reference's f32 code.
+// The mean is HBM-bound (4 B in, 12 B out per pixel).  Every Bayer CFA is a
+// shift of RGGB and every X-Trans sensor's CFA a shift of one 6x6 pattern, so
+// for those the kernel aligns each thread's run of pixels with the pattern:
+// the colour of every site in a run's window is then a compile-time constant
+// (per row phase, and a warp handles one row), the per-colour sums are plain
+// adds and the counts constants.  Other CFAs take the per-pixel kernel.  Both
+// sum each colour's sites in row-major order and divide once, as the
+// reference's f32 code does; built with --fmad=false.
 #include "common.cuh"
 
 namespace imops {
 namespace simple {
 
-// Cfa: CfaFixed<2, 2> / CfaFixed<6, 6> (modulo by a constant) for Bayer and
+// One output pixel: the mean of each colour's sites among the 8 neighbours
+// (the window clamped at the image edges), the centre's own colour keeping
+// the centre sample.  Cfa: CfaFixed<2, 2> / CfaFixed<6, 6> for Bayer and
 // X-Trans, CfaDev for other periods; coordinates here are never negative.
 template <class Cfa>
-__global__ void mean3x3_kernel(const float* __restrict__ in, int W, int H, const __grid_constant__ Cfa cfa,
-                               float* __restrict__ out) {
-    int col = blockIdx.x * blockDim.x + threadIdx.x;
-    int row = blockIdx.y * blockDim.y + threadIdx.y;
-    if (col >= W || row >= H) return;
-    int centre = cfa.at(row, col);
+__device__ __forceinline__ void mean_px(const float* __restrict__ in, int W, int H, const Cfa& cfa, int row,
+                                        int col, float* o) {
+    const int centre = cfa.at(row, col);
     if (row >= 1 && row + 1 < H && col >= 1 && col + 1 < W) {
         // interior: the whole 3x3 window, unrolled and branch-free; each
         // colour's sum takes its sites in row-major order (predicated adds)
@@ -41,7 +43,6 @@ __global__ void mean3x3_kernel(const float* __restrict__ in, int W, int H, const
                 n2 = k == 2 ? n2 + 1.0f : n2;
             }
         const float self = __ldg(in + (size_t)row * W + col);
-        float* o = out + ((size_t)row * W + col) * 3;
         o[0] = centre == 0 ? self : (n0 > 0.0f ? s0 / n0 : 0.0f);
         o[1] = centre == 1 ? self : (n1 > 0.0f ? s1 / n1 : 0.0f);
         o[2] = centre == 2 ? self : (n2 > 0.0f ? s2 / n2 : 0.0f);
@@ -69,14 +70,230 @@ __global__ void mean3x3_kernel(const float* __restrict__ in, int W, int H, const
             }
         }
     const float self = __ldg(in + (size_t)row * W + col);
+    o[0] = centre == 0 ? self : (n0 > 0.0f ? s0 / n0 : 0.0f);
+    o[1] = centre == 1 ? self : (n1 > 0.0f ? s1 / n1 : 0.0f);
+    o[2] = centre == 2 ? self : (n2 > 0.0f ? s2 / n2 : 0.0f);
+}
+
+// One thread per output pixel, for CFAs that are no shift of a canonical
+// pattern.
+template <class Cfa>
+__global__ void mean3x3_kernel(const float* __restrict__ in, int W, int H, const __grid_constant__ Cfa cfa,
+                               float* __restrict__ out) {
+    int col = blockIdx.x * blockDim.x + threadIdx.x;
+    int row = blockIdx.y * blockDim.y + threadIdx.y;
+    if (col >= W || row >= H) return;
     float v[3];
-    v[0] = centre == 0 ? self : (n0 > 0.0f ? s0 / n0 : 0.0f);
-    v[1] = centre == 1 ? self : (n1 > 0.0f ? s1 / n1 : 0.0f);
-    v[2] = centre == 2 ? self : (n2 > 0.0f ? s2 / n2 : 0.0f);
+    mean_px(in, W, H, cfa, row, col, v);
     float* o = out + ((size_t)row * W + col) * 3;
     o[0] = v[0];
     o[1] = v[1];
     o[2] = v[2];
+}
+
+// Canonical patterns, colour codes as parse_cfa assigns them (R 0, G 1, B 2),
+// two bits a cell, packed at compile time.
+__host__ __device__ constexpr int colour_code(char ch) { return ch == 'R' ? 0 : ch == 'G' ? 1 : 2; }
+__host__ __device__ constexpr unsigned long long pack2(const char* p, int from, int n) {
+    unsigned long long v = 0ull;
+    for (int i = 0; i < n; i++) v |= (unsigned long long)colour_code(p[from + i]) << (2 * i);
+    return v;
+}
+struct BayerCanon {  // RGGB
+    static constexpr int PW = 2, PH = 2;
+    static constexpr unsigned long long LO = pack2("RGGB", 0, 4), HI = 0ull;
+    __host__ __device__ static constexpr int at(int r, int c) {
+        return (int)((r * PW + c < 18 ? LO >> (2 * (r * PW + c)) : HI >> (2 * (r * PW + c - 18))) & 3ull);
+    }
+};
+struct XTransCanon {  // the X-Trans sensors' 6x6 period
+    static constexpr int PW = 6, PH = 6;
+    static constexpr unsigned long long LO = pack2("GGRGGBGGBGGRBRGRBG", 0, 18);
+    static constexpr unsigned long long HI = pack2("GGBGGRGGRGGBRBGBRG", 0, 18);
+    __host__ __device__ static constexpr int at(int r, int c) {
+        return (int)((r * PW + c < 18 ? LO >> (2 * (r * PW + c)) : HI >> (2 * (r * PW + c - 18))) & 3ull);
+    }
+};
+
+// Phase-aligned kernel geometry: a warp handles one image row, RUN pixels a
+// lane, 32 * RUN pixels a warp; RUN is a multiple of both periods.
+constexpr int RUN = 6;
+constexpr int WARP_PX = 32 * RUN;              // 192
+constexpr int IN_STRIDE = WARP_PX + 4;         // 194 staged columns, padded to a 16-byte multiple
+constexpr int OUT_STRIDE = 3 * WARP_PX + 4;    // an RGB row and up to 3 floats of alignment offset
+constexpr int MEAN_WARPS = 8;
+
+// The RUN pixels of one lane at canonical row phase RP: window v = rows
+// y-1..y+1, columns x0-1..x0+RUN; pixel j sits at canonical column j mod PW.
+// Same adds in the same order as mean_px's interior branch, with the colour
+// tests and counts folded away.
+template <class P, int RP>
+__device__ __forceinline__ void run_aligned(const float (&v)[3][RUN + 2], float* o) {
+#pragma unroll
+    for (int j = 0; j < RUN; j++) {
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                if (a == 1 && b == 1) continue;
+                const int k = P::at((RP + a + P::PH - 1) % P::PH, (j + b + P::PW - 1) % P::PW);
+                const float x = v[a][j + b];
+                if (k == 0) {
+                    s0 = s0 + x;
+                    n0 = n0 + 1.0f;
+                } else if (k == 1) {
+                    s1 = s1 + x;
+                    n1 = n1 + 1.0f;
+                } else {
+                    s2 = s2 + x;
+                    n2 = n2 + 1.0f;
+                }
+            }
+        const int centre = P::at(RP, j % P::PW);
+        const float self = v[1][j + 1];
+        o[3 * j + 0] = centre == 0 ? self : (n0 > 0.0f ? s0 / n0 : 0.0f);
+        o[3 * j + 1] = centre == 1 ? self : (n1 > 0.0f ? s1 / n1 : 0.0f);
+        o[3 * j + 2] = centre == 2 ? self : (n2 > 0.0f ? s2 / n2 : 0.0f);
+    }
+}
+
+template <class P, int RP>
+__device__ __forceinline__ void run_phase(int rp, const float (&v)[3][RUN + 2], float* o) {
+    if constexpr (RP < P::PH) {
+        if (rp == RP) run_aligned<P, RP>(v, o);
+        else run_phase<P, RP + 1>(rp, v, o);
+    }
+}
+
+// The CFA is P shifted: colour(y, x) = P::at((y - oy) mod PH, (x - ox) mod PW)
+// with 0 <= ox < PW, 0 <= oy < PH.  Warp w of block (bx, by) develops row
+// y = 8 by + w, pixels x_start + 192 bx .. + 191 with x_start = 0 when
+// ox == 0 else ox - PW, so every lane's run starts at canonical column 0.
+// The warp stages its three rows in shared memory (coalesced loads), each
+// lane computes its run from there -- or, when the run or its window touches
+// the image edge, each pixel with mean_px -- into a shared output row that
+// the warp then stores coalesced.
+template <class P>
+__global__ void __launch_bounds__(32 * MEAN_WARPS) mean3x3_aligned_kernel(
+    const float* __restrict__ in, int W, int H, int ox, int oy, const __grid_constant__ CfaFixed<P::PW, P::PH> cfa,
+    float* __restrict__ out) {
+    __shared__ __align__(16) float sin_[MEAN_WARPS][3][IN_STRIDE];
+    __shared__ __align__(16) float sout[MEAN_WARPS][OUT_STRIDE];
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int y = blockIdx.y * MEAN_WARPS + w;
+    if (y >= H) return;  // whole warp: only warp-level synchronisation below
+    const int xs = ox == 0 ? 0 : ox - P::PW;
+    const int xw = xs + blockIdx.x * WARP_PX;  // first pixel of the warp
+    // stage rows y-1..y+1, columns xw-1 .. xw+192 (zeros outside the image;
+    // only runs whose window lies inside read them).  All 21 loads of a lane
+    // are issued before the first store, so a warp keeps them in flight
+    // together; warps whose rows lie inside the image skip the per-element
+    // tests.
+    constexpr int NQ = (WARP_PX + 2 + 31) / 32;
+    float t[3][NQ];
+    if (y >= 1 && y + 1 < H && xw >= 1 && xw + WARP_PX + 1 <= W) {
+        const float* src = in + (size_t)(y - 1) * W + (xw - 1) + lane;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int q = 0; q < NQ; q++)
+                t[a][q] = lane + 32 * q < WARP_PX + 2 ? __ldg(src + (size_t)a * W + 32 * q) : 0.0f;
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const int yy = y + a - 1;
+            const bool yin = yy >= 0 && yy < H;
+            const float* src = in + (size_t)(yin ? yy : 0) * W;
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const int i = lane + 32 * q, x = xw - 1 + i;
+                t[a][q] = yin && i < WARP_PX + 2 && x >= 0 && x < W ? __ldg(src + x) : 0.0f;
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int q = 0; q < NQ; q++)
+            if (lane + 32 * q < WARP_PX + 2) sin_[w][a][lane + 32 * q] = t[a][q];
+    __syncwarp();
+    // the warp's pixels inside the image, and the shared output row's offset
+    // m: float k of the row goes to address dst0 + (k - K0), and m makes
+    // shared and global 16-byte boundaries coincide
+    const int p0 = xw > 0 ? xw : 0, p1 = xw + WARP_PX < W ? xw + WARP_PX : W;
+    float* dst0 = out + ((size_t)y * W + p0) * 3;
+    const int m = ((int)(((uintptr_t)dst0 >> 2) & 3) - 3 * (p0 - xw)) & 3;
+    const int x0 = xw + RUN * lane;
+    float* o = &sout[w][m + 3 * RUN * lane];
+    if (y >= 1 && y + 1 < H && x0 >= 1 && x0 + RUN + 1 <= W) {
+        float v[3][RUN + 2];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int c = 0; c < RUN + 2; c += 2) {
+                const float2 t2 = *reinterpret_cast<const float2*>(&sin_[w][a][RUN * lane + c]);
+                v[a][c] = t2.x;
+                v[a][c + 1] = t2.y;
+            }
+        const int rp = (y + P::PH - oy) % P::PH;
+        float r[3 * RUN];
+        run_phase<P, 0>(rp, v, r);
+        if (m & 1) {
+#pragma unroll
+            for (int c = 0; c < 3 * RUN; c++) o[c] = r[c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3 * RUN; c += 2) *reinterpret_cast<float2*>(o + c) = make_float2(r[c], r[c + 1]);
+        }
+    } else {
+        for (int j = 0; j < RUN; j++) {
+            const int x = x0 + j;
+            if (x >= 0 && x < W) mean_px(in, W, H, cfa, y, x, o + 3 * j);
+        }
+    }
+    __syncwarp();
+    if (p1 <= p0) return;
+    // shared floats K0..K1-1 -> dst0: a scalar head up to a 16-byte boundary,
+    // float4 chunks, a scalar tail
+    const int K0 = m + 3 * (p0 - xw), K1 = m + 3 * (p1 - xw);
+    const int c0 = (K0 + 3) >> 2, c1 = K1 >> 2;
+    const float* so = sout[w];
+    if (c0 >= c1) {
+        for (int k = K0 + lane; k < K1; k += 32) dst0[k - K0] = so[k];
+        return;
+    }
+    if (K0 + lane < 4 * c0) dst0[lane] = so[K0 + lane];
+    for (int c = c0 + lane; c < c1; c += 32)
+        *reinterpret_cast<float4*>(dst0 + (4 * c - K0)) = *reinterpret_cast<const float4*>(so + 4 * c);
+    if (4 * c1 + lane < K1) dst0[4 * c1 + lane - K0] = so[4 * c1 + lane];
+}
+
+// (ox, oy) with colour(y, x) == P::at((y - oy) mod PH, (x - ox) mod PW) for
+// every site of c's period, or false when c is no shift of P.
+template <class P>
+bool canonical_offset(const CfaDev& c, int* ox, int* oy) {
+    if (c.pw != P::PW || c.ph != P::PH) return false;
+    for (int dy = 0; dy < P::PH; dy++)
+        for (int dx = 0; dx < P::PW; dx++) {
+            bool ok = true;
+            for (int r = 0; r < P::PH && ok; r++)
+                for (int q = 0; q < P::PW && ok; q++)
+                    ok = c.col[r * P::PW + q] == P::at((r - dy + P::PH) % P::PH, (q - dx + P::PW) % P::PW);
+            if (ok) {
+                *ox = dx;
+                *oy = dy;
+                return true;
+            }
+        }
+    return false;
+}
+
+template <class P>
+void launch_aligned(const float* mosaic, int w, int h, const CfaDev& c, int ox, int oy, float* rgb, cudaStream_t s) {
+    const int xs = ox == 0 ? 0 : ox - P::PW;
+    dim3 block(32, MEAN_WARPS), grid((w - xs + WARP_PX - 1) / WARP_PX, (h + MEAN_WARPS - 1) / MEAN_WARPS);
+    mean3x3_aligned_kernel<P><<<grid, block, 0, s>>>(mosaic, w, h, ox, oy, CfaFixed<P::PW, P::PH>::from(c), rgb);
 }
 
 __global__ void quad_kernel(const float* __restrict__ in, int W, int nw, int nh, int factor, int4 cols,
@@ -107,11 +324,18 @@ extern "C" int imops_demosaic_markesteijn(const float* mosaic, int w, int h, con
     int rc = parse_cfa(cfa, shift_x, shift_y, &c);
     if (rc) return rc;
     if (!mosaic || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: NULL buffer");
+    if (((uintptr_t)mosaic | (uintptr_t)rgb) & 3)
+        return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: buffers must be 4-byte aligned float arrays");
     if (w <= 0 || h <= 0) return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: empty image");
     if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, "injected launch failure (markesteijn)");
     dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
     cudaStream_t s = as_stream(stream);
-    if (c.pw == 2 && c.ph == 2)
+    int ox, oy;
+    if (simple::canonical_offset<simple::BayerCanon>(c, &ox, &oy))
+        simple::launch_aligned<simple::BayerCanon>(mosaic, w, h, c, ox, oy, rgb, s);
+    else if (simple::canonical_offset<simple::XTransCanon>(c, &ox, &oy))
+        simple::launch_aligned<simple::XTransCanon>(mosaic, w, h, c, ox, oy, rgb, s);
+    else if (c.pw == 2 && c.ph == 2)
         simple::mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, CfaFixed<2, 2>::from(c), rgb);
     else if (c.pw == 6 && c.ph == 6)
         simple::mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, CfaFixed<6, 6>::from(c), rgb);

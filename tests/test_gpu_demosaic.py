@@ -127,6 +127,61 @@ def test_markesteijn_single_pixel_edges(oracle_lib, gpu):
         assert np.array_equal(out, ref), shape
 
 
+@pytest.mark.parametrize("sx", range(6))
+@pytest.mark.parametrize("sy", range(6))
+def test_markesteijn_xtrans_phases_several_warps(oracle_lib, gpu, sx, sy):
+    """Rows wider than one warp's 192-pixel span and an odd height: every
+    phase alignment of the warps' runs against the image edges."""
+    import torch
+    import imops_b200 as im
+    rng = np.random.default_rng(100 + sx * 6 + sy)
+    m = rng.random((29, 401), dtype=np.float32)
+    ref = oracle_lib.mean3x3(m, synthetic.XTRANS, shift=(sx, sy))
+    out = im.demosaic_markesteijn(torch.from_numpy(m).to(gpu), synthetic.XTRANS, shift=(sx, sy)).cpu().numpy()
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("shift", BAYER_SHIFTS)
+def test_markesteijn_bayer_several_warps(oracle_lib, gpu, shift):
+    import torch
+    import imops_b200 as im
+    m = synthetic.mosaic_f32(31, 579, seed=6)
+    ref = oracle_lib.mean3x3(m, "RGGB", shift=shift)
+    out = im.demosaic_markesteijn(torch.from_numpy(m).to(gpu), "RGGB", shift=shift).cpu().numpy()
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("pattern", ["RBGGRGBGGRGBGBRGGRRGBGGBGRBGGRGBGRGG", "RGBG", "RGEB",
+                                     "GGRGGBGGBGGRBRGRBGGGBGGRGGRGGBRBGBEG"])
+def test_markesteijn_other_cfas(oracle_lib, gpu, pattern):
+    """CFAs that are no shift of RGGB or of the X-Trans period (a scrambled
+    6x6, greens on one row, a fourth colour) take the per-pixel kernel."""
+    import torch
+    import imops_b200 as im
+    rng = np.random.default_rng(len(pattern))
+    m = rng.random((27, 230), dtype=np.float32)
+    ref = oracle_lib.mean3x3(m, pattern)
+    out = im.demosaic_markesteijn(torch.from_numpy(m).to(gpu), pattern).cpu().numpy()
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("pattern", [synthetic.XTRANS, "RGGB"])
+def test_markesteijn_non_finite_samples(oracle_lib, gpu, pattern):
+    """NaN and infinite samples reach only the sums of their own colour, as in
+    the reference's per-colour loops."""
+    import torch
+    import imops_b200 as im
+    rng = np.random.default_rng(3)
+    m = rng.random((40, 300), dtype=np.float32)
+    idx = rng.choice(m.size, 60, replace=False)
+    m.flat[idx[:20]] = np.nan
+    m.flat[idx[20:40]] = np.inf
+    m.flat[idx[40:]] = -np.inf
+    ref = oracle_lib.mean3x3(m, pattern)
+    out = im.demosaic_markesteijn(torch.from_numpy(m).to(gpu), pattern).cpu().numpy()
+    np.testing.assert_array_equal(out, ref)
+
+
 @pytest.mark.parametrize("factor", [2, 4, 8])
 def test_quad_previews(oracle_lib, gpu, factor):
     import torch
