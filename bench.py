@@ -405,9 +405,31 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_e2e = float(t.item())
 
+    # the box's host link: plain pinned copies of one frame's RGB in each
+    # direction (CUDA events on a side stream), and the frame rate they and
+    # the kernels allow when upload, kernels and download overlap
+    def link_gbs(dst, src):
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            dst.copy_(src, non_blocking=True)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            for _ in range(3):
+                dst.copy_(src, non_blocking=True)
+            b.record(s)
+        b.synchronize()
+        return 3 * src.numel() * src.element_size() / (a.elapsed_time(b) / 1e3) / 1e9
+
+    rgb_d = torch.empty(H * W * 3, dtype=torch.float32, device=dev)
+    d2h_gbs = link_gbs(rgb_h.view(-1), rgb_d)
+    h2d_gbs = link_gbs(rgb_d, rgb_h.view(-1))
+    del rgb_d
+    t_frame = max(H * W * 12 / (d2h_gbs * 1e9), H * W * 2 / (h2d_gbs * 1e9), t_total / args.steps / 1e3)
+
     mp = H * W / 1e6
     value = world * mp * args.steps / (t_total / 1e3)
     e2e = world * mp * args.steps / (t_e2e / 1e3)
+    e2e_bound = world * mp / t_frame
     fwd_bwd = world * mp * args.steps / (t_fb / 1e3)
     bw, peak_kind = peaks()
     dom_bytes = H * W * 14  # u16 mosaic in (2 B) + f32 RGB out (12 B) per pixel
@@ -439,7 +461,11 @@ def main():
                     "d2h_bytes_per_step": H * W * 12, "api": "new_raw_image_u16_c + run_pixel_pipeline_c + "
                     "get_image_rgb_f32_c per frame; one host thread uploads and submits, a second reads the frames "
                     "back, so upload, kernels and download of consecutive frames overlap (pinned host buffers, host "
-                    "clock)"},
+                    "clock)",
+                    "link": {"d2h_gbs": round(d2h_gbs, 2), "h2d_gbs": round(h2d_gbs, 2),
+                             "bound_mp_s": round(e2e_bound, 2), "frac_of_bound": round(e2e / e2e_bound, 3),
+                             "note": "plain pinned copies of one frame's f32 RGB on this box; the bound is the "
+                                     "slowest of download, upload and kernels per frame"}},
             "gpu_launches": int(launches),
             "clocks": clk_summary,
         }

@@ -82,6 +82,48 @@ def test_develop_matches_oracle_chain(oracle_lib, gpu):
     assert np.abs(out - ref).max() < 1e-4
 
 
+LSB = 1.0 / 65535.0  # one 16-bit step of linear [0, 1]
+FLIP_LSB = 8.0  # errors above this are AMaZE taking another branch in f32 than in f64
+
+
+def test_forward_error_vs_fp64_in_lsb(oracle_lib, gpu):
+    """Error of the forward against the FP64 oracle chain, in 16-bit LSB.  The
+    colour forward (AMaZE + WB + camera matrix) equals the reference-order
+    f32 chain bit for bit, so its error is the reference's own f32 error: a
+    few pixels where a comparison in AMaZE resolves differently in f32 than in
+    f64 (decision flips, counted separately), sub-LSB elsewhere.  The film
+    forward (81-bin baseline, grain on) adds its f32 kernels' error."""
+    import torch
+    import imops_b200 as im
+    H, W = 480, 768
+    raw_np = synthetic.mosaic_u16(H, W, seed=31)
+    raw = torch.from_numpy(raw_np.view(np.int16)).to(gpu)
+
+    def chain(prec):
+        m = oracle_lib.scale_u16(raw_np, (0, 0, W, H), synthetic.BLACK, synthetic.WHITE, precision=prec)
+        rgb = oracle_lib.wb(oracle_lib.amaze(m, "RGGB", precision=prec), synthetic.WB, precision=prec)
+        return oracle_lib.camera_cst(rgb, synthetic.CALIB_D65, oracle_lib.CS_ACESCG, precision=prec)
+
+    c32, c64 = chain("f32"), chain("f64")
+    colour = im.develop_u16(raw, (0, 0, W, H), synthetic.BLACK, synthetic.WHITE, _params(im, False)).cpu().numpy()
+    assert np.array_equal(colour, c32)
+    e = np.abs(colour.astype(np.float64) - c64) / LSB
+    flip = e.max(axis=2) > FLIP_LSB
+    ok = ~flip
+    film = im.develop_u16(raw, (0, 0, W, H), synthetic.BLACK, synthetic.WHITE, _params(im, True)).cpu().numpy()
+    f64 = oracle_lib.film_baseline(c64, oracle_lib.baseline_params(seed=3), precision="f64")
+    ef = np.abs(film.astype(np.float64) - f64) / LSB
+    figures = {
+        "pixels": H * W, "colour_flips": int(flip.sum()), "colour_max_lsb": float(e[ok].max()),
+        "colour_rms_lsb": float(np.sqrt((e[ok] ** 2).mean())), "film_max_lsb": float(ef[ok].max()),
+        "film_rms_lsb": float(np.sqrt((ef[ok] ** 2).mean())), "film_max_lsb_all": float(ef.max()),
+    }
+    print("forward vs FP64:", figures)
+    assert flip.sum() <= 5e-4 * H * W
+    assert figures["colour_rms_lsb"] < 0.1
+    assert figures["film_max_lsb"] < 10.0 and figures["film_rms_lsb"] < 0.5
+
+
 def test_develop_film_requires_acescg(gpu):
     import torch
     import imops_b200 as im
