@@ -107,16 +107,47 @@ struct Levels {
     float v[288];
 };
 
-__global__ void scale_u16_kernel_p(const uint16_t* __restrict__ raw, int raw_w, int cx, int cy, int cw, int ch,
-                                   int pw, int ph, Levels lv, float* __restrict__ out) {
-    size_t n = (size_t)cw * ch;
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-        int y = (int)(k / cw), x = (int)(k % cw);
-        int sy = cy + y, sx = cx + x;
-        int site = (sy % ph) * pw + (sx % pw);
-        float v = (float)__ldg(raw + (size_t)sy * raw_w + sx);
-        float bl = lv.v[site], wh = lv.v[144 + site];
-        out[k] = (v - bl) / (wh - bl);
+// One thread per column, SCALE_ROWS rows: the CFA site's column is found
+// once and its row stepped, the levels are read from shared memory.  A full
+// group of rows issues all its loads before the first division, so a thread
+// keeps SCALE_ROWS loads in flight.
+constexpr int SCALE_ROWS = 16;
+
+__global__ void scale_u16_kernel(const uint16_t* __restrict__ raw, int raw_w, int cx, int cy, int cw, int ch, int pw,
+                                 int ph, const __grid_constant__ Levels lv, float* __restrict__ out) {
+    __shared__ float sl[288];
+    for (int i = threadIdx.x; i < pw * ph; i += blockDim.x) {
+        sl[i] = lv.v[i];
+        sl[144 + i] = lv.v[144 + i];
+    }
+    __syncthreads();
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y0 = blockIdx.y * SCALE_ROWS;
+    if (x >= cw) return;
+    const int sx = cx + x, col = sx % pw;
+    int rowph = (cy + y0) % ph;
+    const uint16_t* src = raw + (size_t)(cy + y0) * raw_w + sx;
+    float* dst = out + (size_t)y0 * cw + x;
+    const int rows = ch - y0 < SCALE_ROWS ? ch - y0 : SCALE_ROWS;
+    if (rows == SCALE_ROWS) {
+        float v[SCALE_ROWS];
+#pragma unroll
+        for (int r = 0; r < SCALE_ROWS; r++) v[r] = (float)__ldg(src + (size_t)r * raw_w);
+#pragma unroll
+        for (int r = 0; r < SCALE_ROWS; r++) {
+            const int site = rowph * pw + col;
+            const float bl = sl[site], wh = sl[144 + site];
+            dst[(size_t)r * cw] = (v[r] - bl) / (wh - bl);
+            rowph = rowph + 1 == ph ? 0 : rowph + 1;
+        }
+        return;
+    }
+    for (int r = 0; r < rows; r++) {
+        const int site = rowph * pw + col;
+        const float v = (float)__ldg(src + (size_t)r * raw_w);
+        const float bl = sl[site], wh = sl[144 + site];
+        dst[(size_t)r * cw] = (v - bl) / (wh - bl);
+        rowph = rowph + 1 == ph ? 0 : rowph + 1;
     }
 }
 
@@ -168,9 +199,9 @@ extern "C" int imops_scale_u16(const uint16_t* raw, int raw_w, int raw_h, int cr
         lv.v[i] = black[i];
         lv.v[144 + i] = white[i];
     }
-    size_t n = (size_t)crop_w * crop_h;
-    color::scale_u16_kernel_p<<<color::stream_grid(n, 256), 256, 0, as_stream(stream)>>>(
-        raw, raw_w, crop_x, crop_y, crop_w, crop_h, period_w, period_h, lv, out);
+    dim3 grid((crop_w + 255) / 256, (crop_h + color::SCALE_ROWS - 1) / color::SCALE_ROWS);
+    color::scale_u16_kernel<<<grid, 256, 0, as_stream(stream)>>>(raw, raw_w, crop_x, crop_y, crop_w, crop_h,
+                                                                  period_w, period_h, lv, out);
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "scale_u16 launch");
     return IMOPS_OK;

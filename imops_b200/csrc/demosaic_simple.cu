@@ -10,7 +10,9 @@
 // adds and the counts constants.  Other CFAs take the per-pixel kernel.  Both
 // sum each colour's sites in row-major order and divide once, as the
 // reference's f32 code does; built with --fmad=false.
+#include "color.cuh"
 #include "common.cuh"
+#include "demosaic_simple.cuh"
 
 namespace imops {
 namespace simple {
@@ -75,16 +77,23 @@ __device__ __forceinline__ void mean_px(const float* __restrict__ in, int W, int
     o[2] = centre == 2 ? self : (n2 > 0.0f ? s2 / n2 : 0.0f);
 }
 
+// The mean alone.
+struct NoEpilogue {
+    __device__ __forceinline__ void apply(float&, float&, float&) const {}
+};
+
 // One thread per output pixel, for CFAs that are no shift of a canonical
-// pattern.
-template <class Cfa>
+// pattern; epi (NoEpilogue or color::Epilogue) maps each pixel's RGB before
+// the store.
+template <class Cfa, class Epi>
 __global__ void mean3x3_kernel(const float* __restrict__ in, int W, int H, const __grid_constant__ Cfa cfa,
-                               float* __restrict__ out) {
+                               const __grid_constant__ Epi epi, float* __restrict__ out) {
     int col = blockIdx.x * blockDim.x + threadIdx.x;
     int row = blockIdx.y * blockDim.y + threadIdx.y;
     if (col >= W || row >= H) return;
     float v[3];
     mean_px(in, W, H, cfa, row, col, v);
+    epi.apply(v[0], v[1], v[2]);
     float* o = out + ((size_t)row * W + col) * 3;
     o[0] = v[0];
     o[1] = v[1];
@@ -174,10 +183,10 @@ __device__ __forceinline__ void run_phase(int rp, const float (&v)[3][RUN + 2], 
 // lane computes its run from there -- or, when the run or its window touches
 // the image edge, each pixel with mean_px -- into a shared output row that
 // the warp then stores coalesced.
-template <class P>
+template <class P, class Epi>
 __global__ void __launch_bounds__(32 * MEAN_WARPS) mean3x3_aligned_kernel(
     const float* __restrict__ in, int W, int H, int ox, int oy, const __grid_constant__ CfaFixed<P::PW, P::PH> cfa,
-    float* __restrict__ out) {
+    const __grid_constant__ Epi epi, float* __restrict__ out) {
     __shared__ __align__(16) float sin_[MEAN_WARPS][3][IN_STRIDE];
     __shared__ __align__(16) float sout[MEAN_WARPS][OUT_STRIDE];
     const int lane = threadIdx.x, w = threadIdx.y;
@@ -239,6 +248,8 @@ __global__ void __launch_bounds__(32 * MEAN_WARPS) mean3x3_aligned_kernel(
         const int rp = (y + P::PH - oy) % P::PH;
         float r[3 * RUN];
         run_phase<P, 0>(rp, v, r);
+#pragma unroll
+        for (int j = 0; j < RUN; j++) epi.apply(r[3 * j], r[3 * j + 1], r[3 * j + 2]);
         if (m & 1) {
 #pragma unroll
             for (int c = 0; c < 3 * RUN; c++) o[c] = r[c];
@@ -249,7 +260,14 @@ __global__ void __launch_bounds__(32 * MEAN_WARPS) mean3x3_aligned_kernel(
     } else {
         for (int j = 0; j < RUN; j++) {
             const int x = x0 + j;
-            if (x >= 0 && x < W) mean_px(in, W, H, cfa, y, x, o + 3 * j);
+            if (x >= 0 && x < W) {
+                float q[3];
+                mean_px(in, W, H, cfa, y, x, q);
+                epi.apply(q[0], q[1], q[2]);
+                o[3 * j] = q[0];
+                o[3 * j + 1] = q[1];
+                o[3 * j + 2] = q[2];
+            }
         }
     }
     __syncwarp();
@@ -289,11 +307,43 @@ bool canonical_offset(const CfaDev& c, int* ox, int* oy) {
     return false;
 }
 
-template <class P>
-void launch_aligned(const float* mosaic, int w, int h, const CfaDev& c, int ox, int oy, float* rgb, cudaStream_t s) {
+template <class P, class Epi>
+void launch_aligned(const float* mosaic, int w, int h, const CfaDev& c, int ox, int oy, const Epi& epi, float* rgb,
+                    cudaStream_t s) {
     const int xs = ox == 0 ? 0 : ox - P::PW;
     dim3 block(32, MEAN_WARPS), grid((w - xs + WARP_PX - 1) / WARP_PX, (h + MEAN_WARPS - 1) / MEAN_WARPS);
-    mean3x3_aligned_kernel<P><<<grid, block, 0, s>>>(mosaic, w, h, ox, oy, CfaFixed<P::PW, P::PH>::from(c), rgb);
+    mean3x3_aligned_kernel<P, Epi><<<grid, block, 0, s>>>(mosaic, w, h, ox, oy, CfaFixed<P::PW, P::PH>::from(c), epi,
+                                                          rgb);
+}
+
+template <class Epi>
+void launch_mean(const float* mosaic, int w, int h, const CfaDev& c, const Epi& epi, float* rgb, cudaStream_t s) {
+    dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
+    int ox, oy;
+    if (canonical_offset<BayerCanon>(c, &ox, &oy))
+        launch_aligned<BayerCanon>(mosaic, w, h, c, ox, oy, epi, rgb, s);
+    else if (canonical_offset<XTransCanon>(c, &ox, &oy))
+        launch_aligned<XTransCanon>(mosaic, w, h, c, ox, oy, epi, rgb, s);
+    else if (c.pw == 2 && c.ph == 2)
+        mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, CfaFixed<2, 2>::from(c), epi, rgb);
+    else if (c.pw == 6 && c.ph == 6)
+        mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, CfaFixed<6, 6>::from(c), epi, rgb);
+    else
+        mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, c, epi, rgb);
+}
+
+int mean3x3(const float* mosaic, int w, int h, const CfaDev& c, const color::Epilogue* epi, float* rgb,
+            cudaStream_t s) {
+    if (!mosaic || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: NULL buffer");
+    if (((uintptr_t)mosaic | (uintptr_t)rgb) & 3)
+        return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: buffers must be 4-byte aligned float arrays");
+    if (w <= 0 || h <= 0) return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: empty image");
+    if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, "injected launch failure (markesteijn)");
+    if (epi) launch_mean(mosaic, w, h, c, *epi, rgb, s);
+    else launch_mean(mosaic, w, h, c, NoEpilogue{}, rgb, s);
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "markesteijn launch");
+    return IMOPS_OK;
 }
 
 __global__ void quad_kernel(const float* __restrict__ in, int W, int nw, int nh, int factor, int4 cols,
@@ -323,27 +373,7 @@ extern "C" int imops_demosaic_markesteijn(const float* mosaic, int w, int h, con
     CfaDev c;
     int rc = parse_cfa(cfa, shift_x, shift_y, &c);
     if (rc) return rc;
-    if (!mosaic || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: NULL buffer");
-    if (((uintptr_t)mosaic | (uintptr_t)rgb) & 3)
-        return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: buffers must be 4-byte aligned float arrays");
-    if (w <= 0 || h <= 0) return fail(IMOPS_ERR_INVALID_ARGUMENT, "markesteijn: empty image");
-    if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, "injected launch failure (markesteijn)");
-    dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
-    cudaStream_t s = as_stream(stream);
-    int ox, oy;
-    if (simple::canonical_offset<simple::BayerCanon>(c, &ox, &oy))
-        simple::launch_aligned<simple::BayerCanon>(mosaic, w, h, c, ox, oy, rgb, s);
-    else if (simple::canonical_offset<simple::XTransCanon>(c, &ox, &oy))
-        simple::launch_aligned<simple::XTransCanon>(mosaic, w, h, c, ox, oy, rgb, s);
-    else if (c.pw == 2 && c.ph == 2)
-        simple::mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, CfaFixed<2, 2>::from(c), rgb);
-    else if (c.pw == 6 && c.ph == 6)
-        simple::mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, CfaFixed<6, 6>::from(c), rgb);
-    else
-        simple::mean3x3_kernel<<<grid, block, 0, s>>>(mosaic, w, h, c, rgb);
-    note_launch();
-    IMOPS_CUDA_TRY(cudaGetLastError(), "markesteijn launch");
-    return IMOPS_OK;
+    return simple::mean3x3(mosaic, w, h, c, nullptr, rgb, as_stream(stream));
 }
 
 extern "C" int imops_demosaic_quad(const float* mosaic, int w, int h, const char* cfa, int shift_x, int shift_y,

@@ -7,6 +7,7 @@
 
 #include "amaze.cuh"
 #include "color.cuh"
+#include "demosaic_simple.cuh"
 
 namespace imops {
 namespace develop {
@@ -70,8 +71,8 @@ extern "C" int imops_develop_u16(const uint16_t* raw, int raw_w, int raw_h, int 
         if ((rc = imops_scale_u16(raw, raw_w, raw_h, crop_x, crop_y, crop_w, crop_h, black, white, period_w,
                                   period_h, m, stream)))
             return rc;
-        if ((rc = imops_demosaic_markesteijn(m, crop_w, crop_h, P.cfa, crop_x, crop_y, rgb, stream))) return rc;
-        if ((rc = color::run_epilogue(rgb, (size_t)crop_w * crop_h, e, s, "develop colour"))) return rc;
+        // the 3x3 mean with the colour epilogue applied before its store
+        if ((rc = simple::mean3x3(m, crop_w, crop_h, cfa, &e, rgb, s))) return rc;
     } else {
         return fail(IMOPS_ERR_INVALID_ARGUMENT, "develop: demosaic must be AMaZE or Markesteijn");
     }
@@ -93,8 +94,7 @@ extern "C" int imops_develop_f32(const float* mosaic, int w, int h, int shift_x,
     if (P.demosaic == IMOPS_DEMOSAIC_AMAZE) {
         rc = amaze::demosaic_color_f32(mosaic, w, h, cfa, P.clip_pt, e, rgb, s);
     } else if (P.demosaic == IMOPS_DEMOSAIC_MARKESTEIJN) {
-        if ((rc = imops_demosaic_markesteijn(mosaic, w, h, P.cfa, shift_x, shift_y, rgb, stream))) return rc;
-        rc = color::run_epilogue(rgb, (size_t)w * h, e, s, "develop colour");
+        rc = simple::mean3x3(mosaic, w, h, cfa, &e, rgb, s);
     } else {
         return fail(IMOPS_ERR_INVALID_ARGUMENT, "develop: demosaic must be AMaZE or Markesteijn");
     }

@@ -25,6 +25,25 @@ def test_scale_u16_crop_and_levels(oracle_lib, gpu):
     assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize("period", [(6, 6), (1, 1), (2, 2)])
+def test_scale_u16_period_levels_several_blocks(oracle_lib, gpu, period):
+    """Per-site levels over a 6x6 (X-Trans), 1x1 and 2x2 period, a crop at an
+    odd origin, rows and columns spanning several blocks and a partial last
+    row group."""
+    import torch
+    import imops_b200 as im
+    raw = synthetic.mosaic_u16(157, 611, seed=4, pattern=synthetic.XTRANS)
+    n = period[0] * period[1]
+    rng = np.random.default_rng(n)
+    black = [float(v) for v in rng.uniform(580.0, 620.0, n).astype(np.float32)]
+    white = [float(v) for v in rng.uniform(15000.0, 16383.0, n).astype(np.float32)]
+    crop = (5, 7, 600, 141)
+    ref = oracle_lib.scale_u16(raw, crop, black, white, cfa_period=period)
+    t = torch.from_numpy(raw.view(np.int16)).to(gpu)
+    out = im.scale_u16(t, crop, black, white, period=period).cpu().numpy()
+    assert np.array_equal(out, ref)
+
+
 def test_cfa_coeffs(oracle_lib, gpu):
     import torch
     import imops_b200 as im

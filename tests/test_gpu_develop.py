@@ -67,6 +67,35 @@ def test_develop_markesteijn_xtrans(gpu):
     assert torch.equal(fused, staged)
 
 
+@pytest.mark.parametrize("crop", [(0, 0, 600, 141), (5, 4, 590, 137)])
+@pytest.mark.parametrize("cfa", [synthetic.XTRANS, "RGGB"])
+def test_develop_mean_route_equals_staged(gpu, crop, cfa):
+    """The 3x3-mean route of develop_u16 (scaling, then the mean with the
+    colour epilogue applied before its store) equals the separate calls, for
+    X-Trans and Bayer, gains and an ACEScg target, rows of several warps."""
+    import torch
+    import imops_b200 as im
+    raw = torch.from_numpy(synthetic.mosaic_u16(150, 610, seed=24, pattern=cfa).view(np.int16)).to(gpu)
+    p = _params(im, False, demosaic=1, target=im.CS_ACESCG, cfa=cfa.encode(), ev=(0.4, -0.2))
+    period = (6, 6) if len(cfa) == 36 else (2, 2)
+    fused = im.develop_u16(raw, crop, synthetic.BLACK, synthetic.WHITE, p, period=period)
+    staged = _staged(im, gpu, raw, crop, p, False)
+    assert torch.equal(fused, staged)
+
+
+def test_develop_f32_mean_route_equals_staged(gpu):
+    import torch
+    import imops_b200 as im
+    m = torch.from_numpy(synthetic.mosaic_f32(97, 420, seed=25, pattern=synthetic.XTRANS)).to(gpu)
+    p = _params(im, False, demosaic=1, target=im.CS_ACESCG, cfa=synthetic.XTRANS.encode(), ev=(0.25,))
+    fused = im.develop_f32(m, p, shift=(2, 3))
+    staged = im.demosaic_markesteijn(m, synthetic.XTRANS, shift=(2, 3))
+    im.cfa_coeffs(staged, synthetic.WB)
+    im.exp(staged, 0.25)
+    im.camera_cst(staged, synthetic.CALIB_D65, im.CS_ACESCG)
+    assert torch.equal(fused, staged)
+
+
 def test_develop_matches_oracle_chain(oracle_lib, gpu):
     import torch
     import imops_b200 as im
