@@ -68,11 +68,12 @@ def test_develop_markesteijn_xtrans(gpu):
 
 
 @pytest.mark.parametrize("crop", [(0, 0, 600, 141), (5, 4, 590, 137)])
-@pytest.mark.parametrize("cfa", [synthetic.XTRANS, "RGGB"])
+@pytest.mark.parametrize("cfa", [synthetic.XTRANS, "RGGB", "RGBG"])
 def test_develop_mean_route_equals_staged(gpu, crop, cfa):
     """The 3x3-mean route of develop_u16 (scaling, then the mean with the
-    colour epilogue applied before its store) equals the separate calls, for
-    X-Trans and Bayer, gains and an ACEScg target, rows of several warps."""
+    colour epilogue applied before its store; "RGBG", no shift of RGGB,
+    through the per-pixel mean) equals the separate calls, with gains and an
+    ACEScg target, rows of several warps."""
     import torch
     import imops_b200 as im
     raw = torch.from_numpy(synthetic.mosaic_u16(150, 610, seed=24, pattern=cfa).view(np.int16)).to(gpu)
@@ -80,6 +81,27 @@ def test_develop_mean_route_equals_staged(gpu, crop, cfa):
     period = (6, 6) if len(cfa) == 36 else (2, 2)
     fused = im.develop_u16(raw, crop, synthetic.BLACK, synthetic.WHITE, p, period=period)
     staged = _staged(im, gpu, raw, crop, p, False)
+    assert torch.equal(fused, staged)
+
+
+@pytest.mark.parametrize("cfa,period", [(synthetic.XTRANS, (6, 6)), (synthetic.XTRANS, (1, 1)), ("RGGB", (2, 2))])
+def test_develop_mean_route_site_levels(gpu, cfa, period):
+    """Per-site black and white levels over the level period: the develop
+    route equals imops_scale_u16 then the mean."""
+    import torch
+    import imops_b200 as im
+    raw = torch.from_numpy(synthetic.mosaic_u16(203, 433, seed=26, pattern=cfa).view(np.int16)).to(gpu)
+    n = period[0] * period[1]
+    rng = np.random.default_rng(7 + n)
+    black = [float(v) for v in rng.uniform(580.0, 620.0, n).astype(np.float32)]
+    white = [float(v) for v in rng.uniform(15000.0, 16383.0, n).astype(np.float32)]
+    p = _params(im, False, demosaic=1, target=im.CS_CAMERA, cfa=cfa.encode())
+    for i in range(4):
+        p.wb[i] = 1.0
+    crop = (7, 3, 420, 197)
+    fused = im.develop_u16(raw, crop, black, white, p, period=period)
+    m = im.scale_u16(raw, crop, black, white, period=period)
+    staged = im.demosaic_markesteijn(m, cfa, shift=crop[:2])
     assert torch.equal(fused, staged)
 
 
