@@ -356,7 +356,9 @@ def main():
                      white=synthetic.WHITE)
     Lp = im.lib()
 
-    def e2e_batch(frames):
+    host_ms = {"upload": [], "submit": [], "download": []}  # per call, host clock
+
+    def e2e_batch(frames, log=False):
         """Two host threads, as an application that streams frames would use
         the C-ABI: this one uploads each frame and submits its pipeline
         (new_raw_image_u16_c returns once the upload is done,
@@ -374,7 +376,10 @@ def main():
                 if img is None:
                     return
                 try:
+                    t_a = time.perf_counter()
                     im.check(Lp.get_image_rgb_f32_c(img._h, ctypes.c_void_p(rgb_h.data_ptr()), H * W * 3))
+                    if log:
+                        host_ms["download"].append((time.perf_counter() - t_a) * 1e3)
                 except Exception as e:  # reported by the submitting thread
                     errors.append(e)
                 del img
@@ -383,8 +388,13 @@ def main():
         t.start()
         try:
             for _ in range(frames):
+                t_a = time.perf_counter()
                 img = Image(Lp.new_raw_image_u16_c(ctypes.c_void_p(raw_h.data_ptr()), W, H, ctypes.byref(meta)))
+                t_b = time.perf_counter()
                 run_pixel_pipeline(img, cfg)
+                if log:
+                    host_ms["upload"].append((t_b - t_a) * 1e3)
+                    host_ms["submit"].append((time.perf_counter() - t_b) * 1e3)
                 pending.put(img)
                 del img
         finally:
@@ -398,7 +408,7 @@ def main():
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    e2e_batch(args.steps)
+    e2e_batch(args.steps, log=True)
     t_e2e = (time.perf_counter() - t0) * 1e3
     if dist:
         t = torch.tensor([t_e2e], device=dev)
@@ -462,6 +472,8 @@ def main():
                     "get_image_rgb_f32_c per frame; one host thread uploads and submits, a second reads the frames "
                     "back, so upload, kernels and download of consecutive frames overlap (pinned host buffers, host "
                     "clock)",
+                    "host_ms": {k: {"median": round(statistics.median(v), 3), "max": round(max(v), 3)}
+                                for k, v in host_ms.items() if v},
                     "link": {"d2h_gbs": round(d2h_gbs, 2), "h2d_gbs": round(h2d_gbs, 2),
                              "bound_mp_s": round(e2e_bound, 2), "frac_of_bound": round(e2e / e2e_bound, 3),
                              "note": "plain pinned copies of one frame's f32 RGB on this box; the bound is the "

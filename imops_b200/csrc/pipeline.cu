@@ -34,34 +34,66 @@ namespace pipe {
 // Each image gets one of a few library-owned streams, round robin, so the
 // frames a host submits one after another can overlap on the GPU (one
 // frame's compute with the previous frame's download).
+//
+// Image buffers come from a memory pool of the library's own per device
+// (the default pool, shared with the rest of the process, is left as it
+// is).  It keeps freed memory (release threshold: never) and reuses it in
+// stream order only: a buffer freed on a stream serves the next allocation on
+// that stream, so an image reuses the buffers of the image that held its
+// stream before it, with no wait on other streams and no growth of the pool
+// that depends on timing.
 constexpr int POOL_STREAMS = 3;
 struct DevState {
     bool init = false;
     cudaStream_t streams[POOL_STREAMS] = {};
+    cudaMemPool_t pool = nullptr;
     unsigned next = 0;
 };
 std::mutex g_dev_mu;
 DevState g_dev[128];
 
-int device_stream(cudaStream_t* out) {
+// The current device's state, created on first use; call with g_dev_mu held.
+int dev_state(DevState** out) {
     int dev = 0;
     IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev < 0 || dev >= 128) return fail(IMOPS_ERR_INVALID_ARGUMENT, "device index above 127");
-    std::lock_guard<std::mutex> lock(g_dev_mu);
     DevState& d = g_dev[dev];
     if (!d.init) {
         for (int i = 0; i < POOL_STREAMS; i++)
             IMOPS_CUDA_TRY(cudaStreamCreateWithFlags(&d.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
-        // keep freed image memory in the device pool so images can be
-        // created and freed per frame without returning memory to the OS
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-            uint64_t thr = UINT64_MAX;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-        }
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        IMOPS_CUDA_TRY(cudaMemPoolCreate(&d.pool, &props), "cudaMemPoolCreate(image buffers)");
+        uint64_t keep = UINT64_MAX;
+        int off = 0;
+        IMOPS_CUDA_TRY(cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep), "image pool");
+        IMOPS_CUDA_TRY(cudaMemPoolSetAttribute(d.pool, cudaMemPoolReuseAllowOpportunistic, &off), "image pool");
+        IMOPS_CUDA_TRY(cudaMemPoolSetAttribute(d.pool, cudaMemPoolReuseAllowInternalDependencies, &off),
+                       "image pool");
         d.init = true;
     }
-    *out = d.streams[d.next++ % POOL_STREAMS];
+    *out = &d;
+    return IMOPS_OK;
+}
+
+int device_stream(cudaStream_t* out) {
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    DevState* d = nullptr;
+    int rc = dev_state(&d);
+    if (rc) return rc;
+    *out = d->streams[d->next++ % POOL_STREAMS];
+    return IMOPS_OK;
+}
+
+int image_pool(cudaMemPool_t* out) {
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    DevState* d = nullptr;
+    int rc = dev_state(&d);
+    if (rc) return rc;
+    *out = d->pool;
     return IMOPS_OK;
 }
 
@@ -78,7 +110,10 @@ int buf_alloc(DevBuf& b, size_t bytes, cudaStream_t s) {
         b.p = nullptr;
         b.bytes = 0;
     }
-    IMOPS_CUDA_TRY(cudaMallocAsync(&b.p, bytes, s), "cudaMallocAsync(image buffer)");
+    cudaMemPool_t pool = nullptr;
+    int rc = image_pool(&pool);
+    if (rc) return rc;
+    IMOPS_CUDA_TRY(cudaMallocFromPoolAsync(&b.p, bytes, pool, s), "cudaMallocFromPoolAsync(image buffer)");
     b.bytes = bytes;
     return IMOPS_OK;
 }
