@@ -472,8 +472,8 @@ def main():
                     "get_image_rgb_f32_c per frame; one host thread uploads and submits, a second reads the frames "
                     "back, so upload, kernels and download of consecutive frames overlap (pinned host buffers, host "
                     "clock)",
-                    "host_ms": {k: {"median": round(statistics.median(v), 3), "max": round(max(v), 3)}
-                                for k, v in host_ms.items() if v},
+                    "host_ms": {k: {"median": round(statistics.median(v), 3), "max": round(max(v), 3),
+                                    "max_frame": v.index(max(v))} for k, v in host_ms.items() if v},
                     "link": {"d2h_gbs": round(d2h_gbs, 2), "h2d_gbs": round(h2d_gbs, 2),
                              "bound_mp_s": round(e2e_bound, 2), "frac_of_bound": round(e2e / e2e_bound, 3),
                              "note": "plain pinned copies of one frame's f32 RGB on this box; the bound is the "
