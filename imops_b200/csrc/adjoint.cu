@@ -137,14 +137,14 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
                 float2 xd = __fmul2_rn(d0, c.ne2[0][l]);
                 xd = __ffma2_rn(d1, c.ne2[1][l], xd);
                 xd = __ffma2_rn(d2, c.ne2[2][l], xd);
-                const float2 t = make_float2(exp2f(xd.x), exp2f(xd.y));
+                const float2 t = make_float2(film::ex2_fast(xd.x), film::ex2_fast(xd.y));
 #pragma unroll
                 for (int j = 0; j < 3; j++) oo[j] = __ffma2_rn(c.Cs2[j][l], t, oo[j]);
             }
             float xl = D[0] * c.ne_l[0];
             xl = fmaf(D[1], c.ne_l[1], xl);
             xl = fmaf(D[2], c.ne_l[2], xl);
-            const float tl = exp2f(xl);
+            const float tl = film::ex2_fast(xl);
             o0 = fmaf(c.Cs_l[0], tl, oo[0].x + oo[0].y);
             o1 = fmaf(c.Cs_l[1], tl, oo[1].x + oo[1].y);
             o2v = fmaf(c.Cs_l[2], tl, oo[2].x + oo[2].y);
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(BLK) pixel_kernel(const float* __restrict__ x,
                 float d = D[0] * c.eps[0][l];
                 d = fmaf(D[1], c.eps[1][l], d);
                 d = fmaf(D[2], c.eps[2][l], d);
-                const float t = exp2f(-d);
+                const float t = film::ex2_fast(-d);
                 o0 = fmaf(c.Cs[l][0], t, o0);
                 o1 = fmaf(c.Cs[l][1], t, o1);
                 o2v = fmaf(c.Cs[l][2], t, o2v);
