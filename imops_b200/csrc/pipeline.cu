@@ -59,20 +59,32 @@ int dev_state(DevState** out) {
     if (dev < 0 || dev >= 128) return fail(IMOPS_ERR_INVALID_ARGUMENT, "device index above 127");
     DevState& d = g_dev[dev];
     if (!d.init) {
-        for (int i = 0; i < POOL_STREAMS; i++)
-            IMOPS_CUDA_TRY(cudaStreamCreateWithFlags(&d.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
+        // all or nothing: a failure leaves no stream or pool behind, and the
+        // next call tries again
+        cudaStream_t st[POOL_STREAMS] = {};
+        cudaMemPool_t pool = nullptr;
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < POOL_STREAMS && e == cudaSuccess; i++)
+            e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
         cudaMemPoolProps props = {};
         props.allocType = cudaMemAllocationTypePinned;
         props.handleTypes = cudaMemHandleTypeNone;
         props.location.type = cudaMemLocationTypeDevice;
         props.location.id = dev;
-        IMOPS_CUDA_TRY(cudaMemPoolCreate(&d.pool, &props), "cudaMemPoolCreate(image buffers)");
+        if (e == cudaSuccess) e = cudaMemPoolCreate(&pool, &props);
         uint64_t keep = UINT64_MAX;
         int off = 0;
-        IMOPS_CUDA_TRY(cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep), "image pool");
-        IMOPS_CUDA_TRY(cudaMemPoolSetAttribute(d.pool, cudaMemPoolReuseAllowOpportunistic, &off), "image pool");
-        IMOPS_CUDA_TRY(cudaMemPoolSetAttribute(d.pool, cudaMemPoolReuseAllowInternalDependencies, &off),
-                       "image pool");
+        if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &off);
+        if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &off);
+        if (e != cudaSuccess) {
+            for (int i = 0; i < POOL_STREAMS; i++)
+                if (st[i]) cudaStreamDestroy(st[i]);
+            if (pool) cudaMemPoolDestroy(pool);
+            return fail(IMOPS_ERR_CUDA, std::string("image streams / pool: ") + cudaGetErrorString(e));
+        }
+        for (int i = 0; i < POOL_STREAMS; i++) d.streams[i] = st[i];
+        d.pool = pool;
         d.init = true;
     }
     *out = &d;
