@@ -19,7 +19,7 @@
 // buffers in HBM (4 directions x G, R, B, Lab, difference); the stencils
 // re-read their neighbours from L1/L2.  Built with --fmad=false: the same
 // IEEE f32 operations in the same order as the oracle, including its cube
-// root (Newton's method from an exponent-divided-by-3 first guess).
+// root (t r^2 with r = t^(-1/3) by a division-free Newton iteration).
 #include "common.cuh"
 
 namespace imops {
@@ -171,17 +171,23 @@ __global__ void refine_kernel(const __grid_constant__ Img im, const float* __res
     }
 }
 
-// cube root of t > 0: Newton's method from bits / 3 + 2/3 of the exponent bias
+// cube root of t > 0 as t r^2, r = t^(-1/3) by Newton's method for the
+// reciprocal cube root, r <- r (4 - t r^3) / 3: four steps from the first
+// guess 0x54AAAAAA - bits(t) / 3 (at most 8.2% high here), no division
 __device__ __forceinline__ float cbrt_nt(float t) {
-    float y = __uint_as_float(__float_as_uint(t) / 3u + 0x2A555555u);
+    float r = __uint_as_float(0x54AAAAAAu - __float_as_uint(t) / 3u);
 #pragma unroll
-    for (int it = 0; it < 3; it++) y = (y + y + t / (y * y)) * (1.0f / 3.0f);
-    return y;
+    for (int it = 0; it < 4; it++) {
+        const float r2 = r * r, r3 = r2 * r, q = t * r3;
+        r = (r * (4.0f - q)) * (1.0f / 3.0f);
+    }
+    return (t * r) * r;
 }
 
+// CIELab's f, the linear part as one multiply-add of folded constants
 __device__ __forceinline__ float lab_f(float t) {
     if (t > 216.0f / 24389.0f) return cbrt_nt(t);
-    return (24389.0f / 27.0f * t + 16.0f) / 116.0f;
+    return 7.787037037037037f * t + 0.13793103448275862f;
 }
 
 __global__ void lab_kernel(const float* __restrict__ R, const float* __restrict__ G, const float* __restrict__ B,
@@ -189,12 +195,11 @@ __global__ void lab_kernel(const float* __restrict__ R, const float* __restrict_
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         for (int d = 0; d < 4; d++) {
             const float r = R[d * n + i], g = G[d * n + i], b = B[d * n + i];
-            // linear sRGB -> XYZ (CSS Color 4) over the D65 white
-            const float x = (0.41239079926595934f * r + 0.357584339383878f * g + 0.1804807884018343f * b) /
-                            0.9504559270516716f;
+            // linear sRGB -> XYZ (CSS Color 4) over the D65 white, folded into
+            // the X and Z rows
+            const float x = 0.4338873455660398f * r + 0.3762240091374988f * g + 0.18988864529646143f * b;
             const float y = 0.21263900587151027f * r + 0.715168678767756f * g + 0.07219231536073371f * b;
-            const float z = (0.01933081871559182f * r + 0.11919477979462598f * g + 0.9505321522496607f * b) /
-                            1.0890577507598784f;
+            const float z = 0.017750040070973232f * r + 0.10944762085523847f * g + 0.8728023390737883f * b;
             const float fx = lab_f(x), fy = lab_f(y), fz = lab_f(z);
             L[(d * 3 + 0) * n + i] = 116.0f * fy - 16.0f;
             L[(d * 3 + 1) * n + i] = 500.0f * (fx - fy);

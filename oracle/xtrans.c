@@ -31,9 +31,11 @@
  *     Passes: 1, 2, 3, 2, 3, 2 (three green estimates, each followed by
  *     red / blue).
  *  4. perceptual difference: CIELab of each direction's RGB, taking camera
- *     RGB as linear sRGB (CSS Color 4 matrix, D65 white); the cube root by
- *     Newton's method from an exponent-divided-by-3 first guess (own code,
- *     the same IEEE operations on CPU and GPU).
+ *     RGB as linear sRGB (CSS Color 4 matrix with the D65 white folded into
+ *     its X and Z rows); the cube root as t r^2 with r = t^(-1/3) by Newton's
+ *     method for the reciprocal cube root, r <- r (4 - t r^3) / 3, from a
+ *     first guess made from the bits (own code, no division, the same IEEE
+ *     operations on CPU and GPU).
  *     D_d = |Lab_d(p) - Lab_d(p + s_d)|^2 + |Lab_d(p) - Lab_d(p - s_d)|^2.
  *  5. vote: T(q) = 8 min_d D_d(q); H_d(p) = #{q in 3x3(p): D_d(q) <= T(q)};
  *     the directions with H_d >= Hmax - Hmax / 8 (integer division) are
@@ -152,37 +154,48 @@ static real xt_refine(const XtImg *im, const real *G, const real *Rp, const real
     return xt_clamp(im->m[i] - k, lo, hi, n);
 }
 
-/* step 4: cube root of t > 0 by Newton's method, first guess from the
- * exponent divided by 3 (bits / 3 + 2/3 of the f32 exponent bias) */
+/* step 4: cube root of t > 0 as t * r * r, r = t^(-1/3) by Newton's method
+ * for the reciprocal cube root, r <- r (4 - t r^3) / 3, which needs no
+ * division.  First guess 0x54AAAAAA - bits(t) / 3: at most 8.2% high for the
+ * t here, inside the iteration's convergence bound (t r^3 < 4). */
 static real xt_cbrt(real t)
 {
     float tf = (float)t;
     uint32_t u;
     memcpy(&u, &tf, 4);
-    u = u / 3u + 0x2A555555u;
-    float yf;
-    memcpy(&yf, &u, 4);
-    real y = (real)yf;
-    /* three steps take the 6% first guess to f32 accuracy (1.6e-7) */
-    for (int it = 0; it < 3; it++) y = (y + y + t / (y * y)) * (K(1.0) / K(3.0));
+    u = 0x54AAAAAAu - u / 3u;
+    float rf;
+    memcpy(&rf, &u, 4);
+    real r = (real)rf;
+    /* four steps: the cube root to 4.6e-7 relative in f32 */
+    for (int it = 0; it < 4; it++) {
+        real r2 = r * r, r3 = r2 * r, q = t * r3;
+        r = (r * (K(4.0) - q)) * (K(1.0) / K(3.0));
+    }
 #ifndef ORACLE_F32
-    for (int it = 0; it < 2; it++) y = (y + y + t / (y * y)) * (1.0 / 3.0);
+    for (int it = 0; it < 2; it++) {
+        double r2 = r * r, r3 = r2 * r, q = t * r3;
+        r = (r * (4.0 - q)) * (1.0 / 3.0);
+    }
 #endif
-    return y;
+    return (t * r) * r;
 }
 
+/* CIELab's f: (24389/27 t + 16) / 116 as one multiply-add of folded
+ * constants below the threshold */
 static real xt_f(real t)
 {
     if (t > K(216.0) / K(24389.0)) return xt_cbrt(t);
-    return (K(24389.0) / K(27.0) * t + K(16.0)) / K(116.0);
+    return K(7.787037037037037) * t + K(0.13793103448275862);
 }
 
 static void xt_lab(real r, real g, real b, real lab[3])
 {
-    /* linear sRGB -> XYZ (CSS Color 4), divided by the D65 white */
-    real x = (K(0.41239079926595934) * r + K(0.357584339383878) * g + K(0.1804807884018343) * b) / K(0.9504559270516716);
+    /* linear sRGB -> XYZ (CSS Color 4) over the D65 white: the X row divided
+     * by 0.9504559270516716 and the Z row by 1.0890577507598784 (in double) */
+    real x = K(0.4338873455660398) * r + K(0.3762240091374988) * g + K(0.18988864529646143) * b;
     real y = K(0.21263900587151027) * r + K(0.715168678767756) * g + K(0.07219231536073371) * b;
-    real z = (K(0.01933081871559182) * r + K(0.11919477979462598) * g + K(0.9505321522496607) * b) / K(1.0890577507598784);
+    real z = K(0.017750040070973232) * r + K(0.10944762085523847) * g + K(0.8728023390737883) * b;
     real fx = xt_f(x), fy = xt_f(y), fz = xt_f(z);
     lab[0] = K(116.0) * fy - K(16.0);
     lab[1] = K(500.0) * (fx - fy);
