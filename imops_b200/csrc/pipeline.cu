@@ -23,6 +23,7 @@
 
 #include "amaze.cuh"
 #include "color.cuh"
+#include "demosaic_simple.cuh"
 #include "config.hpp"
 #include "display.cuh"
 
@@ -244,7 +245,8 @@ const char* cs_debug(const ImopsImage& img) {
 
 struct Demosaic : Module {
     int algorithm = IMOPS_DEMOSAIC_AMAZE;
-    // per-pixel modules fused into AMaZE's output stage by run_pixel_pipeline_c
+    // per-pixel modules fused into the output stage of AMaZE or the 3x3 mean
+    // by run_pixel_pipeline_c
     color::Epilogue fused = color::identity_epilogue();
     int fused_cs = IMOPS_CS_CAMERA;
     int process(ImopsImage& img) override {
@@ -287,7 +289,9 @@ struct Demosaic : Module {
                 rc = amaze::demosaic_color_f32(mosaic, w, h, c, 1.0f, e, rgb, s);
             }
         } else if (algorithm == IMOPS_DEMOSAIC_MARKESTEIJN) {
-            rc = imops_demosaic_markesteijn(mosaic, w, h, img.cfa.c_str(), cx, cy, rgb, s);
+            CfaDev c;
+            rc = parse_cfa(img.cfa.c_str(), cx, cy, &c);
+            if (!rc) rc = simple::mean3x3(mosaic, w, h, c, &fused, rgb, s);
         } else {
             int f = algorithm == IMOPS_DEMOSAIC_FAST ? 2 : (algorithm == IMOPS_DEMOSAIC_SUPERFAST ? 4 : 8);
             rc = imops_demosaic_quad(mosaic, w, h, img.cfa.c_str(), cx, cy, f, rgb, s);
@@ -891,7 +895,8 @@ extern "C" ImopsImage* run_pixel_pipeline_c(ImopsImage* image, ImopsPipeline* pi
         }
         auto* dem = dynamic_cast<pipe::Demosaic*>(mods[k].get());
         size_t fused_until = k;
-        if (dem && dem->algorithm == IMOPS_DEMOSAIC_AMAZE && image->raw_kind != 0 && !image->cfa.empty())
+        if (dem && (dem->algorithm == IMOPS_DEMOSAIC_AMAZE || dem->algorithm == IMOPS_DEMOSAIC_MARKESTEIJN) &&
+            image->raw_kind != 0 && !image->cfa.empty())
             fused_until = pipe::plan_fusion(*image, mods, k, &dem->fused, &dem->fused_cs);
         if (mods[k]->process(*image) != IMOPS_OK) return nullptr;
         k = fused_until;

@@ -75,6 +75,26 @@ def test_pipeline_markesteijn_exp_linear_srgb(gpu, oracle_lib):
     assert np.array_equal(got, ref)
 
 
+def test_pipeline_markesteijn_fused_chain_u16(gpu, oracle_lib):
+    """A u16 X-Trans frame through Demosaic(markesteijn) with CFACoeffs, Exp and
+    CST fused into the 3x3 mean's store: equal to the oracle chain."""
+    from imops_b200.pipeline import Image, parse_config, run_pixel_pipeline
+    raw = synthetic.mosaic_u16(90, 126, seed=34, pattern=synthetic.XTRANS)
+    cfg = ('[[pipeline_modules]]\nname = "Demosaic"\nalgorithm = "markesteijn"\n'
+           '[[pipeline_modules]]\nname = "CFACoeffs"\n'
+           '[[pipeline_modules]]\nname = "Exp"\nev = 0.4\n'
+           '[[pipeline_modules]]\nname = "CST"\ntarget_color_space = "AcesCg"\n')
+    img = Image.from_u16(raw, _meta(cfa=synthetic.XTRANS, crop=(3, 2, 114, 80)))
+    run_pixel_pipeline(img, parse_config(cfg))
+    got = img.rgb_f32()
+    m = oracle_lib.scale_u16(raw, (3, 2, 114, 80), synthetic.BLACK, synthetic.WHITE, cfa_period=(1, 1))
+    ref = oracle_lib.mean3x3(m, synthetic.XTRANS, shift=(3, 2))
+    ref = oracle_lib.wb(ref, synthetic.WB)
+    ref = oracle_lib.exposure(ref, 0.4)
+    ref = oracle_lib.camera_cst(ref, synthetic.CALIB_D65, oracle_lib.CS_ACESCG)
+    assert np.array_equal(got, ref)
+
+
 def test_pipeline_amaze_fused_chain_equals_oracle(gpu, oracle_lib):
     from imops_b200.pipeline import Image, parse_config, run_pixel_pipeline
     m = synthetic.mosaic_f32(256, 320, seed=33)
