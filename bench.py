@@ -9,8 +9,12 @@ sigma 0.02).  Metric: megapixels per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-N > 1 runs under torchrun, one rank per GPU, each developing its own frame
-(weak scaling, no collective on the data path); time = max over ranks.
+N > 1 runs one rank per GPU, each developing its own frame (weak scaling,
+no collective on the data path); time = max over ranks.  Started under
+torchrun the ranks come from its environment; started plainly with
+--gpus N > 1, bench.py launches the N ranks itself (torchrun on this node,
+127.0.0.1).  --dry-run runs the launch and rank plumbing (gloo, barrier,
+max-over-ranks reduction, rank 0's JSON line) without touching a GPU.
 """
 from __future__ import annotations
 
@@ -19,6 +23,8 @@ import ctypes
 import json
 import os
 import queue
+import signal
+import socket
 import statistics
 import subprocess
 import sys
@@ -56,7 +62,76 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="imops_b200", choices=["imops_b200", "reference"])
+    ap.add_argument("--dry-run", action="store_true",
+                    help="launch and rank plumbing only (gloo, no GPU work); prints a line with dry_run: true")
     return ap.parse_args()
+
+
+def _free_port() -> int:
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+LAUNCH_TIMEOUT_S = 1800  # last bound on a self-launched run, far above the process groups' 120 s timeout
+
+
+def launch_ranks(args) -> int:
+    """--gpus N (N > 1) outside torchrun: run N ranks of this script, one per
+    GPU, under torchrun on this node and return its exit status.  Rank 0
+    prints the JSON line."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), os.path.abspath(__file__),
+           *sys.argv[1:]]
+    proc = subprocess.Popen(cmd, start_new_session=True)
+    try:
+        return proc.wait(timeout=LAUNCH_TIMEOUT_S)
+    except subprocess.TimeoutExpired:
+        os.killpg(proc.pid, signal.SIGKILL)  # torchrun and its ranks: the group this call started
+        proc.wait()
+        print(f"bench.py: {args.gpus} ranks did not finish within {LAUNCH_TIMEOUT_S} s", file=sys.stderr)
+        return 124
+
+
+def init_ranks(world: int, backend: str):
+    """The process group of a multi-rank run (short timeout, so ranks that
+    wait for one another end with an error), or None for one rank."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def dry_run(args, rank, world):
+    """The launch and rank plumbing without a GPU: every rank times a small
+    host computation, the time is reduced to the max over ranks, and rank 0
+    prints the line with n_gpus = the number of ranks that took part."""
+    import numpy as np
+    import torch
+
+    dist = init_ranks(world, "gloo")
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(args.warmup + args.steps):
+        np.sort(np.random.default_rng(rank * 1000 + k).random(1 << 16))
+    t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64)
+    ranks = torch.ones(1, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(ranks, op=dist.ReduceOp.SUM)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": None, "unit": "MP/s", "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "dry_run": True, "impl": args.impl, "ranks_reporting": int(ranks.item()),
+                          "max_rank_s": round(float(t.item()), 6), "config": workload_config(world)}), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def peaks():
@@ -186,6 +261,38 @@ def cpu_sample(threads: int):
     return h * w / 1e6 / dt, f"{w}x{h} crop of the 6048x4024 frame: AMaZE + WB + CST + 81-bin film (f32 oracle)"
 
 
+def cpu_check_error(raw_np, colour, film, film_other_scan=None):
+    """Error of this rank's frame against FP64, whole frame: max and RMS
+    absolute error in linear [0, 1] and in 16-bit LSB of
+      colour      the colour forward (AMaZE + WB + camera matrix) against the
+                  FP64 colour chain; AMaZE decision flips (more than 8 LSB from
+                  FP64, where a comparison resolves differently in f32) apart;
+      film_stage  the film output against the FP64 film of the same colour;
+      film_chain  the film output against the FP64 chain end to end (flips
+                  apart): the film's curves amplify the colour stage's error.
+    Host cores, after the timed regions; the oracle is the checker here."""
+    import oracle
+    from imops_b200 import synthetic
+    t0 = time.perf_counter()
+    r = lambda d: {k: (round(v, 9) if k.endswith("abs") else round(v, 4)) for k, v in d.items()}
+    bp = oracle.baseline_params(seed=SEED)
+    stage64 = oracle.film_baseline(colour, bp, precision="f64")
+    out = {"vs": "FP64 oracle (scaling, AMaZE, WB, camera matrix, 81-bin film with grain), whole frame",
+           "pixels": int(raw_np.size), "film_stage": r(oracle.error_figures(film, stage64))}
+    if film_other_scan is not None:
+        out["film_stage_other_scan"] = r(oracle.error_figures(film_other_scan, stage64))
+    del stage64
+    c64 = oracle.colour_chain(raw_np, synthetic.BLACK, synthetic.WHITE, synthetic.WB, synthetic.CALIB_D65)
+    flips = oracle.decision_flips(colour, c64)
+    out["amaze_decision_flips"] = int(flips.sum())
+    out["colour"] = r(oracle.error_figures(colour, c64, skip=flips))
+    chain64 = oracle.film_baseline(c64, bp, precision="f64")
+    out["film_chain"] = r(oracle.error_figures(film, chain64, skip=flips))
+    out["film_chain_incl_flips_max_lsb"] = round(oracle.error_figures(film, chain64)["max_lsb"], 2)
+    out["check_s"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
 def workload_config(world):
     """The workload both arms report (the reference arm times a bounded sample
     of it, described in its cpu_baseline.sample)."""
@@ -204,7 +311,7 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             vals.append(v)
     value = sum(vals) / len(vals)
-    line = {"metric": METRIC, "value": round(value, 3), "unit": "MP/s", "n_gpus": args.gpus, "steps": args.steps,
+    line = {"metric": METRIC, "value": round(value, 3), "unit": "MP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1536 * 1024 / 1e3 / value, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(world),
@@ -217,9 +324,13 @@ def run_reference(args, rank, world):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.dry_run:
+        return dry_run(args, rank, world)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
@@ -231,12 +342,7 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = init_ranks(world, "nccl")
 
     raw_np = synthetic.mosaic_u16(H, W, seed=SEED + rank)
     raw = torch.from_numpy(raw_np.view(np.int16)).to(dev)
@@ -291,6 +397,35 @@ def main():
         t = torch.tensor([t_total], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_total = float(t.item())
+
+    # the film stage with each of the 81-bin scan's two forms (contractions on
+    # the CUDA cores in FP32, or on the tensor cores in BF16 hi/lo), timed
+    # alike on the same colour output: K steps each, L2 flushed between
+    colour_d = rgb.clone()
+    im.check(L.imops_develop_u16(ctypes.c_void_p(raw.data_ptr()), W, H, 0, 0, W, H, black, white, 2, 2,
+                                 ctypes.byref(p_dem), ctypes.c_void_p(colour_d.data_ptr()), sp))
+    arm_ms = {}
+    for arm_name, arm in (("fp32", im.SCAN_FP32), ("bf16_tc", im.SCAN_BF16_TC)):
+        p_arm = im.baseline_film_defaults(seed=SEED, scan=arm)
+
+        def film_arm(events=None):
+            rgb.copy_(colour_d)
+            if events:
+                events[0].record(stream)
+            im.check(L.imops_film_process(ctypes.c_void_p(rgb.data_ptr()), W, H, im.CS_ACESCG,
+                                          ctypes.byref(p_all.film_params), ctypes.byref(p_arm), sp))
+            if events:
+                events[1].record(stream)
+
+        for _ in range(args.warmup):
+            film_arm()
+        eva = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            film_arm(eva[k])
+        torch.cuda.synchronize()
+        arm_ms[arm_name] = sum(e[0].elapsed_time(e[1]) for e in eva) / args.steps
+    del colour_d
 
     # forward + backward of the differentiable colour + film model (24
     # parameters: WB, camera->ACEScg matrix, EV, curves, halation) on the same
@@ -446,6 +581,20 @@ def main():
     achieved = dom_bytes / (t_dem / 1e3) / 1e9
     if rank == 0:
         clk_summary = clk.summary()
+        # this frame's outputs for the error check: the colour forward, then the film
+        im.check(L.imops_develop_u16(ctypes.c_void_p(raw.data_ptr()), W, H, 0, 0, W, H, black, white, 2, 2,
+                                     ctypes.byref(p_dem), ctypes.c_void_p(rgb.data_ptr()), sp))
+        colour_np = rgb.cpu().numpy()
+        im.check(L.imops_film_process(ctypes.c_void_p(rgb.data_ptr()), W, H, im.CS_ACESCG,
+                                      ctypes.byref(p_all.film_params), ctypes.byref(p_all.baseline), sp))
+        film_np = rgb.cpu().numpy()
+        p_other = im.baseline_film_defaults(seed=SEED)
+        p_other.scan = im.SCAN_BF16_TC if p_all.baseline.scan == im.SCAN_FP32 else im.SCAN_FP32
+        rgb.copy_(torch.from_numpy(colour_np).to(dev))
+        im.check(L.imops_film_process(ctypes.c_void_p(rgb.data_ptr()), W, H, im.CS_ACESCG,
+                                      ctypes.byref(p_all.film_params), ctypes.byref(p_other), sp))
+        other_np = rgb.cpu().numpy()
+        error = cpu_check_error(raw_np, colour_np, film_np, other_np)
         cpu_v, cpu_sample_desc = cpu_sample(os.cpu_count() or 1)
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "MP/s", "n_gpus": world, "steps": args.steps,
@@ -453,6 +602,11 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(world),
             "stages_ms": {"amaze_colour": round(t_dem, 4), "film": round(t_film, 4)},
+            "scan": {"in_value": "fp32" if p_all.baseline.scan == im.SCAN_FP32 else "bf16_tc",
+                     "film_ms": {k: round(v, 4) for k, v in arm_ms.items()},
+                     "note": "film stage alone per arm, K steps each with the L2 flushed between; the 81-bin scan's "
+                             "contractions in FP32 on the CUDA cores, or BF16 hi/lo with FP32 accumulation on the "
+                             "tensor cores (tcgen05); error.film_stage_other_scan is the arm not in value"},
             "fwd_bwd": {"value": round(fwd_bwd, 2), "unit": "MP/s", "ms_per_step": round(t_fb / args.steps, 4),
                         "stages_ms": {"amaze_cam_plus_model_fwd": round(t_fb_fwd, 4),
                                       "model_bwd": round(t_fb_bwd, 4)},
@@ -462,6 +616,9 @@ def main():
                          "achieved": round(achieved, 2), "peak": bw, "unit": "GB/s",
                          "frac": round(achieved / bw, 5), "traffic": ncu_traffic(), "peak_kind": peak_kind,
                          "bytes_per_launch": dom_bytes,
+                         "traffic_note": "ncu dram__bytes_read + dram__bytes_write of one launch (scaled from the "
+                                         "committed capture): a lower bound, since output lines still dirty in L2 "
+                                         "when the kernel ends are written back after it",
                          "note": "AMaZE is FP32-issue bound (~25 IEEE divides/px on 1.78x overlapping tiles); "
                                  "the HBM fraction is reported against 14 B/px compulsory traffic",
                          "issue": issue_fraction(t_dem, clk_summary)},
@@ -478,6 +635,7 @@ def main():
                              "bound_mp_s": round(e2e_bound, 2), "frac_of_bound": round(e2e / e2e_bound, 3),
                              "note": "plain pinned copies of one frame's f32 RGB on this box; the bound is the "
                                      "slowest of download, upload and kernels per frame"}},
+            "error": error,
             "gpu_launches": int(launches),
             "clocks": clk_summary,
         }

@@ -235,6 +235,7 @@ def sigmoid_tone_map(rgb, stream=None):
 
 STOCK_BWSTUB, STOCK_COLORNEG200, STOCK_PORTRA400, STOCK_EKTAR100, STOCK_FUJIPRO400H = 0, 1, 2, 3, 4
 STOCK_EKTACHROMEE100, STOCK_TRIX400, STOCK_BASELINE81 = 5, 6, 100
+SCAN_FP32, SCAN_BF16_TC = 0, 1
 FORMAT_35MM, FORMAT_6X6, FORMAT_4X5 = 0, 1, 2
 FILM_NEGATIVE_LINEAR, FILM_POSITIVE_LINEAR = 0, 1
 
@@ -252,7 +253,7 @@ class BaselineFilm(ctypes.Structure):
     _fields_ = [("dmax", ctypes.c_float * 3), ("k", ctypes.c_float * 3), ("x0", ctypes.c_float * 3),
                 ("hal_strength", ctypes.c_float), ("hal_sigma", ctypes.c_float), ("hal_radius", ctypes.c_int),
                 ("hal_threshold", ctypes.c_float), ("grain_sigma", ctypes.c_float), ("grain_blur", ctypes.c_float),
-                ("grain_on", ctypes.c_int), ("seed", ctypes.c_uint64)]
+                ("grain_on", ctypes.c_int), ("seed", ctypes.c_uint64), ("scan", ctypes.c_int)]
 
 
 def baseline_film_defaults(**overrides) -> BaselineFilm:

@@ -12,6 +12,7 @@
 // Layout: per-layer planes (row-major f32), so every pass is a coalesced
 // stream; RGB stays interleaved as in Image.rgb_data.
 #include <cmath>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -416,45 +417,59 @@ __global__ void dir_apply_kernel(float* __restrict__ planes, const float* __rest
 // grain (grain.rs:20-100): SplitMix64 is counter based, so pixel x of row y
 // uses draws 12x+1..12x+12 of the row stream and is generated independently.
 
-// The blurred grain field of one layer in one pass: Irwin-Hall noise over a
-// tile plus its halo (grain_noise_at), mirrored at the
-// image edge; the row then column passes of blur() in shared memory with the
-// same taps and summation order (so the field equals blur(noise) bit for
-// bit); the field written, and the block's sum of squares (f64) stored in
-// partial[plane][block] for the variance.  Plane z holds RNG layer
-// layer0 + z.  Radius <= GR_MAXR.
+// The blurred grain fields of LAYERS consecutive RNG layers of one tile in one
+// pass: Irwin-Hall noise over the tile plus its halo (grain_noise_at),
+// mirrored at the image edge; per layer the row then column passes of blur()
+// in shared memory with the same taps and summation order (so each field
+// equals blur(noise) bit for bit); the fields written, and each layer's block
+// sum of squares (f64) stored in partial[plane][block] for the variance.
+// Plane z holds RNG layer layer0 + z.  Radius <= GR_MAXR.
 constexpr int GR_TW = 128, GR_TH = 64, GR_MAXR = 16;
 constexpr int GR_THREADS = 512, GR_TY = GR_THREADS / 32;
 
-// Noise of pixel (y, x) of a layer (grain.rs:20-45, 53-66): the sum of 12
-// uniforms minus 6, the uniforms being draws 12x+1 .. 12x+12 of the row's
-// SplitMix64 stream, seeded seed*0xD1B54A32D192ED03 + layer*0x9E3779B97F4A7C15 + y.
-__device__ __forceinline__ float grain_noise_at(uint64_t seed, int layer, int y, int x) {
+// Noise of pixel (y, x) in LAYERS consecutive layers layer0, layer0+1, ...
+// (grain.rs:20-45, 53-66).  Layer L of row y is the SplitMix64 stream seeded
+// seed*0xD1B54A32D192ED03 + L*golden + y, and pixel x takes its draws
+// 12x+1 .. 12x+12, the sum of those 12 uniforms minus 6.  Draw k of layer L
+// has the state seed*C + y + (L + 12x + k)*golden, which is draw L + k of
+// layer 0's stream: consecutive layers share all but one of their draws.  So
+// the layers of pixel x take the LAYERS + 11 draws 12x+layer0+1 .. of one
+// stream, each draw mixed once, and layer layer0 + z sums draws z+1 .. z+12
+// of them in order (each sum in f32, in the reference's order).
+template <int LAYERS>
+__device__ __forceinline__ void grain_noise_at(uint64_t seed, int layer0, int y, int x, float (&out)[LAYERS]) {
     const uint64_t golden = 0x9E3779B97F4A7C15ull;
     // state of draw k is s0 + k * golden (mod 2^64): stepped, not multiplied
-    uint64_t z0 = seed * 0xD1B54A32D192ED03ull + (uint64_t)layer * golden + (uint64_t)y + 12 * (uint64_t)x * golden;
-    float acc = 0.0f;
+    uint64_t z0 = seed * 0xD1B54A32D192ED03ull + (uint64_t)layer0 * golden + (uint64_t)y + 12 * (uint64_t)x * golden;
+    float acc[LAYERS];
 #pragma unroll
-    for (int k = 1; k <= 12; k++) {
+    for (int z = 0; z < LAYERS; z++) acc[z] = 0.0f;
+#pragma unroll
+    for (int k = 1; k <= LAYERS + 11; k++) {
         z0 += golden;
-        uint64_t z = (z0 ^ (z0 >> 30)) * 0xBF58476D1CE4E5B9ull;
-        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-        acc += __ull2float_rn(z ^ (z >> 31)) / 18446744073709551616.0f;
+        uint64_t v = (z0 ^ (z0 >> 30)) * 0xBF58476D1CE4E5B9ull;
+        v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+        const float u = __ull2float_rn(v ^ (v >> 31)) / 18446744073709551616.0f;
+#pragma unroll
+        for (int z = 0; z < LAYERS; z++)
+            if (k >= z + 1 && k <= z + 12) acc[z] += u;
     }
-    return acc - 6.0f;
+#pragma unroll
+    for (int z = 0; z < LAYERS; z++) out[z] = acc[z] - 6.0f;
 }
 
+template <int LAYERS>
 __global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restrict__ noise, int W, int H, uint64_t seed,
                                                           int layer0, Taps tp, double* __restrict__ partial) {
     extern __shared__ float gsm[];
     __shared__ double red[GR_TY];
-    const int layer = layer0 + (int)blockIdx.z, R = tp.R;
+    const int R = tp.R;
     const int x0 = blockIdx.x * GR_TW, y0 = blockIdx.y * GR_TH;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const int NW = GR_TW + 2 * R, NH = GR_TH + 2 * R;
     const int GR_SW = NW;
-    float* sn = gsm;             // noise, tile + halo: NH x NW
-    float* sr = gsm + NH * NW;   // row-blurred: NH x GR_TW
+    float* sn = gsm;                     // noise, tile + halo: LAYERS x NH x NW
+    float* sr = gsm + LAYERS * NH * NW;  // row-blurred: NH x GR_TW (one layer at a time)
     // flat over the tile + halo so every lane draws (the halo row is not a
     // multiple of the warp width)
     // (row, column) of idx stepped without a division: idx advances by
@@ -463,9 +478,12 @@ __global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restri
     int r = tid / NW, c = tid - (tid / NW) * NW;
     // blocks whose tile + halo lies inside the image need no mirroring
     const bool inner = x0 - R >= 0 && y0 - R >= 0 && x0 + GR_TW + R <= W && y0 + GR_TH + R <= H;
+    float v[LAYERS];
     if (inner) {
         for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
-            sn[idx] = grain_noise_at(seed, layer, y0 - R + r, x0 - R + c);
+            grain_noise_at<LAYERS>(seed, layer0, y0 - R + r, x0 - R + c, v);
+#pragma unroll
+            for (int z = 0; z < LAYERS; z++) sn[z * NH * NW + idx] = v[z];
             r += dq;
             c += dr;
             if (c >= NW) {
@@ -475,7 +493,9 @@ __global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restri
         }
     } else {
         for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
-            sn[idx] = grain_noise_at(seed, layer, reflect(y0 - R + r, H), reflect(x0 - R + c, W));
+            grain_noise_at<LAYERS>(seed, layer0, reflect(y0 - R + r, H), reflect(x0 - R + c, W), v);
+#pragma unroll
+            for (int z = 0; z < LAYERS; z++) sn[z * NH * NW + idx] = v[z];
             r += dq;
             c += dr;
             if (c >= NW) {
@@ -484,43 +504,46 @@ __global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restri
             }
         }
     }
-    __syncthreads();
-    for (int r = ty; r < NH; r += GR_TY)
-        for (int c = tx; c < GR_TW; c += 32) {
-            float acc = 0.0f;
-            // radius 3 (a 1 px grain blur, every stock here) unrolled
-            if (R == 3) {
-#pragma unroll
-                for (int k = 0; k <= 6; k++) acc = fmaf(sn[r * GR_SW + c + k], tp.t[k], acc);
-            } else {
-                for (int k = 0; k <= 2 * R; k++) acc = fmaf(sn[r * GR_SW + c + k], tp.t[k], acc);
-            }
-            sr[r * GR_TW + c] = acc;
-        }
-    __syncthreads();
     const size_t n = (size_t)W * H;
-    double sq = 0.0;
-    for (int r = ty; r < GR_TH; r += GR_TY)
-        for (int c = tx; c < GR_TW; c += 32) {
-            const int y = y0 + r, x = x0 + c;
-            if (y >= H || x >= W) continue;
-            float acc = 0.0f;
-            if (R == 3) {
+    for (int z = 0; z < LAYERS; z++) {
+        const float* snz = sn + z * NH * NW;
+        __syncthreads();  // the noise is complete; sr is free again
+        for (int r = ty; r < NH; r += GR_TY)
+            for (int c = tx; c < GR_TW; c += 32) {
+                float acc = 0.0f;
+                // radius 3 (a 1 px grain blur, every stock here) unrolled
+                if (R == 3) {
 #pragma unroll
-                for (int k = 0; k <= 6; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
-            } else {
-                for (int k = 0; k <= 2 * R; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
+                    for (int k = 0; k <= 6; k++) acc = fmaf(snz[r * GR_SW + c + k], tp.t[k], acc);
+                } else {
+                    for (int k = 0; k <= 2 * R; k++) acc = fmaf(snz[r * GR_SW + c + k], tp.t[k], acc);
+                }
+                sr[r * GR_TW + c] = acc;
             }
-            noise[blockIdx.z * n + (size_t)y * W + x] = acc;
-            sq += (double)acc * (double)acc;
+        __syncthreads();
+        double sq = 0.0;
+        for (int r = ty; r < GR_TH; r += GR_TY)
+            for (int c = tx; c < GR_TW; c += 32) {
+                const int y = y0 + r, x = x0 + c;
+                if (y >= H || x >= W) continue;
+                float acc = 0.0f;
+                if (R == 3) {
+#pragma unroll
+                    for (int k = 0; k <= 6; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
+                } else {
+                    for (int k = 0; k <= 2 * R; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
+                }
+                noise[z * n + (size_t)y * W + x] = acc;
+                sq += (double)acc * (double)acc;
+            }
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+        if (tx == 0) red[ty] = sq;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < GR_TY; w++) t += red[w];
+            partial[(size_t)z * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x] = t;
         }
-    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-    if (tx == 0) red[ty] = sq;
-    __syncthreads();
-    if (tid == 0) {
-        double t = 0.0;
-        for (int w = 0; w < GR_TY; w++) t += red[w];
-        partial[(size_t)blockIdx.z * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x] = t;
     }
 }
 
@@ -551,14 +574,33 @@ size_t grain_partials(int W, int H, int layers) {
 int grain_fields(float* noise, int W, int H, uint64_t seed, int layer0, int layers, const Taps& tp, double* partial,
                  double* sums, cudaStream_t s) {
     if (tp.R > GR_MAXR) return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "film: grain blur radius above 16 px");
-    dim3 b(32, GR_TY), g((W + GR_TW - 1) / GR_TW, (H + GR_TH - 1) / GR_TH, layers);
+    dim3 b(32, GR_TY), g((W + GR_TW - 1) / GR_TW, (H + GR_TH - 1) / GR_TH);
     const int NW = GR_TW + 2 * tp.R, NH = GR_TH + 2 * tp.R;
-    const size_t smem = (size_t)NH * (NW + GR_TW) * sizeof(float);
-    IMOPS_CUDA_TRY(cudaFuncSetAttribute(grain_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                   "cudaFuncSetAttribute(grain)");
-    grain_field_kernel<<<g, b, smem, s>>>(noise, W, H, seed, layer0, tp, partial);
-    note_launch();
-    sum_partials_kernel<<<layers, 1024, 0, s>>>(partial, (int)(g.x * g.y), sums);
+    // three layers per block (their draws shared) while their noise fits in
+    // shared memory; otherwise one block per (tile, layer)
+    const size_t smem3 = (size_t)NH * (3 * NW + GR_TW) * sizeof(float);
+    const size_t n = (size_t)W * H, nb = (size_t)g.x * g.y;
+    int z = 0;
+    if (layers >= 3 && smem3 <= 200 * 1024) {
+        IMOPS_CUDA_TRY(cudaFuncSetAttribute(grain_field_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem3),
+                       "cudaFuncSetAttribute(grain)");
+        for (; z + 3 <= layers; z += 3) {
+            grain_field_kernel<3><<<g, b, smem3, s>>>(noise + z * n, W, H, seed, layer0 + z, tp, partial + z * nb);
+            note_launch();
+        }
+    }
+    if (z < layers) {
+        const size_t smem1 = (size_t)NH * (NW + GR_TW) * sizeof(float);
+        IMOPS_CUDA_TRY(cudaFuncSetAttribute(grain_field_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem1),
+                       "cudaFuncSetAttribute(grain)");
+        for (; z < layers; z++) {
+            grain_field_kernel<1><<<g, b, smem1, s>>>(noise + z * n, W, H, seed, layer0 + z, tp, partial + z * nb);
+            note_launch();
+        }
+    }
+    sum_partials_kernel<<<layers, 1024, 0, s>>>(partial, (int)nb, sums);
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "grain fields");
     return IMOPS_OK;
@@ -784,6 +826,338 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
         rgb[3 * p + 1] = fmaf(c.P.C_last[1], tl, o1.x + o1.y);
         rgb[3 * p + 2] = fmaf(c.P.C_last[2], tl, o2.x + o2.y);
     }
+}
+
+// ---------------------------------------------------------------------------
+// The 81-bin scan on the tensor cores (tcgen05, sm_100a): the same fused
+// kernel (halation column pass, logistic curves, grain) with the two spectral
+// contractions as BF16 MMAs with FP32 accumulation and a hi/lo split of both
+// operands, per tile of 128 pixels (one warpgroup, one TMEM lane a pixel):
+//   MMA1  x[128 x 96] = A1[128 x 16] . B1[96 x 16]^T      (A1, B1 in SMEM)
+//         A1 row = (Dh, Dl, Dh, Dl) of the three layer densities, B1 row of
+//         bin l = (eh, eh, el, el) of -eps(l) (log2 units), so
+//         x = (Dh + Dl) . (eh + el) = -d(l) to f32 accuracy;
+//   T = 2^x per bin (MUFU), split into bf16 T = Th + Tl, written over x in TMEM;
+//   MMA2  rgb[128 x 16] += Th . Ch + Th . Cl + Tl . Ch    (A from TMEM, B in SMEM)
+//         over six K-blocks of 16 bins (81 bins padded to 96 with zeros).
+// Dropping Tl . Cl and bf16 rounding leave about 2^-17 relative per term.
+namespace tc {
+
+constexpr int NBP = 96;                   // bins padded to the MMA's granularity
+constexpr uint32_t SBO_K16 = 256;         // K = 16 tiles: two 128-byte K-groups per 8-row group
+constexpr uint32_t SBO_K96 = 1536;        // K = 96 tiles: twelve K-groups per 8-row group
+constexpr int B1_WORDS = NBP * 16 / 2;    // 96 bins x 16 bf16
+constexpr int B2_WORDS = 16 * NBP / 2;    // 16 channel rows (3 used) x 96 bins
+
+// Byte offset of bf16 element (row r, k) in a K-major tile without swizzle:
+// core matrices of 8 rows x 16 bytes, K-groups 128 bytes apart (LBO), 8-row
+// groups `sbo` apart.
+__host__ __device__ __forceinline__ uint32_t cm_off(int r, int k, uint32_t sbo) {
+    return (uint32_t)(r >> 3) * sbo + (uint32_t)(k >> 3) * 128u + (uint32_t)(r & 7) * 16u + (uint32_t)(k & 7) * 2u;
+}
+
+// B operands, already in their shared-memory layout
+struct Tables {
+    uint32_t b1[B1_WORDS];
+    uint32_t b2h[B2_WORDS];
+    uint32_t b2l[B2_WORDS];
+};
+
+// dynamic shared memory (bytes)
+constexpr uint32_t WIN_BYTES = (R64_COL_TH + 2 * HAL_R) * R64_COL_TW * 4;
+constexpr uint32_t OFF_TAB = WIN_BYTES;
+constexpr uint32_t OFF_B1 = OFF_TAB, OFF_B2H = OFF_B1 + B1_WORDS * 4, OFF_B2L = OFF_B2H + B2_WORDS * 4;
+constexpr uint32_t OFF_A1 = OFF_B2L + B2_WORDS * 4;  // two warpgroups x 128 rows x 16 bf16
+constexpr uint32_t OFF_BAR = OFF_A1 + 2 * 4096;      // four mbarriers
+constexpr uint32_t OFF_SLOT = OFF_BAR + 32;          // TMEM base address
+constexpr uint32_t SMEM_USED = OFF_SLOT + 16;
+// Requested per CTA: at most two CTAs an SM, whose 2 x 256 TMEM columns fit
+// the SM's 512, so no CTA waits in tcgen05.alloc for another to finish.
+constexpr uint32_t SMEM_REQ = 80 * 1024;
+static_assert(SMEM_USED <= SMEM_REQ && 3 * SMEM_REQ > 228 * 1024, "two CTAs an SM");
+
+// instruction descriptors: BF16 A and B (K-major), FP32 D, M = 128
+constexpr uint32_t idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+constexpr uint32_t IDESC_X = idesc(NBP), IDESC_RGB = idesc(16);
+
+constexpr int WAIT_LIMIT = 1 << 22;  // try_wait polls before an MMA is declared lost
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor, no swizzle, LBO 128 bytes
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t sbo) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_ss(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p; }"
+                 ::"r"(d), "l"(a), "l"(b), "r"(id), "r"(acc));
+}
+__device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p; }"
+                 ::"r"(d), "r"(a), "l"(b), "r"(id), "r"(acc));
+}
+__device__ __forceinline__ void commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+// Bounded wait for phase `parity` of an mbarrier: false when it gave up.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+    for (int it = 0; it < WAIT_LIMIT; it++) {
+        uint32_t ok;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
+__device__ __forceinline__ void ld16(uint32_t ta, uint32_t (&v)[16]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                 : "r"(ta));
+}
+__device__ __forceinline__ void ld4(uint32_t ta, uint32_t (&v)[4]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "r"(ta));
+}
+__device__ __forceinline__ void st8(uint32_t ta, const uint32_t (&v)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
+                 ::"r"(ta), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
+}
+__device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// bf16x2 of (a, b), round to nearest: a in the low half (the even K index)
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+}
+// hi = bf16(a), bf16(b); lo = bf16 of what hi leaves out
+__device__ __forceinline__ void split_bf16(float a, float b, uint32_t& hi, uint32_t& lo) {
+    hi = pack_bf16(a, b);
+    lo = pack_bf16(a - __uint_as_float(hi << 16), b - __uint_as_float(hi & 0xFFFF0000u));
+}
+
+}  // namespace tc
+
+struct Base81TC {
+    BaselineSpec B;
+    float2 tap2[2 * HAL_R + 2];
+    tc::Tables T;
+};
+
+// Lost MMA completions (a bounded wait that gave up), counted across launches.
+__device__ unsigned g_tc_timeouts = 0;
+
+__global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 2) scan81_tc_kernel(
+    const float* __restrict__ a, const float* __restrict__ hr, const float* __restrict__ noise,
+    const double* __restrict__ sumsq, int W, int H, const __grid_constant__ Base81TC c, float* __restrict__ rgb) {
+    using namespace tc;
+    static_assert(R64_COL_GROUPS == 8, "two warpgroups of four warps");
+    extern __shared__ __align__(1024) uint8_t dsm[];
+    float* s = reinterpret_cast<float*>(dsm);
+    const int x0 = blockIdx.x * R64_COL_TW, y0 = blockIdx.y * R64_COL_TH;
+    const int tx = threadIdx.x, ty = threadIdx.y, x = x0 + tx, tid = ty * 32 + tx;
+    const int g = ty >> 2;     // warpgroup
+    const int row = tid & 127; // this thread's MMA row (TMEM lane)
+    const uint32_t sb = smem_u32(dsm);
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&c.T);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(dsm + OFF_TAB);
+        for (int i = tid; i < (int)(sizeof(Tables) / 4); i += blockDim.x * blockDim.y) dst[i] = src[i];
+    }
+    if (x < W) stage_col_window<R64_COL_TH>(s, hr, W, H, x, y0, tx, ty);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(dsm + OFF_SLOT);
+    if (tid == 0) {
+        for (int i = 0; i < 4; i++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sb + OFF_BAR + 8 * i));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (ty == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(sb + OFF_SLOT));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tables are read by the MMAs
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tm = *slot + (uint32_t)(g * 128);                // this warpgroup's 128 columns
+    const uint32_t tl = tm + (((uint32_t)(ty & 3) * 32u) << 16);    // this warp's 32 lanes
+    const uint32_t bar_x = sb + OFF_BAR + 16 * g, bar_rgb = bar_x + 8;
+    const uint32_t a1 = sb + OFF_A1 + 4096u * g;
+    uint8_t* a1p = dsm + OFF_A1 + 4096u * g;
+
+    const size_t n = (size_t)W * H;
+    float norm[3] = {1.f, 1.f, 1.f};
+    if (c.B.grain_sigma > 0.0f)
+        for (int e = 0; e < 3; e++) {
+            double var = sumsq[e] / (double)n;
+            norm[e] = var > 1e-12 ? (float)(1.0 / sqrt(var)) : 1.0f;
+        }
+    const int rb = ty * R64_COL_OUT;
+    float2 bs[R64_COL_OUT / 2];
+#pragma unroll
+    for (int q = 0; q < R64_COL_OUT / 2; q++) bs[q] = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int m = 0; m < R64_COL_OUT + 2 * HAL_R; m++) {
+        const float v = s[(rb + m) * R64_COL_TW + tx];
+        const float2 vv = make_float2(v, v);
+#pragma unroll
+        for (int q = 0; q < R64_COL_OUT / 2; q++) {
+            const int k = m - 2 * q;
+            if (k >= 0 && k <= 2 * HAL_R + 1) bs[q] = __ffma2_rn(vv, c.tap2[k], bs[q]);
+        }
+    }
+    const bool grain = c.B.grain_sigma > 0.0f;
+    const bool xin = x < W;
+    uint32_t parity = 0;
+    bool alive = true;
+#pragma unroll 1
+    for (int j = 0; j < R64_COL_OUT; j++) {
+        const int y = y0 + rb + j;
+        const bool valid = xin && y < H;
+        float D[3] = {0.0f, 0.0f, 0.0f};
+        if (valid) {
+            const size_t p = (size_t)y * W + x;
+            float bsum = bs[0].x;
+#pragma unroll
+            for (int q = 0; q < R64_COL_OUT / 2; q++) {
+                if (2 * q == j) bsum = bs[q].x;
+                if (2 * q + 1 == j) bsum = bs[q].y;
+            }
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+                float E = a[e * n + p] + c.B.hal_strength * c.B.bleed[e] * bsum;
+                float le = log10f(fmaxf(E, 1e-6f));
+                D[e] = c.B.dmax[e] / (1.0f + expf(-c.B.k[e] * (le - c.B.x0[e])));
+                if (grain) D[e] += c.B.grain_sigma * noise[e * n + p] * norm[e];
+            }
+        }
+        // A1 row: k 0..11 = (Dh0 Dh1 Dh2 Dl0 Dl1 Dl2 Dh0 Dh1 Dh2 Dl0 Dl1 Dl2), 12..15 zero
+        {
+            uint32_t h01, l01, h2, l2;
+            split_bf16(D[0], D[1], h01, l01);
+            split_bf16(D[2], 0.0f, h2, l2);
+            const uint32_t w0 = h01, w1 = (h2 & 0xFFFFu) | (l01 << 16), w2 = (l01 >> 16) | (l2 << 16);
+            *reinterpret_cast<uint4*>(a1p + cm_off(row, 0, SBO_K16)) = make_uint4(w0, w1, w2, w0);
+            *reinterpret_cast<uint4*>(a1p + cm_off(row, 8, SBO_K16)) = make_uint4(w1, w2, 0u, 0u);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        wg_sync(1 + g);
+        if (row == 0 && alive) {
+            fence_after();
+            mma_ss(tm, sdesc(a1, SBO_K16), sdesc(sb + OFF_B1, SBO_K16), IDESC_X, 0u);
+            commit(bar_x);
+        }
+        if (alive && !bar_wait(bar_x, parity)) {
+            alive = false;
+            atomicAdd(&g_tc_timeouts, 1u);
+        }
+        fence_after();
+        // T = 2^x per bin, split to bf16 hi/lo over the same columns: K-block q
+        // (bins 16q .. 16q+15) keeps its hi words in columns 16q .. 16q+7 and
+        // its lo words in 16q+8 .. 16q+15
+#pragma unroll
+        for (int q = 0; q < NBP / 16; q++) {
+            uint32_t v[16], hw[8], lw[8];
+            ld16(tl + 16u * q, v);
+            wait_ld();
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int b0 = 16 * q + 2 * i;
+                const float t0 = b0 < NB81 ? ex2_fast(__uint_as_float(v[2 * i])) : 0.0f;
+                const float t1 = b0 + 1 < NB81 ? ex2_fast(__uint_as_float(v[2 * i + 1])) : 0.0f;
+                split_bf16(t0, t1, hw[i], lw[i]);
+            }
+            st8(tl + 16u * q, hw);
+            st8(tl + 16u * q + 8u, lw);
+        }
+        wait_st();
+        fence_before();
+        wg_sync(1 + g);
+        if (row == 0 && alive) {
+            fence_after();
+#pragma unroll
+            for (int q = 0; q < NBP / 16; q++) {
+                const uint64_t bh = sdesc(sb + OFF_B2H + 256u * q, SBO_K96), bl = sdesc(sb + OFF_B2L + 256u * q, SBO_K96);
+                mma_ts(tm + NBP, tm + 16u * q, bh, IDESC_RGB, q > 0 ? 1u : 0u);
+                mma_ts(tm + NBP, tm + 16u * q, bl, IDESC_RGB, 1u);
+                mma_ts(tm + NBP, tm + 16u * q + 8u, bh, IDESC_RGB, 1u);
+            }
+            commit(bar_rgb);
+        }
+        if (alive && !bar_wait(bar_rgb, parity)) {
+            alive = false;
+            atomicAdd(&g_tc_timeouts, 1u);
+        }
+        fence_after();
+        uint32_t o[4];
+        ld4(tl + NBP, o);
+        wait_ld();
+        if (valid) {
+            const size_t p = (size_t)y * W + x;
+            rgb[3 * p] = __uint_as_float(o[0]);
+            rgb[3 * p + 1] = __uint_as_float(o[1]);
+            rgb[3 * p + 2] = __uint_as_float(o[2]);
+        }
+        fence_before();
+        parity ^= 1u;
+    }
+    __syncthreads();
+    fence_after();
+    if (ty == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(*slot));
+}
+
+// Host: bf16 of an f32, round to nearest even (finite values)
+static uint16_t host_bf16(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+static float host_bf16_value(uint16_t h) {
+    uint32_t u = (uint32_t)h << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// Host: the tensor-core scan's B operands in their shared-memory layout.
+static void build_base81_tc(const Stock& st, Base81TC* hp) {
+    std::memset(hp, 0, sizeof(*hp));
+    hp->B = st.base;
+    for (int k = 0; k <= 2 * HAL_R + 1; k++)
+        hp->tap2[k] = make_float2(k <= 2 * HAL_R ? st.hal_taps[k] : 0.0f, k >= 1 ? st.hal_taps[k - 1] : 0.0f);
+    const ScanSpec81& S = st.scan81;
+    auto put = [](uint32_t* words, uint32_t byte_off, uint16_t v) {
+        reinterpret_cast<uint16_t*>(words)[byte_off / 2] = v;
+    };
+    for (int l = 0; l < NB81; l++)
+        for (int e = 0; e < 3; e++) {
+            const float ne = -S.eps[e][l];
+            const uint16_t hi = host_bf16(ne), lo = host_bf16(ne - host_bf16_value(hi));
+            // row l of B1 against A1's (Dh, Dl, Dh, Dl): (eh, eh, el, el)
+            put(hp->T.b1, tc::cm_off(l, e, tc::SBO_K16), hi);
+            put(hp->T.b1, tc::cm_off(l, 3 + e, tc::SBO_K16), hi);
+            put(hp->T.b1, tc::cm_off(l, 6 + e, tc::SBO_K16), lo);
+            put(hp->T.b1, tc::cm_off(l, 9 + e, tc::SBO_K16), lo);
+        }
+    for (int ch = 0; ch < 3; ch++)
+        for (int l = 0; l < NB81; l++) {
+            const float cv = S.C[l][ch];
+            const uint16_t hi = host_bf16(cv), lo = host_bf16(cv - host_bf16_value(hi));
+            put(hp->T.b2h, tc::cm_off(ch, l, tc::SBO_K96), hi);
+            put(hp->T.b2l, tc::cm_off(ch, l, tc::SBO_K96), lo);
+        }
 }
 
 // Host: the pair tables of the 81-bin scan and halation taps.
@@ -1036,20 +1410,43 @@ int stage_ctx(const ImopsFilmParams* P, int W, int H, size_t extra, cudaStream_t
 namespace imops {
 namespace film {
 
-// Baseline preset forward on an ACEScg image in place.
+// Bytes of the baseline preset's working set for a W x H image: the three
+// layer exposures, the halation source and its row pass, three grain fields,
+// the grain's block sums (and the Arena's 256-byte alignment).
+size_t baseline_scratch_bytes(int W, int H) {
+    const size_t n = (size_t)W * H;
+    return (3 + 1 + 1 + 3) * n * 4 + grain_partials(W, H, 3) * 8 + 4096;
+}
+
+int baseline_stock(int W, const ImopsBaselineFilm& P, Stock* st) {
+    if (P.scan != IMOPS_SCAN_FP32 && P.scan != IMOPS_SCAN_BF16_TC)
+        return fail(IMOPS_ERR_INVALID_ARGUMENT, "film: unknown scan (IMOPS_SCAN_FP32 or IMOPS_SCAN_BF16_TC)");
+    float pitch;
+    return build_stock(IMOPS_STOCK_BASELINE81, 0, W, -1.0f, &P, st, &pitch);
+}
+
+// Baseline preset forward on an ACEScg image in place, with the working set
+// in the library's per-(device, stream) workspace.
 int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp, cudaStream_t s) {
     ImopsBaselineFilm P;
     if (Pp) P = *Pp;
     else imops_baseline_film_defaults(&P);
     Stock st;
-    float pitch;
-    int rc = build_stock(IMOPS_STOCK_BASELINE81, 0, W, -1.0f, &P, &st, &pitch);
+    int rc = baseline_stock(W, P, &st);
     if (rc) return rc;
-    const size_t n = (size_t)W * H;
-    size_t bytes = (3 + 1 + 1 + 3) * n * 4 + grain_partials(W, H, 3) * 8 + 4096;
     void* ws = nullptr;
-    if ((rc = workspace(s, bytes, &ws))) return rc;
-    Arena A{static_cast<char*>(ws), 0};
+    if ((rc = workspace(s, baseline_scratch_bytes(W, H), &ws))) return rc;
+    return baseline_forward_in(rgb, W, H, P, st, ws, s);
+}
+
+// The baseline preset's kernels with the working set at `scratch` (256-byte
+// aligned, baseline_scratch_bytes(W, H) long).  Every byte the kernels read
+// there is written earlier in the same call.
+int baseline_forward_in(float* rgb, int W, int H, const ImopsBaselineFilm& P, const Stock& st, void* scratch,
+                        cudaStream_t s) {
+    int rc;
+    const size_t n = (size_t)W * H;
+    Arena A{static_cast<char*>(scratch), 0};
     double* sums = A.take<double>(4);
     float* a = A.take<float>(3 * n);
     float* hal = A.take<float>(n);
@@ -1068,7 +1465,16 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
         if ((rc = grain_fields(noise, W, H, P.seed, 0, 3, tp, gpart, sums, s))) return rc;
     }
     dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + R64_COL_TH - 1) / R64_COL_TH);
-    scan81_fused_kernel<<<cg, cb, 0, s>>>(a, hr, noise, sums, W, H, hp, rgb);
+    if (P.scan == IMOPS_SCAN_BF16_TC) {
+        Base81TC tp;
+        build_base81_tc(st, &tp);
+        IMOPS_CUDA_TRY(cudaFuncSetAttribute(scan81_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)tc::SMEM_REQ),
+                       "cudaFuncSetAttribute(tensor-core scan)");
+        scan81_tc_kernel<<<cg, cb, tc::SMEM_REQ, s>>>(a, hr, noise, sums, W, H, tp, rgb);
+    } else {
+        scan81_fused_kernel<<<cg, cb, 0, s>>>(a, hr, noise, sums, W, H, hp, rgb);
+    }
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "baseline film kernels");
     return IMOPS_OK;
@@ -1214,3 +1620,9 @@ extern "C" int imops_film_process(float* rgb, int w, int h, int color_space, con
     return film::process_reference(rgb, w, h, *params, s);
 }
 
+extern "C" int imops_tensor_timeouts(unsigned* count) {
+    clear_error();
+    if (!count) return fail(IMOPS_ERR_INVALID_ARGUMENT, "imops_tensor_timeouts: NULL output");
+    IMOPS_CUDA_TRY(cudaMemcpyFromSymbol(count, film::g_tc_timeouts, sizeof(unsigned)), "read tensor-core timeouts");
+    return IMOPS_OK;
+}

@@ -122,5 +122,13 @@ int grid_for_n(size_t n);
 // (film/mod.rs:155-166).
 float relative_to_absolute_y(float y, float box_iso);
 
+// The baseline 81-bin preset: its working-set size for a W x H image, its
+// stock description, and its kernels run with the working set at `scratch`
+// (256-byte aligned, at least baseline_scratch_bytes(W, H) bytes).
+size_t baseline_scratch_bytes(int W, int H);
+int baseline_stock(int W, const ImopsBaselineFilm& P, Stock* st);
+int baseline_forward_in(float* rgb, int W, int H, const ImopsBaselineFilm& P, const Stock& st, void* scratch,
+                        cudaStream_t s);
+
 }  // namespace film
 }  // namespace imops

@@ -669,4 +669,5 @@ extern "C" void imops_baseline_film_defaults(ImopsBaselineFilm* p) {
     p->grain_blur = 1.0f;
     p->grain_on = 1;
     p->seed = 1;
+    p->scan = IMOPS_SCAN_FP32;
 }

@@ -245,11 +245,12 @@ const char* cs_debug(const ImopsImage& img) {
 
 struct Demosaic : Module {
     int algorithm = IMOPS_DEMOSAIC_AMAZE;
-    // per-pixel modules fused into the output stage of AMaZE or the 3x3 mean
-    // by run_pixel_pipeline_c
-    color::Epilogue fused = color::identity_epilogue();
-    int fused_cs = IMOPS_CS_CAMERA;
-    int process(ImopsImage& img) override {
+    int process(ImopsImage& img) override { return process_fused(img, nullptr, IMOPS_CS_CAMERA); }
+    // `fused`: the per-pixel modules run_pixel_pipeline_c folds into the
+    // output stage of AMaZE or the 3x3 mean (nullptr: none), and the colour
+    // space they leave.  Passed per call, so one pipeline object keeps no
+    // per-image state.
+    int process_fused(ImopsImage& img, const color::Epilogue* fused, int fused_cs) {
         if (img.raw_kind == 0) return fail(IMOPS_ERR_INVALID_ARGUMENT, "Demosaic: the image has no raw data");
         if (img.cfa.empty()) return fail(IMOPS_ERR_INVALID_ARGUMENT, "A CFA must be set to demosaic raw images");
         const int w = (int)img.width, h = (int)img.height;
@@ -280,7 +281,7 @@ struct Demosaic : Module {
         if (algorithm == IMOPS_DEMOSAIC_AMAZE) {
             CfaDev c;
             if ((rc = parse_cfa(img.cfa.c_str(), cx, cy, &c))) return rc;
-            const color::Epilogue& e = fused;
+            const color::Epilogue e = fused ? *fused : color::identity_epilogue();
             if (img.raw_kind == 1) {
                 float bl[1] = {img.meta.black_level}, wh[1] = {img.meta.white_level};
                 rc = amaze::demosaic_color_u16(static_cast<const uint16_t*>(img.raw.p), (int)img.raw_w,
@@ -291,7 +292,7 @@ struct Demosaic : Module {
         } else if (algorithm == IMOPS_DEMOSAIC_MARKESTEIJN) {
             CfaDev c;
             rc = parse_cfa(img.cfa.c_str(), cx, cy, &c);
-            if (!rc) rc = simple::mean3x3(mosaic, w, h, c, &fused, rgb, s);
+            if (!rc) rc = simple::mean3x3(mosaic, w, h, c, fused, rgb, s);
         } else {
             int f = algorithm == IMOPS_DEMOSAIC_FAST ? 2 : (algorithm == IMOPS_DEMOSAIC_SUPERFAST ? 4 : 8);
             rc = imops_demosaic_quad(mosaic, w, h, img.cfa.c_str(), cx, cy, f, rgb, s);
@@ -308,8 +309,6 @@ struct Demosaic : Module {
         img.height = oh;
         img.has_cs = fused_cs != IMOPS_CS_CAMERA;
         img.color_space = fused_cs;
-        fused = color::identity_epilogue();
-        fused_cs = IMOPS_CS_CAMERA;
         return IMOPS_OK;
     }
 };
@@ -895,10 +894,15 @@ extern "C" ImopsImage* run_pixel_pipeline_c(ImopsImage* image, ImopsPipeline* pi
         }
         auto* dem = dynamic_cast<pipe::Demosaic*>(mods[k].get());
         size_t fused_until = k;
+        color::Epilogue fused = color::identity_epilogue();
+        int fused_cs = IMOPS_CS_CAMERA;
         if (dem && (dem->algorithm == IMOPS_DEMOSAIC_AMAZE || dem->algorithm == IMOPS_DEMOSAIC_MARKESTEIJN) &&
             image->raw_kind != 0 && !image->cfa.empty())
-            fused_until = pipe::plan_fusion(*image, mods, k, &dem->fused, &dem->fused_cs);
-        if (mods[k]->process(*image) != IMOPS_OK) return nullptr;
+            fused_until = pipe::plan_fusion(*image, mods, k, &fused, &fused_cs);
+        // nothing folded in: the demosaic keeps its plain output stage
+        const int rc = dem ? dem->process_fused(*image, fused_until > k ? &fused : nullptr, fused_cs)
+                           : mods[k]->process(*image);
+        if (rc != IMOPS_OK) return nullptr;
         k = fused_until;
     }
     // Returns once the work is queued on the image's stream: every call that

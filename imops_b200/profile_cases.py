@@ -1,7 +1,7 @@
 """Single-launch cases for profiling one kernel of the path under ncu.
 
   python -m imops_b200.profile_cases amaze --width 4096 --height 3072
-  python -m imops_b200.profile_cases film81 --width 4096 --height 3072
+  python -m imops_b200.profile_cases film81 --width 4096 --height 3072 [--scan bf16_tc]
   python -m imops_b200.profile_cases fwdbwd --width 6048 --height 4024
   python -m imops_b200.profile_cases display --width 6048 --height 4024
   python -m imops_b200.profile_cases xtrans --width 6032 --height 4032
@@ -21,6 +21,8 @@ def main() -> None:
     ap.add_argument("case", choices=["amaze", "film81", "develop", "fwdbwd", "display", "xtrans"])
     ap.add_argument("--width", type=int, default=4096)
     ap.add_argument("--height", type=int, default=3072)
+    ap.add_argument("--scan", choices=["fp32", "bf16_tc"], default="fp32",
+                    help="the 81-bin scan's contractions: CUDA cores (FP32) or tensor cores (BF16 hi/lo)")
     a = ap.parse_args()
 
     import torch
@@ -64,11 +66,12 @@ def main() -> None:
         p.calib_d65[i] = synthetic.CALIB_D65[i]
     p.film = 1 if a.case in ("develop", "display") else 0
     p.film_params = im.FilmParams(im.STOCK_BASELINE81, 0, 1, 0, -1.0, 1)
-    p.baseline = im.baseline_film_defaults()
+    scan = im.SCAN_BF16_TC if a.scan == "bf16_tc" else im.SCAN_FP32
+    p.baseline = im.baseline_film_defaults(scan=scan)
     out = im.develop_u16(raw, (0, 0, W, H), synthetic.BLACK, synthetic.WHITE, p)
     if a.case == "film81":
         torch.cuda.synchronize()
-        im.film_process(out, stock=im.STOCK_BASELINE81)
+        im.film_process(out, stock=im.STOCK_BASELINE81, baseline=im.baseline_film_defaults(scan=scan))
     if a.case == "display":
         # the display modules after the scan, one chain launch through the
         # pipeline C-ABI: Exp -> SigmoidToneMap -> CST LinearSrgb -> Gamma

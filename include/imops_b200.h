@@ -234,7 +234,16 @@ typedef struct {
     float grain_blur;       /* 1 px */
     int grain_on;
     uint64_t seed;
+    int scan;               /* IMOPS_SCAN_*: how the 81-bin scan contracts */
 } ImopsBaselineFilm;
+
+/* The baseline preset's 81-bin scan (densitometry.rs:13-73 on its grid):
+ * FP32: both spectral contractions as packed f32x2 FMAs on the CUDA cores;
+ * BF16_TC: both on the tensor cores (tcgen05), BF16 operands split hi + lo
+ * (three products per term), FP32 accumulation.  Both are within 1e-4 of
+ * the FP64 oracle. */
+#define IMOPS_SCAN_FP32 0
+#define IMOPS_SCAN_BF16_TC 1
 
 /* Defaults of the baseline preset (the benchmark workload's values). */
 void imops_baseline_film_defaults(ImopsBaselineFilm *out);
@@ -329,6 +338,12 @@ int imops_develop_f32(const float *mosaic, int w, int h, int shift_x, int shift_
 /* Number of kernels this library has launched in this process (evidence
  * counter for benchmarks; monotone, thread-safe). */
 uint64_t imops_launch_count(void);
+
+/* Tensor-core waits that gave up on the current device since the process
+ * started (a bounded wait for an MMA's completion expired; the kernel then
+ * skips its remaining MMAs and its output is not valid).  Waits for the
+ * device.  0 in normal operation. */
+int imops_tensor_timeouts(unsigned *count);
 
 /* ---- adjoints (no counterpart in the reference, which has no gradients) ----
  * Parameters of the differentiable colour + film model, from demosaiced

@@ -154,6 +154,19 @@ def markesteijn3(mosaic: np.ndarray, cfa: str, shift=(0, 0), precision: str = "f
     return out
 
 
+def xt_cbrt(t: np.ndarray, precision: str = "f32") -> np.ndarray:
+    """The division-free cube root of the 3-pass X-Trans Lab step
+    (oracle/xtrans.c ``xt_cbrt``, the same arithmetic as the kernel's)."""
+    dt = _dt(precision)
+    a = np.ascontiguousarray(t, dtype=dt)
+    out = np.empty_like(a)
+    fn = _f("oracle_xt_cbrt", precision)
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p]
+    fn.restype = None
+    fn(_ptr(a), a.size, _ptr(out))
+    return out
+
+
 def quad(mosaic: np.ndarray, cfa: str, factor: int, shift=(0, 0), precision: str = "f32"):
     dt = _dt(precision)
     m = np.ascontiguousarray(mosaic, dtype=dt)
@@ -457,3 +470,35 @@ def param_grad(x: np.ndarray, target: np.ndarray, params: OracleGrad, scale: flo
                    ctypes.POINTER(OracleBaseline), ctypes.c_double, ctypes.c_void_p]
     _check(fn(_ptr(xx), _ptr(tt), W, H, ctypes.byref(params), ctypes.byref(f), scale, _ptr(g)), "param_grad")
     return g
+
+
+LSB16 = 1.0 / 65535.0  # one 16-bit step of linear [0, 1]
+FLIP_LSB = 8.0  # colour errors above this are AMaZE taking another branch in f32 than in f64
+
+
+def error_figures(got: np.ndarray, ref64: np.ndarray, skip: np.ndarray | None = None) -> dict:
+    """Max and RMS absolute error of `got` against the FP64 oracle `ref64`,
+    in linear [0, 1] and in 16-bit LSB, over the pixels not in `skip` (an
+    (H, W) mask, e.g. AMaZE decision flips, counted apart)."""
+    e = np.abs(got.astype(np.float64) - ref64)
+    if skip is not None:
+        e = e[~skip]
+    mx, rms = float(e.max()), float(np.sqrt(np.mean(e * e)))
+    return {"max_abs": mx, "rms_abs": rms, "max_lsb": mx / LSB16, "rms_lsb": rms / LSB16}
+
+
+def decision_flips(colour_f32: np.ndarray, colour_f64: np.ndarray) -> np.ndarray:
+    """Pixels whose f32 colour forward is more than FLIP_LSB from the FP64
+    chain: AMaZE resolved a comparison differently in f32 than in f64."""
+    return (np.abs(colour_f32.astype(np.float64) - colour_f64) / LSB16).max(axis=2) > FLIP_LSB
+
+
+def colour_chain(raw: np.ndarray, black: float, white: float, wb_coeffs, calib, precision: str = "f64",
+                 threads: int = 0) -> np.ndarray:
+    """u16 frame -> black/white scaling -> AMaZE -> WB -> camera matrix to
+    ACEScg: the colour half of the 24 MP forward (f32: the reference's
+    operation order; f64: the FP64 oracle)."""
+    H, W = raw.shape
+    m = scale_u16(raw, (0, 0, W, H), black, white, precision=precision)
+    rgb = wb(amaze(m, "RGGB", precision=precision, threads=threads), wb_coeffs, precision=precision)
+    return camera_cst(rgb, calib, CS_ACESCG, precision=precision)

@@ -156,8 +156,12 @@ static real xt_refine(const XtImg *im, const real *G, const real *Rp, const real
 
 /* step 4: cube root of t > 0 as t * r * r, r = t^(-1/3) by Newton's method
  * for the reciprocal cube root, r <- r (4 - t r^3) / 3, which needs no
- * division.  First guess 0x54AAAAAA - bits(t) / 3: at most 8.2% high for the
- * t here, inside the iteration's convergence bound (t r^3 < 4). */
+ * division.  First guess 0x54AAAAAA - bits(t) / 3: a float's bit pattern is
+ * nearly a scaled, offset log2, so bits(t^p) ~ p bits(t) + (1 - p) bits(1.0f)
+ * (Blinn, "Floating-point tricks", IEEE CG&A 17(4), 1997), and for p = -1/3
+ * the offset (4/3) 0x3F800000 = 0x54AAAAAA.  The guess is 0 .. 8.17% high
+ * for every normal t (its error repeats every three binades), inside the
+ * iteration's convergence bound (t r^3 < 4). */
 static real xt_cbrt(real t)
 {
     float tf = (float)t;
@@ -187,6 +191,13 @@ static real xt_f(real t)
 {
     if (t > K(216.0) / K(24389.0)) return xt_cbrt(t);
     return K(7.787037037037037) * t + K(0.13793103448275862);
+}
+
+/* The cube root of step 4 over an array (tests check it against the exact
+ * cube root). */
+void OSYM(oracle_xt_cbrt)(const real *t, long n, real *out)
+{
+    for (long i = 0; i < n; i++) out[i] = xt_cbrt(t[i]);
 }
 
 static void xt_lab(real r, real g, real b, real lab[3])

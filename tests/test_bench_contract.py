@@ -29,3 +29,33 @@ def test_ncu_figures_parse():
     assert isinstance(traffic, int) and traffic > 0
     assert isinstance(inst, int) and inst > 0
     assert b.ncu_figure("no_such_figure") is None
+
+
+def _run_bench(*argv):
+    import json
+    import subprocess
+    import sys
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR",
+                                                             "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *argv], capture_output=True, text=True,
+                       timeout=300, env=env, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout  # rank 0 alone prints
+    return json.loads(lines[0])
+
+
+def test_gpus_flag_launches_ranks_itself():
+    """`python bench.py --gpus 2` without torchrun starts two ranks (torchrun
+    on 127.0.0.1); --dry-run keeps them on gloo with no GPU work.  Both ranks
+    take part in the max-over-ranks reduction and rank 0 reports n_gpus 2."""
+    for impl in ("imops_b200", "reference"):
+        line = _run_bench("--gpus", "2", "--dry-run", "--steps", "2", "--warmup", "1", "--impl", impl)
+        assert line["dry_run"] is True and line["impl"] == impl
+        assert line["n_gpus"] == 2 and line["ranks_reporting"] == 2
+        assert line["config"]["parallelism"] == "replicas x2"
+
+
+def test_single_rank_dry_run():
+    line = _run_bench("--dry-run", "--steps", "1", "--warmup", "1")
+    assert line["n_gpus"] == 1 and line["ranks_reporting"] == 1

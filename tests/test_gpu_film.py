@@ -83,18 +83,55 @@ def test_wrong_color_space_and_dimensions(gpu):
     assert e.value.code == 7
 
 
+@pytest.mark.parametrize("scan", [0, 1], ids=["fp32", "bf16_tc"])
 @pytest.mark.parametrize("grain_on", [0, 1])
-def test_baseline_preset_against_fp64_oracle(oracle_lib, gpu, grain_on):
+def test_baseline_preset_against_fp64_oracle(oracle_lib, gpu, grain_on, scan):
+    """The 81-bin preset with the scan's contractions on the CUDA cores
+    (FP32) and on the tensor cores (BF16 hi/lo, FP32 accumulation)."""
     import imops_b200 as im
     rng = np.random.default_rng(11)
     x = (rng.random((96, 160, 3)) * 1.1).astype(np.float32)  # relative ACEScg incl. highlights > 0.8
     x[20:40, 30:60] = 1.05
     p_or = oracle_lib.baseline_params(grain_on=grain_on, seed=5)
     ref = oracle_lib.film_baseline(x, p_or, precision="f64")
-    p = im.baseline_film_defaults(grain_on=grain_on, seed=5)
+    p = im.baseline_film_defaults(grain_on=grain_on, seed=5, scan=scan)
     out = _run(gpu, x, stock=im.STOCK_BASELINE81, baseline=p)
     err = np.abs(out - ref)
     assert err.max() < TOL, f"max {err.max():.3g} rms {np.sqrt((err**2).mean()):.3g}"
+
+
+@pytest.mark.parametrize("H,W", [(128, 32), (1, 1), (37, 45), (300, 1000), (257, 129)])
+def test_tensor_core_scan_shapes(oracle_lib, gpu, H, W):
+    """The tensor-core scan on frames that fill its 128-pixel MMA tiles
+    partly (columns past the width and rows past the height are computed as
+    zeros and not stored): within 1e-4 of the FP64 oracle, and no MMA
+    completion lost."""
+    import ctypes
+
+    import imops_b200 as im
+    x = (synthetic_scene(H, W, seed=H * 7 + W) * 1.2).astype(np.float32)
+    p_or = oracle_lib.baseline_params(grain_on=1, seed=9)
+    ref = oracle_lib.film_baseline(x, p_or, precision="f64")
+    p = im.baseline_film_defaults(grain_on=1, seed=9, scan=im.SCAN_BF16_TC)
+    out = _run(gpu, x, stock=im.STOCK_BASELINE81, baseline=p)
+    assert np.abs(out - ref).max() < TOL
+    n = ctypes.c_uint()
+    im.check(im.lib().imops_tensor_timeouts(ctypes.byref(n)))
+    assert n.value == 0
+
+
+def synthetic_scene(H, W, seed):
+    from imops_b200 import synthetic
+    return synthetic.scene(H, W, seed=seed)
+
+
+def test_scan_arm_rejects_unknown(gpu):
+    import torch
+    import imops_b200 as im
+    t = torch.zeros((8, 8, 3), device=gpu)
+    with pytest.raises(im.ImopsError) as e:
+        im.film_process(t, stock=im.STOCK_BASELINE81, baseline=im.baseline_film_defaults(scan=7))
+    assert e.value.code == 1
 
 
 # Portra400, Ektar100, FujiPro400H (7 emulsions), EktachromeE100 (reversal),

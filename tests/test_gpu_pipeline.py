@@ -190,3 +190,62 @@ def test_pipeline_errors(gpu):
     with pytest.raises(im.ImopsError) as e:
         run_pixel_pipeline(Image.from_rgb(rgb, -1, make_meta()), parse_config('[[pipeline_modules]]\nname = "CFACoeffs"\n'))
     assert "wb_coeffs" in e.value.message
+
+
+@pytest.mark.parametrize("pattern", ["RGGB", "XTRANS"])
+@pytest.mark.parametrize("raw_kind", ["u16", "f32"])
+@pytest.mark.parametrize("target", ["AcesCg", "Srgb"])
+def test_pipeline_markesteijn_fused_chain_variants(gpu, oracle_lib, pattern, raw_kind, target):
+    """Demosaic(markesteijn) + CFACoeffs + BaselineExposureCompensation + CST
+    fused into the 3x3 mean's store, on Bayer (the aligned RGGB kernel) and
+    X-Trans, from a u16 frame and from an f32 mosaic, frames wider than one
+    192-pixel warp run (the interior aligned path and the float4 stores):
+    bit-exact to the oracle chain for linear targets, sRGB within 1e-6 of
+    scale (its transfer function is the f32 pow)."""
+    from imops_b200.pipeline import Image, parse_config, run_pixel_pipeline
+    cfa = synthetic.XTRANS if pattern == "XTRANS" else "RGGB"
+    H, W, crop = 70, 430, (3, 2, 418, 60)
+    cfg = ('[[pipeline_modules]]\nname = "Demosaic"\nalgorithm = "markesteijn"\n'
+           '[[pipeline_modules]]\nname = "CFACoeffs"\n'
+           '[[pipeline_modules]]\nname = "BaselineExposureCompensation"\n'
+           f'[[pipeline_modules]]\nname = "CST"\ntarget_color_space = "{target}"\n')
+    meta = dict(cfa=cfa, baseline_exposure=0.3, shutter=1 / 250, f_number=5.6, iso=400.0)
+    if raw_kind == "u16":
+        raw = synthetic.mosaic_u16(H, W, seed=35, pattern=cfa)
+        img = Image.from_u16(raw, _meta(crop=crop, **meta))
+        m = oracle_lib.scale_u16(raw, crop, synthetic.BLACK, synthetic.WHITE, cfa_period=(1, 1))
+    else:
+        full = synthetic.mosaic_f32(H, W, seed=35, pattern=cfa)
+        m = np.ascontiguousarray(full[crop[1]:crop[1] + crop[3], crop[0]:crop[0] + crop[2]])
+        img = Image.from_mosaic(m, _meta(crop=(crop[0], crop[1], 0, 0), **meta))
+    run_pixel_pipeline(img, parse_config(cfg))
+    got = img.rgb_f32()
+    ref = oracle_lib.mean3x3(m, cfa, shift=crop[:2])
+    ref = oracle_lib.wb(ref, synthetic.WB)
+    ref, applied = oracle_lib.baseline_exposure(ref, 0.3, 1 / 250, 5.6, 400.0)
+    assert applied
+    cs = oracle_lib.CS_SRGB if target == "Srgb" else oracle_lib.CS_ACESCG
+    ref = oracle_lib.camera_cst(ref, synthetic.CALIB_D65, cs)
+    assert got.shape == (crop[3], crop[2], 3)
+    if target == "Srgb":
+        scale = np.abs(ref).max(axis=2, keepdims=True) + 1e-3
+        assert (np.abs(got - ref) / scale).max() < 1e-6
+    else:
+        assert np.array_equal(got, ref)
+
+
+def test_pipeline_markesteijn_nothing_fused(gpu, oracle_lib):
+    """A 3x3-mean Demosaic followed by no foldable module keeps its plain
+    output stage: equal to the mean itself, then Contrast as its own pass."""
+    from imops_b200.pipeline import Image, parse_config, run_pixel_pipeline
+    m = synthetic.mosaic_f32(64, 400, seed=36, pattern=synthetic.XTRANS)
+    cfg = ('[[pipeline_modules]]\nname = "Demosaic"\nalgorithm = "markesteijn"\n'
+           '[[pipeline_modules]]\nname = "Contrast"\nc = 1.2\n')
+    img = Image.from_mosaic(m, _meta(cfa=synthetic.XTRANS))
+    run_pixel_pipeline(img, parse_config(cfg))
+    got = img.rgb_f32()
+    ref = oracle_lib.contrast(oracle_lib.mean3x3(m, synthetic.XTRANS), 1.2)
+    nan = np.isnan(ref)  # negative means (sensor noise below black) to a fractional power
+    assert np.array_equal(np.isnan(got), nan)
+    assert np.abs(got[~nan] - ref[~nan]).max() <= 2e-5 * max(1.0, float(np.abs(ref[~nan]).max()))
+    assert img.info()[2] == -1  # camera RGB: no colour space set

@@ -18,3 +18,18 @@ def test_frame_specs():
         assert 11.9e6 <= W * H <= 45e6
         if s["sensor"] == "bayer":
             assert im.amaze_size_supported(W, H)
+
+
+def test_balanced_bins_split_the_batch():
+    """Size-balanced bins over ranks: every frame in exactly one bin, the same
+    split on every rank, and the largest bin within one frame of the mean
+    load (the greedy bound)."""
+    from experiments.uneven_batch import balanced_bins, frame_cost
+    specs = [frame_spec(i, im.amaze_size_supported) for i in range(16)]
+    for world in (1, 2, 3, 4, 8):
+        bins = balanced_bins(specs, world)
+        assert bins == balanced_bins(specs, world)
+        assert sorted(i for b in bins for i in b) == list(range(16))
+        loads = [sum(frame_cost(specs[i]) for i in b) for b in bins]
+        assert max(loads) <= sum(loads) / world + max(frame_cost(s) for s in specs)
+    assert balanced_bins(specs, 1) == [list(range(16))]
