@@ -1388,27 +1388,3 @@ extern "C" int imops_demosaic_amaze(const float* mosaic, int w, int h, const cha
     amaze::EpiRGB epi{rgb, w};
     return amaze::launch(amaze::SrcF32{mosaic, w}, w, h, c, clip_pt, epi, as_stream(stream));
 }
-
-// ---------------------------------------------------------------------------
-// No-allocation entry point.
-//
-// Some callers cannot call cudaMalloc: code recording work into a CUDA graph
-// (allocation is not a stream operation), host applications whose device
-// memory is owned by their own allocator or budget, and latency-critical
-// paths where cudaMalloc's implicit device synchronisation is unacceptable.
-// The AMaZE kernel keeps every per-tile array in shared memory, so it needs
-// no device scratch at all; imops_demosaic_amaze_noalloc states that as a
-// contract (imops_demosaic_amaze happens to allocate nothing either, but does
-// not promise it).  The first call on a device sets the kernel's
-// shared-memory limit (cudaFuncSetAttribute) and loads it: make that call
-// before any stream capture.
-extern "C" int imops_demosaic_amaze_noalloc(const float* mosaic, int w, int h, const char* cfa, int shift_x,
-                                            int shift_y, float clip_pt, float* rgb, imops_stream_t stream) {
-    using namespace imops;
-    clear_error();
-    CfaDev c;
-    int rc = parse_cfa(cfa, shift_x, shift_y, &c);
-    if (rc) return rc;
-    if (!mosaic || !rgb) return fail(IMOPS_ERR_INVALID_ARGUMENT, "AMaZE no-alloc: NULL buffer");
-    return amaze::launch(amaze::SrcF32{mosaic, w}, w, h, c, clip_pt, amaze::EpiRGB{rgb, w}, as_stream(stream));
-}

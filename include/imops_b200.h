@@ -97,19 +97,6 @@ int imops_scale_u16(const uint16_t *raw, int raw_w, int raw_h, int crop_x, int c
 int imops_demosaic_amaze(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y, float clip_pt,
                          float *rgb, imops_stream_t stream);
 
-/* AMaZE without any device allocation (no counterpart in the reference):
- * for callers that cannot call cudaMalloc -- work being captured into a CUDA
- * graph, host applications that own all device memory through their own
- * allocator, or latency-critical paths that cannot afford cudaMalloc's
- * implicit synchronisation.  Output is identical to imops_demosaic_amaze.
- * The kernel keeps all per-tile state in shared memory, so there is no
- * scratch and no size limit beyond imops_amaze_size_supported.  The first
- * call on a device sets the kernel's shared-memory limit
- * (cudaFuncSetAttribute) and loads it: make that first call before any
- * stream capture.  Calls on different streams may overlap. */
-int imops_demosaic_amaze_noalloc(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y,
-                                 float clip_pt, float *rgb, imops_stream_t stream);
-
 /* Whether imops_demosaic_amaze accepts a w x h image (host-only check). */
 int imops_amaze_size_supported(int w, int h);
 
@@ -258,6 +245,31 @@ void imops_baseline_film_defaults(ImopsBaselineFilm *out);
  * library-owned per-stream workspace (allocated on first use). */
 int imops_film_process(float *rgb, int w, int h, int color_space, const ImopsFilmParams *params,
                        const ImopsBaselineFilm *baseline, imops_stream_t stream);
+
+/* The baseline preset of imops_film_process (stock IMOPS_STOCK_BASELINE81)
+ * without any device allocation.  No counterpart in the reference.  For
+ * callers that cannot call cudaMalloc: a host application that gives the GPU
+ * a fixed memory budget through its own allocator must not have the library
+ * allocate behind its back, and a real-time preview loop cannot take the
+ * device-wide synchronisation cudaMalloc and cudaFree may cause.  The
+ * preset's working planes (32 bytes a pixel) live in one fixed array of
+ * device memory, about 65 MiB, which every GPU that loads the library holds
+ * until the process exits; the caller still passes the image.
+ *  - Images above imops_film_noalloc_max_pixels() pixels (2,097,152: a
+ *    1920 x 1080 preview fits) are rejected with IMOPS_ERR_UNSUPPORTED_SIZE.
+ *  - Output equals imops_film_process with the same preset.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) and caches it: make that first call on each
+ *    device before any stream capture.
+ *  - Every call shares the array and it keeps the last call's contents
+ *    (each call writes all it reads there): calls that may overlap on the
+ *    GPU -- on different streams, or from different threads -- race and
+ *    corrupt each other; order them on one stream or with events. */
+int imops_film_baseline_noalloc(float *rgb, int w, int h, int color_space, const ImopsBaselineFilm *baseline,
+                                imops_stream_t stream);
+
+/* Largest image, in pixels, that imops_film_baseline_noalloc accepts. */
+size_t imops_film_noalloc_max_pixels(void);
 
 /* ---- the reference model's film sub-stages -----------------------------------
  * The stages that film::process (film/mod.rs:77-129) chains, one call each,
