@@ -480,16 +480,34 @@ __global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restri
     const bool inner = x0 - R >= 0 && y0 - R >= 0 && x0 + GR_TW + R <= W && y0 + GR_TH + R <= H;
     float v[LAYERS];
     if (inner) {
-        for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
+        // two samples a thread and iteration (idx and idx + GR_THREADS): two
+        // independent SplitMix64 chains in flight
+        int idx = tid;
+        for (; idx + GR_THREADS < NH * NW; idx += 2 * GR_THREADS) {
+            int r2 = r + dq, c2 = c + dr;
+            if (c2 >= NW) {
+                c2 -= NW;
+                r2++;
+            }
+            float v2[LAYERS];
             grain_noise_at<LAYERS>(seed, layer0, y0 - R + r, x0 - R + c, v);
+            grain_noise_at<LAYERS>(seed, layer0, y0 - R + r2, x0 - R + c2, v2);
 #pragma unroll
-            for (int z = 0; z < LAYERS; z++) sn[z * NH * NW + idx] = v[z];
-            r += dq;
-            c += dr;
+            for (int z = 0; z < LAYERS; z++) {
+                sn[z * NH * NW + idx] = v[z];
+                sn[z * NH * NW + idx + GR_THREADS] = v2[z];
+            }
+            r = r2 + dq;
+            c = c2 + dr;
             if (c >= NW) {
                 c -= NW;
                 r++;
             }
+        }
+        if (idx < NH * NW) {
+            grain_noise_at<LAYERS>(seed, layer0, y0 - R + r, x0 - R + c, v);
+#pragma unroll
+            for (int z = 0; z < LAYERS; z++) sn[z * NH * NW + idx] = v[z];
         }
     } else {
         for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
@@ -724,13 +742,6 @@ struct Base81 {
     float2 tap2[2 * HAL_R + 2];
 };
 
-// -d of bins 2l, 2l+1 for the negated densities (nD0, nD1, nD2) broadcast.
-__device__ __forceinline__ float2 neg_density2(const Pairs81& P, int l, float2 d0, float2 d1, float2 d2) {
-    float2 x = __fmul2_rn(d0, P.ne[0][l]);
-    x = __ffma2_rn(d1, P.ne[1][l], x);
-    return __ffma2_rn(d2, P.ne[2][l], x);
-}
-
 // One thread per 16 consecutive rows of a column: the halation column pass
 // (register sliding window, tap pairs as parameter-bank operands, ascending
 // tap order as in blur_cols), then per pixel the logistic curves, grain and
@@ -769,62 +780,90 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
             if (k >= 0 && k <= 2 * HAL_R + 1) bs[q] = __ffma2_rn(vv, c.tap2[k], bs[q]);
         }
     }
-    // the exposure and noise of the next pixel are loaded while this one is
-    // scanned, so the global-load latency hides behind the 81-bin loop
+    // Two pixels (rows j and j+1 of the column) a step: each table pair is
+    // fetched once for both, and the next step's exposure and noise are
+    // loaded while this step is scanned, so the global-load latency hides
+    // behind the 81-bin loop.  Each pixel's arithmetic is unchanged.
+    static_assert(R64_COL_OUT % 2 == 0, "pixels go in pairs");
     const bool grain = c.B.grain_sigma > 0.0f;
-    float na[3], nz[3] = {0.f, 0.f, 0.f};
-    {
-        const size_t p0 = (size_t)min(y0 + rb, H - 1) * W + x;
+    float na[2][3], nz[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    auto fetch = [&](int jj) {  // rows jj, jj+1 (clamped to the image)
 #pragma unroll
-        for (int e = 0; e < 3; e++) {
-            na[e] = a[e * n + p0];
-            if (grain) nz[e] = noise[e * n + p0];
-        }
-    }
-#pragma unroll 1
-    for (int j = 0; j < R64_COL_OUT; j++) {
-        const int y = y0 + rb + j;
-        if (y >= H) break;
-        const size_t p = (size_t)y * W + x;
-        const float ca[3] = {na[0], na[1], na[2]}, cz[3] = {nz[0], nz[1], nz[2]};
-        if (j + 1 < R64_COL_OUT && y + 1 < H) {
+        for (int u = 0; u < 2; u++) {
+            const size_t pp = (size_t)min(y0 + rb + jj + u, H - 1) * W + x;
 #pragma unroll
             for (int e = 0; e < 3; e++) {
-                na[e] = a[e * n + p + W];
-                if (grain) nz[e] = noise[e * n + p + W];
+                na[u][e] = a[e * n + pp];
+                if (grain) nz[u][e] = noise[e * n + pp];
             }
         }
-        float bsum = bs[0].x;
+    };
+    fetch(0);
+#pragma unroll 1
+    for (int j = 0; j < R64_COL_OUT; j += 2) {
+        const int y = y0 + rb + j;
+        if (y >= H) break;
+        float ca[2][3], cz[2][3];
 #pragma unroll
-        for (int q = 0; q < R64_COL_OUT / 2; q++) {
-            if (2 * q == j) bsum = bs[q].x;
-            if (2 * q + 1 == j) bsum = bs[q].y;
-        }
-        float D[3];
+        for (int u = 0; u < 2; u++)
 #pragma unroll
-        for (int e = 0; e < 3; e++) {
-            float E = ca[e] + c.B.hal_strength * c.B.bleed[e] * bsum;
-            float le = log10f(fmaxf(E, 1e-6f));
-            D[e] = c.B.dmax[e] / (1.0f + expf(-c.B.k[e] * (le - c.B.x0[e])));
-            if (grain) D[e] += c.B.grain_sigma * cz[e] * norm[e];
-        }
-        const float2 d0 = make_float2(D[0], D[0]), d1 = make_float2(D[1], D[1]), d2 = make_float2(D[2], D[2]);
-        float2 o0 = make_float2(0.f, 0.f), o1 = o0, o2 = o0;
+            for (int e = 0; e < 3; e++) {
+                ca[u][e] = na[u][e];
+                cz[u][e] = nz[u][e];
+            }
+        if (j + 2 < R64_COL_OUT && y + 2 < H) fetch(j + 2);
+        float bsum[2] = {bs[0].x, bs[0].y};
+#pragma unroll
+        for (int q = 0; q < R64_COL_OUT / 2; q++)
+            if (2 * q == j) {
+                bsum[0] = bs[q].x;
+                bsum[1] = bs[q].y;
+            }
+        float D[2][3];
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+                float E = ca[u][e] + c.B.hal_strength * c.B.bleed[e] * bsum[u];
+                float le = log10f(fmaxf(E, 1e-6f));
+                D[u][e] = c.B.dmax[e] / (1.0f + expf(-c.B.k[e] * (le - c.B.x0[e])));
+                if (grain) D[u][e] += c.B.grain_sigma * cz[u][e] * norm[e];
+            }
+        float2 d[2][3], o[2][3];
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+                d[u][e] = make_float2(D[u][e], D[u][e]);
+                o[u][e] = make_float2(0.f, 0.f);
+            }
 #pragma unroll
         for (int l = 0; l < NP81; l++) {
-            const float2 xd = neg_density2(c.P, l, d0, d1, d2);
-            const float2 t = make_float2(ex2_fast(xd.x), ex2_fast(xd.y));
-            o0 = __ffma2_rn(c.P.C2[0][l], t, o0);
-            o1 = __ffma2_rn(c.P.C2[1][l], t, o1);
-            o2 = __ffma2_rn(c.P.C2[2][l], t, o2);
+            const float2 n0 = c.P.ne[0][l], n1 = c.P.ne[1][l], n2 = c.P.ne[2][l];
+            const float2 c0 = c.P.C2[0][l], c1 = c.P.C2[1][l], c2 = c.P.C2[2][l];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                float2 xd = __fmul2_rn(d[u][0], n0);
+                xd = __ffma2_rn(d[u][1], n1, xd);
+                xd = __ffma2_rn(d[u][2], n2, xd);
+                const float2 t = make_float2(ex2_fast(xd.x), ex2_fast(xd.y));
+                o[u][0] = __ffma2_rn(c0, t, o[u][0]);
+                o[u][1] = __ffma2_rn(c1, t, o[u][1]);
+                o[u][2] = __ffma2_rn(c2, t, o[u][2]);
+            }
         }
-        float xl = D[0] * c.P.ne_last[0];
-        xl = fmaf(D[1], c.P.ne_last[1], xl);
-        xl = fmaf(D[2], c.P.ne_last[2], xl);
-        const float tl = ex2_fast(xl);
-        rgb[3 * p] = fmaf(c.P.C_last[0], tl, o0.x + o0.y);
-        rgb[3 * p + 1] = fmaf(c.P.C_last[1], tl, o1.x + o1.y);
-        rgb[3 * p + 2] = fmaf(c.P.C_last[2], tl, o2.x + o2.y);
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            if (y + u >= H) break;
+            float xl = D[u][0] * c.P.ne_last[0];
+            xl = fmaf(D[u][1], c.P.ne_last[1], xl);
+            xl = fmaf(D[u][2], c.P.ne_last[2], xl);
+            const float tl = ex2_fast(xl);
+            const size_t p = (size_t)(y + u) * W + x;
+            rgb[3 * p] = fmaf(c.P.C_last[0], tl, o[u][0].x + o[u][0].y);
+            rgb[3 * p + 1] = fmaf(c.P.C_last[1], tl, o[u][1].x + o[u][1].y);
+            rgb[3 * p + 2] = fmaf(c.P.C_last[2], tl, o[u][2].x + o[u][2].y);
+        }
     }
 }
 
@@ -882,7 +921,10 @@ constexpr uint32_t idesc(int n) {
 }
 constexpr uint32_t IDESC_X = idesc(NBP), IDESC_RGB = idesc(16);
 
-constexpr int WAIT_LIMIT = 1 << 22;  // try_wait polls before an MMA is declared lost
+// try_wait suspends the warp until the phase completes or about SUSPEND_NS
+// pass; after WAIT_LIMIT tries (about a second) the MMA is declared lost
+constexpr int WAIT_LIMIT = 1 << 10;
+constexpr uint32_t SUSPEND_NS = 1000000;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -907,8 +949,9 @@ __device__ __forceinline__ void commit(uint32_t bar) {
 __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
     for (int it = 0; it < WAIT_LIMIT; it++) {
         uint32_t ok;
-        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-                     : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; selp.u32 %0, 1, 0, p; }"
+            : "=r"(ok) : "r"(bar), "r"(parity), "r"(SUSPEND_NS) : "memory");
         if (ok) return true;
     }
     return false;
@@ -1019,67 +1062,96 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 2) scan81_tc_kern
     }
     const bool grain = c.B.grain_sigma > 0.0f;
     const bool xin = x < W;
-    uint32_t parity = 0;
-    bool alive = true;
-#pragma unroll 1
-    for (int j = 0; j < R64_COL_OUT; j++) {
-        const int y = y0 + rb + j;
-        const bool valid = xin && y < H;
+    // Per step j (row y0 + rb + j of every warp: 128 pixels a warpgroup) the
+    // MMAs of one step overlap the CUDA-core work of its neighbours: MMA2 of
+    // step j runs while the densities of step j+1 are formed, MMA1 of step
+    // j+1 while step j's pixels are stored.  Exposure and noise are loaded a
+    // step ahead.
+    float la[3] = {0.f, 0.f, 0.f}, lz[3] = {0.f, 0.f, 0.f};  // inputs of the next step
+    auto load_inputs = [&](int jj) {
+        const int yy = y0 + rb + jj;
+        if (xin && yy < H && jj < R64_COL_OUT) {
+            const size_t p = (size_t)yy * W + x;
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+                la[e] = a[e * n + p];
+                lz[e] = grain ? noise[e * n + p] : 0.0f;
+            }
+        }
+    };
+    // densities of step jj into A1 (k 0..11 = Dh0 Dh1 Dh2 Dl0 Dl1 Dl2 Dh0 Dh1
+    // Dh2 Dl0 Dl1 Dl2, 12..15 zero), from the inputs loaded for it
+    auto write_a1 = [&](int jj) {
+        const int yy = y0 + rb + jj;
         float D[3] = {0.0f, 0.0f, 0.0f};
-        if (valid) {
-            const size_t p = (size_t)y * W + x;
+        if (xin && yy < H) {
             float bsum = bs[0].x;
 #pragma unroll
             for (int q = 0; q < R64_COL_OUT / 2; q++) {
-                if (2 * q == j) bsum = bs[q].x;
-                if (2 * q + 1 == j) bsum = bs[q].y;
+                if (2 * q == jj) bsum = bs[q].x;
+                if (2 * q + 1 == jj) bsum = bs[q].y;
             }
 #pragma unroll
             for (int e = 0; e < 3; e++) {
-                float E = a[e * n + p] + c.B.hal_strength * c.B.bleed[e] * bsum;
+                float E = la[e] + c.B.hal_strength * c.B.bleed[e] * bsum;
                 float le = log10f(fmaxf(E, 1e-6f));
                 D[e] = c.B.dmax[e] / (1.0f + expf(-c.B.k[e] * (le - c.B.x0[e])));
-                if (grain) D[e] += c.B.grain_sigma * noise[e * n + p] * norm[e];
+                if (grain) D[e] += c.B.grain_sigma * lz[e] * norm[e];
             }
         }
-        // A1 row: k 0..11 = (Dh0 Dh1 Dh2 Dl0 Dl1 Dl2 Dh0 Dh1 Dh2 Dl0 Dl1 Dl2), 12..15 zero
-        {
-            uint32_t h01, l01, h2, l2;
-            split_bf16(D[0], D[1], h01, l01);
-            split_bf16(D[2], 0.0f, h2, l2);
-            const uint32_t w0 = h01, w1 = (h2 & 0xFFFFu) | (l01 << 16), w2 = (l01 >> 16) | (l2 << 16);
-            *reinterpret_cast<uint4*>(a1p + cm_off(row, 0, SBO_K16)) = make_uint4(w0, w1, w2, w0);
-            *reinterpret_cast<uint4*>(a1p + cm_off(row, 8, SBO_K16)) = make_uint4(w1, w2, 0u, 0u);
-        }
+        uint32_t h01, l01, h2, l2;
+        split_bf16(D[0], D[1], h01, l01);
+        split_bf16(D[2], 0.0f, h2, l2);
+        const uint32_t w0 = h01, w1 = (h2 & 0xFFFFu) | (l01 << 16), w2 = (l01 >> 16) | (l2 << 16);
+        *reinterpret_cast<uint4*>(a1p + cm_off(row, 0, SBO_K16)) = make_uint4(w0, w1, w2, w0);
+        *reinterpret_cast<uint4*>(a1p + cm_off(row, 8, SBO_K16)) = make_uint4(w1, w2, 0u, 0u);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        wg_sync(1 + g);
-        if (row == 0 && alive) {
-            fence_after();
-            mma_ss(tm, sdesc(a1, SBO_K16), sdesc(sb + OFF_B1, SBO_K16), IDESC_X, 0u);
-            commit(bar_x);
-        }
-        if (alive && !bar_wait(bar_x, parity)) {
+    };
+    bool alive = true;
+    auto wait_for = [&](uint32_t bar, uint32_t parity) {
+        if (alive && !bar_wait(bar, parity)) {
             alive = false;
             atomicAdd(&g_tc_timeouts, 1u);
         }
         fence_after();
-        // T = 2^x per bin, split to bf16 hi/lo over the same columns: K-block q
-        // (bins 16q .. 16q+15) keeps its hi words in columns 16q .. 16q+7 and
-        // its lo words in 16q+8 .. 16q+15
+    };
+
+    load_inputs(0);
+    write_a1(0);
+    load_inputs(1);
+    wg_sync(1 + g);
+    if (row == 0) {
+        fence_after();
+        mma_ss(tm, sdesc(a1, SBO_K16), sdesc(sb + OFF_B1, SBO_K16), IDESC_X, 0u);
+        commit(bar_x);
+    }
+#pragma unroll 1
+    for (int j = 0; j < R64_COL_OUT; j++) {
+        const uint32_t parity = (uint32_t)j & 1u;
+        wait_for(bar_x, parity);
+        // T = 2^x per bin, split to bf16 hi/lo over the same columns: K-block
+        // q (bins 16q .. 16q+15) keeps its hi words in columns 16q .. 16q+7
+        // and its lo words in 16q+8 .. 16q+15.  Three K-blocks a batch of
+        // TMEM loads, one wait each.
 #pragma unroll
-        for (int q = 0; q < NBP / 16; q++) {
-            uint32_t v[16], hw[8], lw[8];
-            ld16(tl + 16u * q, v);
+        for (int h = 0; h < 2; h++) {
+            uint32_t v[3][16];
+#pragma unroll
+            for (int q = 0; q < 3; q++) ld16(tl + 16u * (3 * h + q), v[q]);
             wait_ld();
 #pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int b0 = 16 * q + 2 * i;
-                const float t0 = b0 < NB81 ? ex2_fast(__uint_as_float(v[2 * i])) : 0.0f;
-                const float t1 = b0 + 1 < NB81 ? ex2_fast(__uint_as_float(v[2 * i + 1])) : 0.0f;
-                split_bf16(t0, t1, hw[i], lw[i]);
+            for (int q = 0; q < 3; q++) {
+                uint32_t hw[8], lw[8];
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int b0 = 16 * (3 * h + q) + 2 * i;
+                    const float t0 = b0 < NB81 ? ex2_fast(__uint_as_float(v[q][2 * i])) : 0.0f;
+                    const float t1 = b0 + 1 < NB81 ? ex2_fast(__uint_as_float(v[q][2 * i + 1])) : 0.0f;
+                    split_bf16(t0, t1, hw[i], lw[i]);
+                }
+                st8(tl + 16u * (3 * h + q), hw);
+                st8(tl + 16u * (3 * h + q) + 8u, lw);
             }
-            st8(tl + 16u * q, hw);
-            st8(tl + 16u * q + 8u, lw);
         }
         wait_st();
         fence_before();
@@ -1095,22 +1167,29 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 2) scan81_tc_kern
             }
             commit(bar_rgb);
         }
-        if (alive && !bar_wait(bar_rgb, parity)) {
-            alive = false;
-            atomicAdd(&g_tc_timeouts, 1u);
+        // next step's densities while MMA2 runs (A1 is free: MMA1 of this step is done)
+        if (j + 1 < R64_COL_OUT) {
+            write_a1(j + 1);
+            load_inputs(j + 2);
         }
-        fence_after();
+        wait_for(bar_rgb, parity);
         uint32_t o[4];
         ld4(tl + NBP, o);
         wait_ld();
-        if (valid) {
+        fence_before();
+        wg_sync(1 + g);  // A1 of the next step written; this step's rgb read from TMEM
+        if (j + 1 < R64_COL_OUT && row == 0 && alive) {
+            fence_after();
+            mma_ss(tm, sdesc(a1, SBO_K16), sdesc(sb + OFF_B1, SBO_K16), IDESC_X, 0u);
+            commit(bar_x);
+        }
+        const int y = y0 + rb + j;
+        if (xin && y < H) {
             const size_t p = (size_t)y * W + x;
             rgb[3 * p] = __uint_as_float(o[0]);
             rgb[3 * p + 1] = __uint_as_float(o[1]);
             rgb[3 * p + 2] = __uint_as_float(o[2]);
         }
-        fence_before();
-        parity ^= 1u;
     }
     __syncthreads();
     fence_after();

@@ -49,6 +49,9 @@ struct DevState {
     cudaStream_t streams[POOL_STREAMS] = {};
     cudaMemPool_t pool = nullptr;
     unsigned next = 0;
+    // end of the last queued pipeline run's kernels (see order_compute)
+    cudaEvent_t compute_done = nullptr;
+    bool has_compute = false;
 };
 std::mutex g_dev_mu;
 DevState g_dev[128];
@@ -78,14 +81,18 @@ int dev_state(DevState** out) {
         if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &off);
         if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &off);
+        cudaEvent_t ev = nullptr;
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         if (e != cudaSuccess) {
             for (int i = 0; i < POOL_STREAMS; i++)
                 if (st[i]) cudaStreamDestroy(st[i]);
             if (pool) cudaMemPoolDestroy(pool);
+            if (ev) cudaEventDestroy(ev);
             return fail(IMOPS_ERR_CUDA, std::string("image streams / pool: ") + cudaGetErrorString(e));
         }
         for (int i = 0; i < POOL_STREAMS; i++) d.streams[i] = st[i];
         d.pool = pool;
+        d.compute_done = ev;
         d.init = true;
     }
     *out = &d;
@@ -98,6 +105,42 @@ int device_stream(cudaStream_t* out) {
     int rc = dev_state(&d);
     if (rc) return rc;
     *out = d->streams[d->next++ % POOL_STREAMS];
+    return IMOPS_OK;
+}
+
+// Pipeline runs on one device execute their kernels in the order they were
+// queued: a run first makes its image's stream wait for the end of the run
+// queued before it (on whatever stream), and marks its own end.  Images keep
+// their own streams, so one frame's download still overlaps the next frame's
+// kernels, but the kernels of frames submitted back to back do not share the
+// SMs: each frame finishes one frame-time after the one before it instead of
+// all finishing late together, which would leave the copy engines idle and
+// then bunch their downloads.  Holds its own lock (g_order_mu, not the
+// device lock the image buffers take) while the run is queued.
+std::mutex g_order_mu;
+struct ComputeOrder {
+    std::unique_lock<std::mutex> lock;
+    DevState* d = nullptr;
+    cudaStream_t s = nullptr;
+    ~ComputeOrder() {
+        if (d) {
+            cudaEventRecord(d->compute_done, s);
+            d->has_compute = true;
+        }
+    }
+};
+
+int order_compute(cudaStream_t s, ComputeOrder* o) {
+    o->lock = std::unique_lock<std::mutex>(g_order_mu);
+    DevState* d = nullptr;
+    {
+        std::lock_guard<std::mutex> dl(g_dev_mu);
+        int rc = dev_state(&d);
+        if (rc) return rc;
+    }
+    if (d->has_compute) IMOPS_CUDA_TRY(cudaStreamWaitEvent(s, d->compute_done, 0), "cudaStreamWaitEvent(compute order)");
+    o->d = d;
+    o->s = s;
     return IMOPS_OK;
 }
 
@@ -864,6 +907,8 @@ extern "C" ImopsImage* run_pixel_pipeline_c(ImopsImage* image, ImopsPipeline* pi
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev != image->dev) cudaSetDevice(image->dev);
+    pipe::ComputeOrder order;
+    if (pipe::order_compute(image->stream, &order)) return nullptr;
     auto& mods = pipeline->modules;
     for (size_t k = 0; k < mods.size(); k++) {
         if (dynamic_cast<pipe::PixelModule*>(mods[k].get())) {
