@@ -15,19 +15,17 @@
 //      the smallest count; the most homogeneous directions are averaged.
 // Pixels within 10 of an edge take the reference's 3x3 mean.
 //
-// One thread per pixel in six stencil kernels over planar per-direction
-// buffers in HBM (4 directions x G, R, B, Lab, difference); the stencils
-// re-read their neighbours from L1/L2.  Built with --fmad=false: the same
-// IEEE f32 operations in the same order as the oracle, including its cube
-// root (t r^2 with r = t^(-1/3) by a division-free Newton iteration).
+// One block per 32 x 32 tile of interior pixels runs every step in shared
+// memory (see `fused`); a second kernel fills the edge band.  Nothing is
+// allocated.  Built with --fmad=false: the same IEEE f32 operations in the
+// same order as the oracle, including its cube root (t r^2 with
+// r = t^(-1/3) by a division-free Newton iteration).
 #include "common.cuh"
 
 namespace imops {
 namespace xtrans {
 
 constexpr int BAND = 10;  // output band that takes the 3x3 mean
-__constant__ int DY[4] = {0, 1, 1, 1};
-__constant__ int DX[4] = {1, 0, 1, -1};
 
 struct Img {
     const float* m;
@@ -38,137 +36,10 @@ struct Img {
     __device__ __forceinline__ int col(int r, int c) const { return cfa.at(ci(r, H), ci(c, W)); }
 };
 
-// min / max / sum / count of the orthogonal green neighbours
-__device__ __forceinline__ void gbounds(const Img& im, int r, int c, float& lo, float& hi, float& sum, int& n) {
-    const int oy[4] = {0, 0, 1, -1}, ox[4] = {1, -1, 0, 0};
-    n = 0;
-    sum = lo = hi = 0.0f;
-#pragma unroll
-    for (int t = 0; t < 4; t++) {
-        if (im.col(r + oy[t], c + ox[t]) != 1) continue;
-        const float v = im.m[im.at(r + oy[t], c + ox[t])];
-        if (n == 0) {
-            lo = v;
-            hi = v;
-        } else {
-            lo = v < lo ? v : lo;
-            hi = v > hi ? v : hi;
-        }
-        sum = sum + v;
-        n++;
-    }
-}
-
 __device__ __forceinline__ float clampg(float g, float lo, float hi, int n) {
     if (n == 0) return g;
     g = g < lo ? lo : g;
     return g > hi ? hi : g;
-}
-
-__global__ void green1_kernel(const __grid_constant__ Img im, float* __restrict__ G) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= im.W || r >= im.H) return;
-    const size_t n = (size_t)im.W * im.H, i = (size_t)r * im.W + c;
-    if (im.col(r, c) == 1) {
-        for (int d = 0; d < 4; d++) G[d * n + i] = im.m[i];
-        return;
-    }
-    float lo, hi, sum;
-    int cnt;
-    gbounds(im, r, c, lo, hi, sum, cnt);
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-        // nearest green at distance 1 or 2 on each side, both candidates read
-        // (clamped, so in bounds) and chosen by selects, no divergent loop
-        const int dy = DY[d], dx = DX[d];
-        const bool p1 = im.col(r + dy, c + dx) == 1, p2 = im.col(r + 2 * dy, c + 2 * dx) == 1;
-        const bool m1 = im.col(r - dy, c - dx) == 1, m2 = im.col(r - 2 * dy, c - 2 * dx) == 1;
-        const float vp1 = im.m[im.at(r + dy, c + dx)], vp2 = im.m[im.at(r + 2 * dy, c + 2 * dx)];
-        const float vm1 = im.m[im.at(r - dy, c - dx)], vm2 = im.m[im.at(r - 2 * dy, c - 2 * dx)];
-        const int kp = p1 ? 1 : (p2 ? 2 : 0), km = m1 ? 1 : (m2 ? 2 : 0);
-        const float a = p1 ? vp1 : (p2 ? vp2 : 0.0f), b = m1 ? vm1 : (m2 ? vm2 : 0.0f);
-        float g;
-        if (kp && km) g = (a * (float)km + b * (float)kp) / (float)(kp + km);
-        else if (kp) g = a;
-        else if (km) g = b;
-        else g = cnt ? sum / (float)cnt : im.m[i];
-        G[d * n + i] = clampg(g, lo, hi, cnt);
-    }
-}
-
-__global__ void rb_kernel(const __grid_constant__ Img im, const float* __restrict__ G, float* __restrict__ R, float* __restrict__ B) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= im.W || r >= im.H) return;
-    const size_t n = (size_t)im.W * im.H, i = (size_t)r * im.W + c;
-    const int own = im.col(r, c);
-    // window rows / columns (clamped), the red and blue sites as bit masks
-    // and the mosaic values, all in registers
-    size_t ro[3];
-    int co[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        ro[a] = (size_t)im.ci(r + a - 1, im.H) * im.W;
-        co[a] = im.ci(c + a - 1, im.W);
-    }
-    unsigned mr = 0u, mb = 0u;
-    float mv[9];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-            const int cl = im.col(r + a - 1, c + b - 1);
-            mr |= (cl == 0 ? 1u : 0u) << (a * 3 + b);
-            mb |= (cl == 2 ? 1u : 0u) << (a * 3 + b);
-            mv[a * 3 + b] = im.m[ro[a] + co[b]];
-        }
-    int nr = 0, nb = 0;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        nr += (mr >> k) & 1u;
-        nb += (mb >> k) & 1u;
-    }
-    // every direction reads all nine G values (no divergent loads); the red
-    // and blue sums take their sites in row-major order (predicated adds)
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-        const float* Gd = G + d * n;
-        float sr = 0.0f, sb = 0.0f;
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-#pragma unroll
-            for (int b = 0; b < 3; b++) {
-                const int k = a * 3 + b;
-                const float e = mv[k] - Gd[ro[a] + co[b]];
-                sr = ((mr >> k) & 1u) ? sr + e : sr;
-                sb = ((mb >> k) & 1u) ? sb + e : sb;
-            }
-        const float g = Gd[i];
-        R[d * n + i] = own == 0 ? im.m[i] : (nr ? g + sr / (float)nr : g);
-        B[d * n + i] = own == 2 ? im.m[i] : (nb ? g + sb / (float)nb : g);
-    }
-}
-
-__global__ void refine_kernel(const __grid_constant__ Img im, const float* __restrict__ G, const float* __restrict__ R,
-                              const float* __restrict__ B, float* __restrict__ G2) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= im.W || r >= im.H) return;
-    const size_t n = (size_t)im.W * im.H, i = (size_t)r * im.W + c;
-    const int ch = im.col(r, c);
-    if (ch == 1) {
-        for (int d = 0; d < 4; d++) G2[d * n + i] = im.m[i];
-        return;
-    }
-    float lo, hi, sum;
-    int cnt;
-    gbounds(im, r, c, lo, hi, sum, cnt);
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-        const float* C = (ch == 0 ? R : B) + d * n;
-        const float* Gd = G + d * n;
-        const size_t jp = im.at(r + DY[d], c + DX[d]), jm = im.at(r - DY[d], c - DX[d]);
-        const float k = ((C[jp] - Gd[jp]) + (C[jm] - Gd[jm])) * 0.5f;
-        G2[d * n + i] = clampg(im.m[i] - k, lo, hi, cnt);
-    }
 }
 
 // cube root of t > 0 as t r^2, r = t^(-1/3) by Newton's method for the
@@ -197,40 +68,6 @@ __device__ __forceinline__ float lab_f(float t) {
     return 7.787037037037037f * t + 0.13793103448275862f;
 }
 
-__global__ void lab_kernel(const float* __restrict__ R, const float* __restrict__ G, const float* __restrict__ B,
-                           size_t n, float* __restrict__ L) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        for (int d = 0; d < 4; d++) {
-            const float r = R[d * n + i], g = G[d * n + i], b = B[d * n + i];
-            // linear sRGB -> XYZ (CSS Color 4) over the D65 white, folded into
-            // the X and Z rows
-            const float x = 0.4338873455660398f * r + 0.3762240091374988f * g + 0.18988864529646143f * b;
-            const float y = 0.21263900587151027f * r + 0.715168678767756f * g + 0.07219231536073371f * b;
-            const float z = 0.017750040070973232f * r + 0.10944762085523847f * g + 0.8728023390737883f * b;
-            const float fx = lab_f(x), fy = lab_f(y), fz = lab_f(z);
-            L[(d * 3 + 0) * n + i] = 116.0f * fy - 16.0f;
-            L[(d * 3 + 1) * n + i] = 500.0f * (fx - fy);
-            L[(d * 3 + 2) * n + i] = 200.0f * (fy - fz);
-        }
-}
-
-__global__ void diff_kernel(const __grid_constant__ Img im, const float* __restrict__ L, float* __restrict__ D) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= im.W || r >= im.H) return;
-    const size_t n = (size_t)im.W * im.H, i = (size_t)r * im.W + c;
-    for (int d = 0; d < 4; d++) {
-        const size_t jp = im.at(r + DY[d], c + DX[d]), jm = im.at(r - DY[d], c - DX[d]);
-        float sp = 0.0f, sm = 0.0f;
-        for (int k = 0; k < 3; k++) {
-            const float* Lk = L + (d * 3 + k) * n;
-            const float ep = Lk[i] - Lk[jp], em = Lk[i] - Lk[jm];
-            sp = sp + ep * ep;
-            sm = sm + em * em;
-        }
-        D[d * n + i] = sp + sm;
-    }
-}
-
 // the reference's 3x3 same-colour mean (demosaic.rs:108-186), as
 // demosaic_simple.cu computes it
 __device__ void mean3(const Img& im, int r, int c, float* o) {
@@ -256,59 +93,302 @@ __device__ void mean3(const Img& im, int r, int c, float* o) {
     }
 }
 
-__global__ void vote_kernel(const __grid_constant__ Img im, const float* __restrict__ R, const float* __restrict__ G,
-                            const float* __restrict__ B, const float* __restrict__ D, float* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= im.W || r >= im.H) return;
-    const size_t n = (size_t)im.W * im.H, i = (size_t)r * im.W + c;
-    float* o = out + 3 * i;
-    if (r < BAND || r >= im.H - BAND || c < BAND || c >= im.W - BAND) {
+// ---- fused tiles ---------------------------------------------------------
+// An interior output (at least BAND from every edge) depends on inputs within
+// radius 9 only, all inside the image, so a block takes a 32 x 32 tile of
+// interior outputs and runs the whole method for it in shared memory on a
+// 50 x 50 frame (the tile and a halo of 9): per direction the green
+// estimate on the frame less 2, red / blue on radius 6, refinement on 5, red /
+// blue on 4, refinement on 3, red / blue and Lab on 2, the difference on 1,
+// each stage over the cells the next one reads.  The directions run one
+// after another through the same buffers; each thread keeps its four
+// outputs' red, green and blue of every direction in registers for the vote,
+// and the four difference planes stay in shared memory.  Every cell is the
+// same f32 arithmetic, in the same order, as the staged specification.
+namespace fused {
+
+constexpr int T = 32;              // outputs a tile side
+constexpr int S = T + 18;          // frame side (radius 9 each way)
+constexpr int N = S * S;
+constexpr int DS = T + 2;          // difference planes: radius 1
+constexpr int THREADS = 512;
+constexpr int OUT = T * T / THREADS;  // outputs a thread
+__constant__ int OFF[4] = {1, S, S + 1, S - 1};  // frame step of each direction
+
+// Colour facts of a site, by its phase in the 6x6 period (a cell of the
+// frame whose neighbourhood lies inside the image, which every cell an
+// interior output depends on does):
+//   bits 0-1    its colour
+//   bits 2-10   red sites of its 3x3 window, row-major (bit 2 + 3(a+1) + b+1)
+//   bits 11-19  blue sites of the window
+//   bits 20-23  green orthogonal neighbours (0,+1) (0,-1) (+1,0) (-1,0)
+//   bits 24+4d  direction d: green at +1, +2, -1, -2 steps
+struct Masks {
+    unsigned long long m[36];
+};
+constexpr int MB_R = 2, MB_B = 11, MB_GO = 20, MB_DIR = 24;
+
+// shared memory: mosaic, two green buffers, red, blue, two Lab planes (the
+// third takes the free green buffer), four difference planes, the phase
+// table and each frame cell's phase: 91 KB, two blocks an SM
+constexpr size_t SMEM = (size_t)(7 * N + 4 * DS * DS) * sizeof(float) + 36 * 8 + N;
+static_assert((7 * N + 4 * DS * DS) % 2 == 0, "the mask table is 8-byte aligned");
+
+// host: the colour facts of the 36 phases of a 6x6 CFA
+inline Masks build_masks(const CfaDev& c) {
+    Masks M;
+    const int dy[4] = {0, 1, 1, 1}, dx[4] = {1, 0, 1, -1};
+    for (int py = 0; py < 6; py++)
+        for (int px = 0; px < 6; px++) {
+            auto col = [&](int y, int x) { return c.at(py + y, px + x); };
+            unsigned long long v = (unsigned long long)col(0, 0);
+            for (int a = -1; a <= 1; a++)
+                for (int b = -1; b <= 1; b++) {
+                    const int k = (a + 1) * 3 + (b + 1);
+                    if (col(a, b) == 0) v |= 1ull << (MB_R + k);
+                    if (col(a, b) == 2) v |= 1ull << (MB_B + k);
+                }
+            const int oy[4] = {0, 0, 1, -1}, ox[4] = {1, -1, 0, 0};
+            for (int t = 0; t < 4; t++)
+                if (col(oy[t], ox[t]) == 1) v |= 1ull << (MB_GO + t);
+            for (int d = 0; d < 4; d++) {
+                const int st[4] = {1, 2, -1, -2};
+                for (int q = 0; q < 4; q++)
+                    if (col(st[q] * dy[d], st[q] * dx[d]) == 1) v |= 1ull << (MB_DIR + 4 * d + q);
+            }
+            M.m[py * 6 + px] = v;
+        }
+    return M;
+}
+
+struct Frame {
+    float *m, *ga, *gb, *r, *b, *l1, *l2, *d;
+    const uint8_t* ph;                 // phase of each frame cell
+    const unsigned long long* masks;   // Masks, in shared memory
+};
+
+// min / max / sum / count of the green orthogonal neighbours, branch-free in
+// the neighbour order of the specification
+__device__ __forceinline__ void gbounds_f(const Frame& F, int f, unsigned long long M, float& lo, float& hi, float& sum,
+                                          int& n) {
+    const int nb[4] = {f + 1, f - 1, f + S, f - S};
+    n = 0;
+    sum = lo = hi = 0.0f;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        const bool ok = (M >> (MB_GO + t)) & 1ull;
+        const float v = F.m[nb[t]];
+        const bool first = ok && n == 0;
+        lo = first ? v : (ok ? (v < lo ? v : lo) : lo);
+        hi = first ? v : (ok ? (v > hi ? v : hi) : hi);
+        sum = ok ? sum + v : sum;
+        n += ok ? 1 : 0;
+    }
+}
+
+__device__ __forceinline__ float green1_f(const Frame& F, int f, int d, int off) {
+    const unsigned long long M = F.masks[F.ph[f]];
+    float lo, hi, sum;
+    int cnt;
+    gbounds_f(F, f, M, lo, hi, sum, cnt);
+    const unsigned dm = (unsigned)(M >> (MB_DIR + 4 * d)) & 15u;
+    const bool p1 = dm & 1u, p2 = dm & 2u, m1 = dm & 4u, m2 = dm & 8u;
+    const int kp = p1 ? 1 : (p2 ? 2 : 0), km = m1 ? 1 : (m2 ? 2 : 0);
+    const float vp1 = F.m[f + off], vp2 = F.m[f + 2 * off], vm1 = F.m[f - off], vm2 = F.m[f - 2 * off];
+    const float a = p1 ? vp1 : (p2 ? vp2 : 0.0f), b = m1 ? vm1 : (m2 ? vm2 : 0.0f);
+    const float both = (a * (float)km + b * (float)kp) / (float)(kp + km > 0 ? kp + km : 1);
+    const float mean = sum / (float)(cnt > 0 ? cnt : 1);
+    const float g = (kp && km) ? both : (kp ? a : (km ? b : (cnt ? mean : F.m[f])));
+    return (M & 3ull) == 1ull ? F.m[f] : clampg(g, lo, hi, cnt);
+}
+
+// red and blue at f from the green plane G: their sums over the window's
+// red / blue sites in row-major order
+__device__ __forceinline__ void rb_f(const Frame& F, const float* G, int f, float& R, float& B) {
+    const unsigned long long M = F.masks[F.ph[f]];
+    const unsigned mr = (unsigned)(M >> MB_R) & 511u, mb = (unsigned)(M >> MB_B) & 511u;
+    float sr = 0.0f, sbl = 0.0f;
+#pragma unroll
+    for (int a = -1; a <= 1; a++)
+#pragma unroll
+        for (int b = -1; b <= 1; b++) {
+            const int k = (a + 1) * 3 + (b + 1), j = f + a * S + b;
+            const float e = F.m[j] - G[j];
+            sr = ((mr >> k) & 1u) ? sr + e : sr;
+            sbl = ((mb >> k) & 1u) ? sbl + e : sbl;
+        }
+    const int nr = __popc(mr), nb = __popc(mb);
+    const int own = (int)(M & 3ull);
+    const float g = G[f];
+    const float qr = sr / (float)(nr > 0 ? nr : 1), qb = sbl / (float)(nb > 0 ? nb : 1);
+    R = own == 0 ? F.m[f] : (nr ? g + qr : g);
+    B = own == 2 ? F.m[f] : (nb ? g + qb : g);
+}
+
+__device__ __forceinline__ float refine_f(const Frame& F, const float* G, int f, int off) {
+    const unsigned long long M = F.masks[F.ph[f]];
+    const int ch = (int)(M & 3ull);
+    const float* C = ch == 0 ? F.r : F.b;
+    const float k = ((C[f + off] - G[f + off]) + (C[f - off] - G[f - off])) * 0.5f;
+    float lo, hi, sum;
+    int cnt;
+    gbounds_f(F, f, M, lo, hi, sum, cnt);
+    return ch == 1 ? F.m[f] : clampg(F.m[f] - k, lo, hi, cnt);
+}
+
+// the cells [LO, S - LO)^2 of the frame, spread over the block
+template <int LO, class Fn>
+__device__ __forceinline__ void over(Fn fn) {
+    constexpr int W = S - 2 * LO;
+    for (int k = threadIdx.x; k < W * W; k += THREADS) fn((LO + k / W) * S + LO + k % W);
+}
+
+__global__ void __launch_bounds__(THREADS, 2) tile_kernel(const __grid_constant__ Img im, const __grid_constant__ Masks mk,
+                                                         float* __restrict__ out) {
+    extern __shared__ __align__(16) float fsm[];
+    Frame F;
+    F.m = fsm;
+    F.ga = fsm + N;
+    F.gb = fsm + 2 * N;
+    F.r = fsm + 3 * N;
+    F.b = fsm + 4 * N;
+    F.l1 = fsm + 5 * N;
+    F.l2 = fsm + 6 * N;
+    F.d = fsm + 7 * N;
+    unsigned long long* msk = reinterpret_cast<unsigned long long*>(fsm + 7 * N + 4 * DS * DS);
+    uint8_t* phw = reinterpret_cast<uint8_t*>(msk + 36);
+    F.masks = msk;
+    F.ph = phw;
+    const int oy = BAND + blockIdx.y * T, ox = BAND + blockIdx.x * T;  // first output of the tile
+    if (threadIdx.x < 36) msk[threadIdx.x] = mk.m[threadIdx.x];
+    // frame: image rows oy-9 .. oy+T+8 (clamped at the far edges of a partial
+    // tile, whose cells there feed only outputs outside the interior); the
+    // phase of each cell in the period (periodic, unclamped)
+    const int py0 = (oy - 9) % 6, px0 = (ox - 9) % 6;
+    for (int k = threadIdx.x; k < N; k += THREADS) {
+        const int fy = k / S, fx = k % S;
+        const int y = im.ci(oy - 9 + fy, im.H), x = im.ci(ox - 9 + fx, im.W);
+        F.m[k] = im.m[(size_t)y * im.W + x];
+        phw[k] = (uint8_t)(((py0 + fy) % 6) * 6 + (px0 + fx) % 6);
+    }
+    float keep[4][3][OUT];
+    __syncthreads();
+#pragma unroll 1
+    for (int d = 0; d < 4; d++) {
+        const int off = OFF[d];
+        over<2>([&](int f) { F.ga[f] = green1_f(F, f, d, off); });
+        __syncthreads();
+        over<3>([&](int f) { rb_f(F, F.ga, f, F.r[f], F.b[f]); });
+        __syncthreads();
+        over<4>([&](int f) { F.gb[f] = refine_f(F, F.ga, f, off); });
+        __syncthreads();
+        over<5>([&](int f) { rb_f(F, F.gb, f, F.r[f], F.b[f]); });
+        __syncthreads();
+        over<6>([&](int f) { F.ga[f] = refine_f(F, F.gb, f, off); });
+        __syncthreads();
+        over<7>([&](int f) { rb_f(F, F.ga, f, F.r[f], F.b[f]); });
+        __syncthreads();
+        // Lab of this direction's RGB: L into the free green buffer
+        over<7>([&](int f) {
+            const float r = F.r[f], g = F.ga[f], b = F.b[f];
+            const float x = 0.4338873455660398f * r + 0.3762240091374988f * g + 0.18988864529646143f * b;
+            const float y = 0.21263900587151027f * r + 0.715168678767756f * g + 0.07219231536073371f * b;
+            const float z = 0.017750040070973232f * r + 0.10944762085523847f * g + 0.8728023390737883f * b;
+            const float fx = lab_f(x), fy = lab_f(y), fz = lab_f(z);
+            F.gb[f] = 116.0f * fy - 16.0f;
+            F.l1[f] = 500.0f * (fx - fy);
+            F.l2[f] = 200.0f * (fy - fz);
+        });
+        __syncthreads();
+        float* Dd = F.d + d * DS * DS;
+        over<8>([&](int f) {
+            const float* L[3] = {F.gb, F.l1, F.l2};
+            float sp = 0.0f, sm = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float ep = L[k][f] - L[k][f + off], em = L[k][f] - L[k][f - off];
+                sp = sp + ep * ep;
+                sm = sm + em * em;
+            }
+            Dd[(f / S - 8) * DS + (f % S - 8)] = sp + sm;
+        });
+#pragma unroll
+        for (int q = 0; q < OUT; q++) {
+            const int o = threadIdx.x + q * THREADS, f = (o / T + 9) * S + o % T + 9;
+            keep[d][0][q] = F.r[f];
+            keep[d][1][q] = F.ga[f];
+            keep[d][2][q] = F.b[f];
+        }
+        __syncthreads();
+    }
+    // vote over the 3x3 window of the four difference planes
+#pragma unroll
+    for (int q = 0; q < OUT; q++) {
+        const int o = threadIdx.x + q * THREADS, ty = o / T, tx = o % T;
+        const int y = oy + ty, x = ox + tx;
+        if (y >= im.H - BAND || x >= im.W - BAND) continue;
+        int hm[4] = {0, 0, 0, 0};
+        for (int a = -1; a <= 1; a++)
+            for (int b = -1; b <= 1; b++) {
+                const int j = (ty + 1 + a) * DS + (tx + 1 + b);
+                float mn = F.d[j];
+                for (int d = 1; d < 4; d++) mn = F.d[d * DS * DS + j] < mn ? F.d[d * DS * DS + j] : mn;
+                const float t = 8.0f * mn;
+#pragma unroll
+                for (int d = 0; d < 4; d++) hm[d] += F.d[d * DS * DS + j] <= t;
+            }
+        int hx = hm[0];
+#pragma unroll
+        for (int d = 1; d < 4; d++) hx = hm[d] > hx ? hm[d] : hx;
+        const int thr = hx - hx / 8;
+        int cnt = 0;
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            if (hm[d] < thr) continue;
+            s0 = s0 + keep[d][0][q];
+            s1 = s1 + keep[d][1][q];
+            s2 = s2 + keep[d][2][q];
+            cnt++;
+        }
+        const int fc = (ty + 9) * S + tx + 9;
+        const int own = (int)(F.masks[F.ph[fc]] & 3ull);
+        float* po = out + 3 * ((size_t)y * im.W + x);
+        po[0] = own == 0 ? F.m[fc] : s0 / (float)cnt;
+        po[1] = own == 1 ? F.m[fc] : s1 / (float)cnt;
+        po[2] = own == 2 ? F.m[fc] : s2 / (float)cnt;
+    }
+}
+
+// the edge band (within BAND of an edge): the reference's 3x3 mean.  Band
+// pixels are indexed flat: whole rows at the top and bottom, then BAND
+// columns either side of each middle row.
+__global__ void band_kernel(const __grid_constant__ Img im, float* __restrict__ out, int top, int bottom, int left,
+                            int right, size_t total) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
+        int r, c;
+        const size_t rows = (size_t)(top + bottom) * im.W;
+        if (k < rows) {
+            const int rr = (int)(k / im.W);
+            r = rr < top ? rr : im.H - bottom + (rr - top);
+            c = (int)(k % im.W);
+        } else {
+            const size_t q = k - rows;
+            const int per = left + right;
+            r = top + (int)(q / per);
+            const int cc = (int)(q % per);
+            c = cc < left ? cc : im.W - right + (cc - left);
+        }
         float v[3];
         mean3(im, r, c, v);
-        o[0] = v[0];
-        o[1] = v[1];
-        o[2] = v[2];
-        return;
+        float* po = out + 3 * ((size_t)r * im.W + c);
+        po[0] = v[0];
+        po[1] = v[1];
+        po[2] = v[2];
     }
-    int hm[4] = {0, 0, 0, 0};
-    for (int a = -1; a <= 1; a++)
-        for (int b = -1; b <= 1; b++) {
-            const size_t j = (size_t)(r + a) * im.W + (c + b);
-            float mn = D[j];
-            for (int d = 1; d < 4; d++) mn = D[d * n + j] < mn ? D[d * n + j] : mn;
-            const float t = 8.0f * mn;
-#pragma unroll
-            for (int d = 0; d < 4; d++) hm[d] += D[d * n + j] <= t;
-        }
-    int hx = hm[0];
-#pragma unroll
-    for (int d = 1; d < 4; d++) hx = hm[d] > hx ? hm[d] : hx;
-    const int thr = hx - hx / 8;
-    int cnt = 0;
-    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-        if (hm[d] < thr) continue;
-        s0 = s0 + R[d * n + i];
-        s1 = s1 + G[d * n + i];
-        s2 = s2 + B[d * n + i];
-        cnt++;
-    }
-    const int own = im.cfa.at(r, c);  // the site's own colour keeps its sample
-    o[0] = own == 0 ? im.m[i] : s0 / (float)cnt;
-    o[1] = own == 1 ? im.m[i] : s1 / (float)cnt;
-    o[2] = own == 2 ? im.m[i] : s2 / (float)cnt;
 }
 
-// per (device, stream) working planes, grown on demand
-StreamCache g_ws("X-Trans planes");
-
-int workspace(cudaStream_t s, size_t bytes, float** out) {
-    void* p = nullptr;
-    int rc = g_ws.get(s, bytes, &p);
-    *out = static_cast<float*>(p);
-    return rc;
-}
+}  // namespace fused
 
 }  // namespace xtrans
 }  // namespace imops
@@ -325,34 +405,28 @@ extern "C" int imops_demosaic_markesteijn3(const float* mosaic, int w, int h, co
     if (rc) return rc;
     if (c.pw != 6 || c.ph != 6) return fail(IMOPS_ERR_UNSUPPORTED_CFA, "markesteijn3 needs a 6x6 (X-Trans) CFA");
     cudaStream_t s = as_stream(stream);
-    const size_t n = (size_t)w * h;
-    float* ws = nullptr;
-    if ((rc = xtrans::workspace(s, n * 32 * sizeof(float), &ws))) return rc;
     if (fault_injected("launch")) return fail(IMOPS_ERR_CUDA, "injected launch failure (markesteijn3)");
-    float *G = ws, *G2 = ws + 4 * n, *R = ws + 8 * n, *B = ws + 12 * n, *L = ws + 16 * n, *D = ws + 28 * n;
     const xtrans::Img im{mosaic, w, h, CfaFixed<6, 6>::from(c)};
-    const dim3 blk(32, 8), grd((w + 31) / 32, (h + 7) / 8);
-    xtrans::green1_kernel<<<grd, blk, 0, s>>>(im, G);
-    note_launch();
-    for (int pass = 0; pass < 3; pass++) {
-        if (pass > 0) {
-            xtrans::refine_kernel<<<grd, blk, 0, s>>>(im, G, R, B, G2);
-            note_launch();
-            float* t = G;
-            G = G2;
-            G2 = t;
-        }
-        xtrans::rb_kernel<<<grd, blk, 0, s>>>(im, G, R, B);
+    using xtrans::BAND;
+    // interior tiles, then the band (every pixel within BAND of an edge)
+    const int iw = w - 2 * BAND, ih = h - 2 * BAND;
+    if (iw > 0 && ih > 0) {
+        namespace F = xtrans::fused;
+        const dim3 grd((iw + F::T - 1) / F::T, (ih + F::T - 1) / F::T);
+        IMOPS_CUDA_TRY(cudaFuncSetAttribute(F::tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F::SMEM),
+                       "cudaFuncSetAttribute(markesteijn3)");
+        F::tile_kernel<<<grd, F::THREADS, F::SMEM, s>>>(im, F::build_masks(c), rgb);
         note_launch();
     }
-    int g1 = (int)((n + 255) / 256);
-    const int cap = sm_count() * 8;
-    xtrans::lab_kernel<<<g1 < cap ? g1 : cap, 256, 0, s>>>(R, G, B, n, L);
-    note_launch();
-    xtrans::diff_kernel<<<grd, blk, 0, s>>>(im, L, D);
-    note_launch();
-    xtrans::vote_kernel<<<grd, blk, 0, s>>>(im, R, G, B, D, rgb);
-    note_launch();
+    const int top = h < BAND ? h : BAND, bottom = h - top < BAND ? h - top : BAND;
+    const int mid = h - top - bottom;
+    const int left = w < BAND ? w : BAND, right = w - left < BAND ? w - left : BAND;
+    const size_t total = (size_t)(top + bottom) * w + (size_t)mid * (left + right);
+    if (total) {
+        size_t g = (total + 255) / 256, cap = (size_t)sm_count() * 8;
+        xtrans::fused::band_kernel<<<(int)(g < cap ? g : cap), 256, 0, s>>>(im, rgb, top, bottom, left, right, total);
+        note_launch();
+    }
     IMOPS_CUDA_TRY(cudaGetLastError(), "markesteijn3 launch");
     return IMOPS_OK;
 }

@@ -70,7 +70,7 @@ const char *imops_last_error(void);
 const char *imops_version(void);
 
 /* Frees the working sets the stage entry points cache per (device, stream)
- * on the current device (film, adjoint, X-Trans planes, the fused develop's
+ * on the current device (film, adjoint, the fused develop's
  * mosaic buffer), after waiting for the device; the next call allocates
  * again.  No counterpart in the reference (its buffers are Rust Vecs freed
  * with each module).  Call it when no work of this library is in flight on
@@ -111,7 +111,7 @@ int imops_demosaic_markesteijn(const float *mosaic, int w, int h, const char *cf
  * from colour differences, two green refinement passes, and a CIELab
  * homogeneity vote between the directions; pixels within 10 of an edge take
  * the 3x3 mean.  6x6 CFAs only (IMOPS_ERR_UNSUPPORTED_CFA otherwise).
- * Keeps a per-(device, stream) working set of 128 bytes per pixel. */
+ * Allocates nothing: each 32x32 tile runs every step in shared memory. */
 int imops_demosaic_markesteijn3(const float *mosaic, int w, int h, const char *cfa, int shift_x, int shift_y,
                                 float *rgb, imops_stream_t stream);
 

@@ -78,8 +78,9 @@ def test_pipeline_c_abi_returns_null_and_last_error(gpu, monkeypatch):
 
 
 def test_injected_failures_in_xtrans_and_display(gpu, monkeypatch):
-    """The 3-pass X-Trans demosaic (working planes) and the display chain fail
-    with a status and recover the same way."""
+    """The 3-pass X-Trans demosaic and the display chain fail with a status
+    at their launch sites and recover the same way; the X-Trans demosaic
+    allocates nothing, so an allocation fault leaves it unaffected."""
     import torch
 
     import imops_b200 as im
@@ -87,10 +88,11 @@ def test_injected_failures_in_xtrans_and_display(gpu, monkeypatch):
     m = torch.from_numpy(synthetic.mosaic_f32(96, 120, seed=4, pattern=synthetic.XTRANS)).to(gpu)
     ref = im.demosaic_markesteijn3(m, synthetic.XTRANS)
     monkeypatch.setenv("IMOPS_FAULT_INJECT", "alloc")
+    assert torch.equal(im.demosaic_markesteijn3(m, synthetic.XTRANS), ref)
+    monkeypatch.setenv("IMOPS_FAULT_INJECT", "launch")
     with pytest.raises(im.ImopsError) as e:
         im.demosaic_markesteijn3(m, synthetic.XTRANS)
-    assert e.value.code == 5 and "injected allocation failure" in e.value.message
-    monkeypatch.setenv("IMOPS_FAULT_INJECT", "launch")
+    assert e.value.code == 4 and "injected launch failure" in e.value.message
     x = _rgb(gpu)
     with pytest.raises(im.ImopsError) as e:
         im.sigmoid_tone_map(x.clone())

@@ -16,7 +16,8 @@ def _gpu(gpu, x):
     return torch.from_numpy(np.ascontiguousarray(x)).to(gpu)
 
 
-@pytest.mark.parametrize("H,W", [(64, 72), (97, 131), (200, 257)])
+@pytest.mark.parametrize("H,W", [(64, 72), (97, 131), (200, 257), (20, 30), (21, 21), (22, 53), (53, 22), (75, 107),
+                                 (142, 84)])
 def test_matches_oracle_bit_exact(oracle_lib, gpu, H, W):
     import imops_b200 as im
     m = synthetic.mosaic_f32(H, W, seed=H + W, pattern=synthetic.XTRANS)
@@ -86,3 +87,14 @@ def test_rejects_bayer(gpu):
     with pytest.raises(im.ImopsError) as e:
         im.demosaic_markesteijn3(_gpu(gpu, m), "RGGB")
     assert e.value.code == 2
+
+
+def test_other_6x6_cfa_generic_tiles(oracle_lib, gpu):
+    """A 6x6 CFA that is not a shift of the X-Trans period (here a Bayer period
+    tiled to 6x6) takes the generic tile kernel: bit for bit the same method."""
+    import imops_b200 as im
+    pattern = "RGRGRGGBGBGB" * 3
+    m = synthetic.mosaic_f32(90, 118, seed=5, pattern=pattern)
+    ref = oracle_lib.markesteijn3(m, pattern, shift=(1, 2))
+    out = im.demosaic_markesteijn3(_gpu(gpu, m), pattern, shift=(1, 2)).cpu().numpy()
+    assert np.array_equal(out, ref)
