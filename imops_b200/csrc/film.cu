@@ -1521,6 +1521,45 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
 // The baseline preset's kernels with the working set at `scratch` (256-byte
 // aligned, baseline_scratch_bytes(W, H) long).  Every byte the kernels read
 // there is written earlier in the same call.
+// A second stream per device for work that does not depend on the image
+// (the grain fields), forked from and joined back to the caller's stream with
+// events: the grain (one 148 KB block an SM) then runs beside the exposure
+// and the halation row pass, which need the HBM but few SM resources.
+struct SideStream {
+    bool init = false;
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+std::mutex g_side_mu;
+SideStream g_side[64];
+
+// the current device's side stream, created on first use; call with g_side_mu held
+int side_stream(SideStream** out) {
+    int dev = 0;
+    IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return fail(IMOPS_ERR_INVALID_ARGUMENT, "film: device index above 63");
+    SideStream& d = g_side[dev];
+    if (!d.init) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t f = nullptr, j = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            if (st) cudaStreamDestroy(st);
+            if (f) cudaEventDestroy(f);
+            if (j) cudaEventDestroy(j);
+            return cuda_status(e, "film side stream");
+        }
+        d.side = st;
+        d.fork = f;
+        d.join = j;
+        d.init = true;
+    }
+    *out = &d;
+    return IMOPS_OK;
+}
+
 int baseline_forward_in(float* rgb, int W, int H, const ImopsBaselineFilm& P, const Stock& st, void* scratch,
                         cudaStream_t s) {
     int rc;
@@ -1535,13 +1574,27 @@ int baseline_forward_in(float* rgb, int W, int H, const ImopsBaselineFilm& P, co
     Base81 hp;
     build_base81(st, &hp);
     int g = grid_for(n);
-    expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
-    note_launch();
-    if ((rc = blur_rows(hal, hr, W, H, st.hal_taps, HAL_R, s))) return rc;
     if (P.grain_on && P.grain_sigma != 0.0f) {
+        // grain fields on the side stream while the exposure and the row pass
+        // run on s; the scan waits for both.  The lock keeps one call's
+        // record / wait pairs of the shared events together.
         Taps tp;
         if ((rc = taps_for(fmaxf(P.grain_blur, 1.0f), &tp))) return rc;
-        if ((rc = grain_fields(noise, W, H, P.seed, 0, 3, tp, gpart, sums, s))) return rc;
+        std::lock_guard<std::mutex> lock(g_side_mu);
+        SideStream* ss = nullptr;
+        if ((rc = side_stream(&ss))) return rc;
+        IMOPS_CUDA_TRY(cudaEventRecord(ss->fork, s), "cudaEventRecord(film fork)");
+        IMOPS_CUDA_TRY(cudaStreamWaitEvent(ss->side, ss->fork, 0), "cudaStreamWaitEvent(film fork)");
+        if ((rc = grain_fields(noise, W, H, P.seed, 0, 3, tp, gpart, sums, ss->side))) return rc;
+        IMOPS_CUDA_TRY(cudaEventRecord(ss->join, ss->side), "cudaEventRecord(film join)");
+        expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
+        note_launch();
+        if ((rc = blur_rows(hal, hr, W, H, st.hal_taps, HAL_R, s))) return rc;
+        IMOPS_CUDA_TRY(cudaStreamWaitEvent(s, ss->join, 0), "cudaStreamWaitEvent(film join)");
+    } else {
+        expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
+        note_launch();
+        if ((rc = blur_rows(hal, hr, W, H, st.hal_taps, HAL_R, s))) return rc;
     }
     dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + R64_COL_TH - 1) / R64_COL_TH);
     if (P.scan == IMOPS_SCAN_BF16_TC) {
