@@ -23,6 +23,19 @@ namespace film {
 
 constexpr int MAXR = 64;  // largest blur radius handled (129 taps)
 
+// The baseline preset's logistic density curve D = dmax / (1 + e^(-k (log10 E
+// - x0))) from the hardware base-2 logarithm and exponential (lg2 / ex2
+// .approx.ftz, about 2^-22 relative) and a fast reciprocal: log10 E =
+// log2 E * log10(2), e^x = 2^(x log2 e).  Within 1e-6 relative of the
+// library functions' result; the film's tolerance is 1e-4.
+__device__ __forceinline__ float curve_density(float E, float dmax, float k, float x0) {
+    float l2;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l2) : "f"(fmaxf(E, 1e-6f)));
+    const float le = l2 * 0.30102999566398120f;
+    const float t = ex2_fast(-k * (le - x0) * 1.4426950408889634f);
+    return __fdividef(dmax, 1.0f + t);
+}
+
 struct Taps {
     int R;
     float t[2 * MAXR + 1];
@@ -824,9 +837,8 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
         for (int u = 0; u < 2; u++)
 #pragma unroll
             for (int e = 0; e < 3; e++) {
-                float E = ca[u][e] + c.B.hal_strength * c.B.bleed[e] * bsum[u];
-                float le = log10f(fmaxf(E, 1e-6f));
-                D[u][e] = c.B.dmax[e] / (1.0f + expf(-c.B.k[e] * (le - c.B.x0[e])));
+                const float E = ca[u][e] + c.B.hal_strength * c.B.bleed[e] * bsum[u];
+                D[u][e] = curve_density(E, c.B.dmax[e], c.B.k[e], c.B.x0[e]);
                 if (grain) D[u][e] += c.B.grain_sigma * cz[u][e] * norm[e];
             }
         float2 d[2][3], o[2][3];
@@ -1093,9 +1105,8 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 2) scan81_tc_kern
             }
 #pragma unroll
             for (int e = 0; e < 3; e++) {
-                float E = la[e] + c.B.hal_strength * c.B.bleed[e] * bsum;
-                float le = log10f(fmaxf(E, 1e-6f));
-                D[e] = c.B.dmax[e] / (1.0f + expf(-c.B.k[e] * (le - c.B.x0[e])));
+                const float E = la[e] + c.B.hal_strength * c.B.bleed[e] * bsum;
+                D[e] = curve_density(E, c.B.dmax[e], c.B.k[e], c.B.x0[e]);
                 if (grain) D[e] += c.B.grain_sigma * lz[e] * norm[e];
             }
         }
