@@ -437,8 +437,15 @@ __global__ void dir_apply_kernel(float* __restrict__ planes, const float* __rest
 // equals blur(noise) bit for bit); the fields written, and each layer's block
 // sum of squares (f64) stored in partial[plane][block] for the variance.
 // Plane z holds RNG layer layer0 + z.  Radius <= GR_MAXR.
-constexpr int GR_TW = 128, GR_TH = 64, GR_MAXR = 16;
+//
+// Tiles are 128 x 32: the three layers' noise and one row-blurred layer take
+// 80 KB at radius 3, so two blocks (32 warps) share an SM.  Inside the image
+// a thread generates a run of GR_RUN consecutive pixels of a row, whose
+// layers share all but the last two draws of the next pixel
+// (grain_noise_run): 12 GR_RUN + 2 draws a run instead of 14 a pixel.
+constexpr int GR_TW = 128, GR_TH = 32, GR_MAXR = 16, GR_RUN = 4;
 constexpr int GR_THREADS = 512, GR_TY = GR_THREADS / 32;
+static_assert(GR_TW == 128, "the blur loops index tile columns with & 127");
 
 // Noise of pixel (y, x) in LAYERS consecutive layers layer0, layer0+1, ...
 // (grain.rs:20-45, 53-66).  Layer L of row y is the SplitMix64 stream seeded
@@ -471,62 +478,85 @@ __device__ __forceinline__ void grain_noise_at(uint64_t seed, int layer0, int y,
     for (int z = 0; z < LAYERS; z++) out[z] = acc[z] - 6.0f;
 }
 
+// The same for RUN consecutive pixels x .. x+RUN-1 of row y: pixel x+i takes
+// draws 12i+1 .. 12i+LAYERS+11 counted from pixel x's first, so the run
+// mixes its 12 RUN + LAYERS - 1 draws once each; every (pixel, layer) sum adds
+// its 12 draws in the order grain_noise_at does, so the values are identical.
+template <int LAYERS, int RUN>
+__device__ __forceinline__ void grain_noise_run(uint64_t seed, int layer0, int y, int x, float (&out)[RUN][LAYERS]) {
+    const uint64_t golden = 0x9E3779B97F4A7C15ull;
+    uint64_t z0 = seed * 0xD1B54A32D192ED03ull + (uint64_t)layer0 * golden + (uint64_t)y + 12 * (uint64_t)x * golden;
+    float acc[RUN][LAYERS];
+#pragma unroll
+    for (int i = 0; i < RUN; i++)
+#pragma unroll
+        for (int z = 0; z < LAYERS; z++) acc[i][z] = 0.0f;
+#pragma unroll
+    for (int k = 1; k <= 12 * RUN + LAYERS - 1; k++) {
+        z0 += golden;
+        uint64_t v = (z0 ^ (z0 >> 30)) * 0xBF58476D1CE4E5B9ull;
+        v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+        const float u = __ull2float_rn(v ^ (v >> 31)) / 18446744073709551616.0f;
+#pragma unroll
+        for (int i = 0; i < RUN; i++)
+#pragma unroll
+            for (int z = 0; z < LAYERS; z++)
+                if (k >= 12 * i + z + 1 && k <= 12 * i + z + 12) acc[i][z] += u;
+    }
+#pragma unroll
+    for (int i = 0; i < RUN; i++)
+#pragma unroll
+        for (int z = 0; z < LAYERS; z++) out[i][z] = acc[i][z] - 6.0f;
+}
+
 template <int LAYERS>
-__global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restrict__ noise, int W, int H, uint64_t seed,
-                                                          int layer0, Taps tp, double* __restrict__ partial) {
-    extern __shared__ float gsm[];
+__global__ void __launch_bounds__(GR_THREADS, 2) grain_field_kernel(float* __restrict__ noise, int W, int H,
+                                                                    uint64_t seed, int layer0, Taps tp,
+                                                                    double* __restrict__ partial) {
+    extern __shared__ __align__(16) float gsm[];
     __shared__ double red[GR_TY];
     const int R = tp.R;
     const int x0 = blockIdx.x * GR_TW, y0 = blockIdx.y * GR_TH;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    // noise rows are NW samples; stored with a stride of NWP (a multiple of
+    // the run, so runs and their float4 stores stay aligned)
     const int NW = GR_TW + 2 * R, NH = GR_TH + 2 * R;
-    const int GR_SW = NW;
-    float* sn = gsm;                     // noise, tile + halo: LAYERS x NH x NW
-    float* sr = gsm + LAYERS * NH * NW;  // row-blurred: NH x GR_TW (one layer at a time)
-    // flat over the tile + halo so every lane draws (the halo row is not a
-    // multiple of the warp width)
-    // (row, column) of idx stepped without a division: idx advances by
-    // GR_THREADS = dq rows + dr columns
-    const int dq = GR_THREADS / NW, dr = GR_THREADS - dq * NW;
-    int r = tid / NW, c = tid - (tid / NW) * NW;
+    const int NWP = (NW + GR_RUN - 1) / GR_RUN * GR_RUN;
+    float* sn = gsm;                      // noise, tile + halo: LAYERS x NH x NWP
+    float* sr = gsm + LAYERS * NH * NWP;  // row-blurred: NH x GR_TW (one layer at a time)
     // blocks whose tile + halo lies inside the image need no mirroring
     const bool inner = x0 - R >= 0 && y0 - R >= 0 && x0 + GR_TW + R <= W && y0 + GR_TH + R <= H;
-    float v[LAYERS];
     if (inner) {
-        // two samples a thread and iteration (idx and idx + GR_THREADS): two
-        // independent SplitMix64 chains in flight
-        int idx = tid;
-        for (; idx + GR_THREADS < NH * NW; idx += 2 * GR_THREADS) {
-            int r2 = r + dq, c2 = c + dr;
-            if (c2 >= NW) {
-                c2 -= NW;
-                r2++;
-            }
-            float v2[LAYERS];
-            grain_noise_at<LAYERS>(seed, layer0, y0 - R + r, x0 - R + c, v);
-            grain_noise_at<LAYERS>(seed, layer0, y0 - R + r2, x0 - R + c2, v2);
+        // runs of GR_RUN pixels over the rows (the last run of a row may
+        // reach past NW: those samples are generated and never read);
+        // (row, run) of j stepped without a division
+        const int RPR = NWP / GR_RUN, nruns = NH * RPR;
+        const int dq = GR_THREADS / RPR, dr = GR_THREADS - dq * RPR;
+        int r = tid / RPR, q = tid - (tid / RPR) * RPR;
+        for (int j = tid; j < nruns; j += GR_THREADS) {
+            float v[GR_RUN][LAYERS];
+            grain_noise_run<LAYERS, GR_RUN>(seed, layer0, y0 - R + r, x0 - R + q * GR_RUN, v);
 #pragma unroll
             for (int z = 0; z < LAYERS; z++) {
-                sn[z * NH * NW + idx] = v[z];
-                sn[z * NH * NW + idx + GR_THREADS] = v2[z];
+                static_assert(GR_RUN == 4, "one float4 store a run and layer");
+                *reinterpret_cast<float4*>(sn + (z * NH + r) * NWP + q * GR_RUN) =
+                    make_float4(v[0][z], v[1][z], v[2][z], v[3][z]);
             }
-            r = r2 + dq;
-            c = c2 + dr;
-            if (c >= NW) {
-                c -= NW;
+            r += dq;
+            q += dr;
+            if (q >= RPR) {
+                q -= RPR;
                 r++;
             }
         }
-        if (idx < NH * NW) {
-            grain_noise_at<LAYERS>(seed, layer0, y0 - R + r, x0 - R + c, v);
-#pragma unroll
-            for (int z = 0; z < LAYERS; z++) sn[z * NH * NW + idx] = v[z];
-        }
     } else {
+        const int dq = GR_THREADS / NW, dr = GR_THREADS - dq * NW;
+        int r = tid / NW, c = tid - (tid / NW) * NW;
         for (int idx = tid; idx < NH * NW; idx += GR_THREADS) {
+            float v[LAYERS];
             grain_noise_at<LAYERS>(seed, layer0, reflect(y0 - R + r, H), reflect(x0 - R + c, W), v);
 #pragma unroll
-            for (int z = 0; z < LAYERS; z++) sn[z * NH * NW + idx] = v[z];
+            for (int z = 0; z < LAYERS; z++) sn[(z * NH + r) * NWP + c] = v[z];
             r += dq;
             c += dr;
             if (c >= NW) {
@@ -537,38 +567,40 @@ __global__ void __launch_bounds__(GR_THREADS) grain_field_kernel(float* __restri
     }
     const size_t n = (size_t)W * H;
     for (int z = 0; z < LAYERS; z++) {
-        const float* snz = sn + z * NH * NW;
+        const float* snz = sn + z * NH * NWP;
         __syncthreads();  // the noise is complete; sr is free again
-        for (int r = ty; r < NH; r += GR_TY)
-            for (int c = tx; c < GR_TW; c += 32) {
-                float acc = 0.0f;
-                // radius 3 (a 1 px grain blur, every stock here) unrolled
-                if (R == 3) {
+        for (int idx = tid; idx < NH * GR_TW; idx += GR_THREADS) {
+            const int r = idx >> 7, c = idx & (GR_TW - 1);
+            const float* s = snz + r * NWP + c;
+            float acc = 0.0f;
+            // radius 3 (a 1 px grain blur, every stock here) unrolled
+            if (R == 3) {
 #pragma unroll
-                    for (int k = 0; k <= 6; k++) acc = fmaf(snz[r * GR_SW + c + k], tp.t[k], acc);
-                } else {
-                    for (int k = 0; k <= 2 * R; k++) acc = fmaf(snz[r * GR_SW + c + k], tp.t[k], acc);
-                }
-                sr[r * GR_TW + c] = acc;
+                for (int k = 0; k <= 6; k++) acc = fmaf(s[k], tp.t[k], acc);
+            } else {
+                for (int k = 0; k <= 2 * R; k++) acc = fmaf(s[k], tp.t[k], acc);
             }
+            sr[idx] = acc;
+        }
         __syncthreads();
         double sq = 0.0;
-        for (int r = ty; r < GR_TH; r += GR_TY)
-            for (int c = tx; c < GR_TW; c += 32) {
-                const int y = y0 + r, x = x0 + c;
-                if (y >= H || x >= W) continue;
-                float acc = 0.0f;
-                if (R == 3) {
+        for (int idx = tid; idx < GR_TH * GR_TW; idx += GR_THREADS) {
+            const int r = idx >> 7, c = idx & (GR_TW - 1);
+            const int y = y0 + r, x = x0 + c;
+            if (y >= H || x >= W) continue;
+            const float* s = sr + idx;
+            float acc = 0.0f;
+            if (R == 3) {
 #pragma unroll
-                    for (int k = 0; k <= 6; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
-                } else {
-                    for (int k = 0; k <= 2 * R; k++) acc = fmaf(sr[(r + k) * GR_TW + c], tp.t[k], acc);
-                }
-                noise[z * n + (size_t)y * W + x] = acc;
-                sq += (double)acc * (double)acc;
+                for (int k = 0; k <= 6; k++) acc = fmaf(s[k * GR_TW], tp.t[k], acc);
+            } else {
+                for (int k = 0; k <= 2 * R; k++) acc = fmaf(s[k * GR_TW], tp.t[k], acc);
             }
+            noise[z * n + (size_t)y * W + x] = acc;
+            sq += (double)acc * (double)acc;
+        }
         for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-        if (tx == 0) red[ty] = sq;
+        if (threadIdx.x == 0) red[threadIdx.y] = sq;
         __syncthreads();
         if (tid == 0) {
             double t = 0.0;
@@ -607,9 +639,10 @@ int grain_fields(float* noise, int W, int H, uint64_t seed, int layer0, int laye
     if (tp.R > GR_MAXR) return fail(IMOPS_ERR_UNSUPPORTED_SIZE, "film: grain blur radius above 16 px");
     dim3 b(32, GR_TY), g((W + GR_TW - 1) / GR_TW, (H + GR_TH - 1) / GR_TH);
     const int NW = GR_TW + 2 * tp.R, NH = GR_TH + 2 * tp.R;
+    const int NWP = (NW + GR_RUN - 1) / GR_RUN * GR_RUN;
     // three layers per block (their draws shared) while their noise fits in
     // shared memory; otherwise one block per (tile, layer)
-    const size_t smem3 = (size_t)NH * (3 * NW + GR_TW) * sizeof(float);
+    const size_t smem3 = (size_t)NH * (3 * NWP + GR_TW) * sizeof(float);
     const size_t n = (size_t)W * H, nb = (size_t)g.x * g.y;
     int z = 0;
     if (layers >= 3 && smem3 <= 200 * 1024) {
@@ -622,7 +655,7 @@ int grain_fields(float* noise, int W, int H, uint64_t seed, int layer0, int laye
         }
     }
     if (z < layers) {
-        const size_t smem1 = (size_t)NH * (NW + GR_TW) * sizeof(float);
+        const size_t smem1 = (size_t)NH * (NWP + GR_TW) * sizeof(float);
         IMOPS_CUDA_TRY(cudaFuncSetAttribute(grain_field_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem1),
                        "cudaFuncSetAttribute(grain)");
