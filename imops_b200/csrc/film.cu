@@ -70,16 +70,27 @@ __device__ __forceinline__ int reflect(int i, int n) {
 // ---------------------------------------------------------------------------
 // exposure
 
+// The basis weights of one pixel: w = max(0, Minv * rgb).
+__device__ __forceinline__ void basis_weights(const ExposeSpec& X, float r, float g, float b, float (&w)[3]) {
+    w[0] = fmaxf(0.0f, X.minv[0] * r + X.minv[1] * g + X.minv[2] * b);
+    w[1] = fmaxf(0.0f, X.minv[3] * r + X.minv[4] * g + X.minv[5] * b);
+    w[2] = fmaxf(0.0f, X.minv[6] * r + X.minv[7] * g + X.minv[8] * b);
+}
+
+// Layer e's absorbed band-mean fluence from the basis weights.
+__device__ __forceinline__ float layer_exposure(const ExposeSpec& X, const float (&w)[3], int e) {
+    return w[0] * X.A[0][e] + w[1] * X.A[1][e] + w[2] * X.A[2][e];
+}
+
 // rgb (interleaved) -> E planes of absorbed band-mean fluence, optional
 // halation source plane max(0, R - threshold).
 __global__ void expose_kernel(const float* __restrict__ rgb, size_t n, ExposeSpec X, float* __restrict__ planes,
                               float* __restrict__ hal) {
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
         float r = rgb[3 * p], g = rgb[3 * p + 1], b = rgb[3 * p + 2];
-        float w0 = fmaxf(0.0f, X.minv[0] * r + X.minv[1] * g + X.minv[2] * b);
-        float w1 = fmaxf(0.0f, X.minv[3] * r + X.minv[4] * g + X.minv[5] * b);
-        float w2 = fmaxf(0.0f, X.minv[6] * r + X.minv[7] * g + X.minv[8] * b);
-        for (int e = 0; e < X.E; e++) planes[e * n + p] = w0 * X.A[0][e] + w1 * X.A[1][e] + w2 * X.A[2][e];
+        float w[3];
+        basis_weights(X, r, g, b, w);
+        for (int e = 0; e < X.E; e++) planes[e * n + p] = layer_exposure(X, w, e);
         if (X.hal_src) hal[p] = fmaxf(0.0f, r - X.hal_threshold);
     }
 }
@@ -137,15 +148,26 @@ constexpr int R64_ROW_OUT = 4;                      // outputs per thread
 constexpr int R64_ROW_THREADS = 256;
 constexpr int R64_ROW_TILE = R64_ROW_OUT * R64_ROW_THREADS;  // 1024 outputs per block
 
-__global__ void __launch_bounds__(R64_ROW_THREADS) blur_rows_r64_kernel(const float* __restrict__ in,
-                                                                       float* __restrict__ out, int W, int H,
-                                                                       const __grid_constant__ Taps2 tp) {
+// Row-pass sources: a plane, or the baseline preset's halation source
+// max(0, R - threshold) formed from interleaved RGB as it is read.
+struct PlaneSource {
+    const float* __restrict__ p;
+    __device__ float operator()(size_t i) const { return __ldg(p + i); }
+};
+struct HalationSource {
+    const float* __restrict__ rgb;
+    float threshold;
+    __device__ float operator()(size_t i) const { return fmaxf(0.0f, __ldg(rgb + 3 * i) - threshold); }
+};
+
+template <class Src>
+__global__ void __launch_bounds__(R64_ROW_THREADS) blur_rows_r64_kernel(const Src in, float* __restrict__ out, int W,
+                                                                       int H, const __grid_constant__ Taps2 tp) {
     static_assert(R64_ROW_OUT % 2 == 0, "outputs go in pairs");
     __shared__ __align__(16) float s[R64_ROW_TILE + 2 * R64];
     const int y = blockIdx.y, x0 = blockIdx.x * R64_ROW_TILE;
-    const float* row = in + (size_t)y * W;
-    for (int j = threadIdx.x; j < R64_ROW_TILE + 2 * R64; j += blockDim.x)
-        s[j] = __ldg(row + reflect(x0 - R64 + j, W));
+    const size_t row = (size_t)y * W;
+    for (int j = threadIdx.x; j < R64_ROW_TILE + 2 * R64; j += blockDim.x) s[j] = in(row + reflect(x0 - R64 + j, W));
     __syncthreads();
     const int xb = R64_ROW_OUT * threadIdx.x;
     float2 acc[R64_ROW_OUT / 2];
@@ -320,13 +342,28 @@ int blur_rows(const float* in, float* out, int W, int H, const float* taps, int 
     for (int i = 0; i < 2 * R + 1; i++) tp.t[i] = taps[i];
     if (R == R64) {
         dim3 rg((W + R64_ROW_TILE - 1) / R64_ROW_TILE, H);
-        blur_rows_r64_kernel<<<rg, R64_ROW_THREADS, 0, s>>>(in, out, W, H, pair_taps(tp));
+        blur_rows_r64_kernel<<<rg, R64_ROW_THREADS, 0, s>>>(PlaneSource{in}, out, W, H, pair_taps(tp));
     } else {
         dim3 rg((W + ROW_TILE - 1) / ROW_TILE, H);
         blur_rows_kernel<<<rg, ROW_TILE, 0, s>>>(in, out, W, H, tp);
     }
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "blur rows");
+    return IMOPS_OK;
+}
+
+// The baseline preset's halation row pass straight from interleaved RGB: the
+// radius-64 row blur of max(0, R - threshold), the source formed as it is
+// read instead of as a plane of its own.
+static int blur_rows_halation(const float* rgb, float threshold, float* out, int W, int H, const float* taps,
+                              cudaStream_t s) {
+    Taps tp;
+    tp.R = R64;
+    for (int i = 0; i < 2 * R64 + 1; i++) tp.t[i] = taps[i];
+    dim3 rg((W + R64_ROW_TILE - 1) / R64_ROW_TILE, H);
+    blur_rows_r64_kernel<<<rg, R64_ROW_THREADS, 0, s>>>(HalationSource{rgb, threshold}, out, W, H, pair_taps(tp));
+    note_launch();
+    IMOPS_CUDA_TRY(cudaGetLastError(), "halation row pass");
     return IMOPS_OK;
 }
 
@@ -438,12 +475,14 @@ __global__ void dir_apply_kernel(float* __restrict__ planes, const float* __rest
 // sum of squares (f64) stored in partial[plane][block] for the variance.
 // Plane z holds RNG layer layer0 + z.  Radius <= GR_MAXR.
 //
-// Tiles are 128 x 32: the three layers' noise and one row-blurred layer take
-// 80 KB at radius 3, so two blocks (32 warps) share an SM.  Inside the image
+// Tiles are 128 x 39: the three layers' noise and one row-blurred layer take
+// 96 KB at radius 3, so two blocks (32 warps) share an SM.  Inside the image
 // a thread generates a run of GR_RUN consecutive pixels of a row, whose
 // layers share all but the last two draws of the next pixel
-// (grain_noise_run): 12 GR_RUN + 2 draws a run instead of 14 a pixel.
-constexpr int GR_TW = 128, GR_TH = 32, GR_MAXR = 16, GR_RUN = 4;
+// (grain_noise_run): 12 GR_RUN + 2 draws a run instead of 14 a pixel.  The
+// 45 rows of a tile and its halo at radius 3 are 1530 runs, three for each
+// of the 512 threads.
+constexpr int GR_TW = 128, GR_TH = 39, GR_MAXR = 16, GR_RUN = 4;
 constexpr int GR_THREADS = 512, GR_TY = GR_THREADS / 32;
 static_assert(GR_TW == 128, "the blur loops index tile columns with & 127");
 
@@ -784,17 +823,20 @@ struct Pairs81 {
 
 struct Base81 {
     BaselineSpec B;
+    ExposeSpec X;
     Pairs81 P;
     float2 tap2[2 * HAL_R + 2];
 };
 
 // One thread per 16 consecutive rows of a column: the halation column pass
 // (register sliding window, tap pairs as parameter-bank operands, ascending
-// tap order as in blur_cols), then per pixel the logistic curves, grain and
-// the 81-bin scan with its tables as parameter-bank operands.
+// tap order as in blur_cols), then per pixel the exposure of the three layers
+// from its RGB, the logistic curves, grain and the 81-bin scan with its
+// tables as parameter-bank operands; the result replaces the pixel's RGB
+// (each pixel is read, a step ahead, and written by the same thread).
 __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kernel(
-    const float* __restrict__ a, const float* __restrict__ hr, const float* __restrict__ noise,
-    const double* __restrict__ sumsq, int W, int H, const __grid_constant__ Base81 c, float* __restrict__ rgb) {
+    const float* __restrict__ hr, const float* __restrict__ noise, const double* __restrict__ sumsq, int W, int H,
+    const __grid_constant__ Base81 c, float* __restrict__ rgb) {
     static_assert(HAL_R == R64, "the fused scan's column pass is the radius-64 window");
     static_assert(R64_COL_OUT % 2 == 0, "column outputs go in pairs");
     __shared__ float s[(R64_COL_TH + 2 * HAL_R) * R64_COL_TW];
@@ -827,9 +869,9 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
         }
     }
     // Two pixels (rows j and j+1 of the column) a step: each table pair is
-    // fetched once for both, and the next step's exposure and noise are
-    // loaded while this step is scanned, so the global-load latency hides
-    // behind the 81-bin loop.  Each pixel's arithmetic is unchanged.
+    // fetched once for both, and the next step's RGB and noise are loaded
+    // while this step is scanned, so the global-load latency hides behind
+    // the 81-bin loop.  Each pixel's arithmetic is unchanged.
     static_assert(R64_COL_OUT % 2 == 0, "pixels go in pairs");
     const bool grain = c.B.grain_sigma > 0.0f;
     float na[2][3], nz[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
@@ -839,7 +881,7 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
             const size_t pp = (size_t)min(y0 + rb + jj + u, H - 1) * W + x;
 #pragma unroll
             for (int e = 0; e < 3; e++) {
-                na[u][e] = a[e * n + pp];
+                na[u][e] = rgb[3 * pp + e];
                 if (grain) nz[u][e] = noise[e * n + pp];
             }
         }
@@ -851,12 +893,15 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kern
         if (y >= H) break;
         float ca[2][3], cz[2][3];
 #pragma unroll
-        for (int u = 0; u < 2; u++)
+        for (int u = 0; u < 2; u++) {
+            float w[3];
+            basis_weights(c.X, na[u][0], na[u][1], na[u][2], w);
 #pragma unroll
             for (int e = 0; e < 3; e++) {
-                ca[u][e] = na[u][e];
+                ca[u][e] = layer_exposure(c.X, w, e);
                 cz[u][e] = nz[u][e];
             }
+        }
         if (j + 2 < R64_COL_OUT && y + 2 < H) fetch(j + 2);
         float bsum[2] = {bs[0].x, bs[0].y};
 #pragma unroll
@@ -1039,6 +1084,7 @@ __device__ __forceinline__ void split_bf16(float a, float b, uint32_t& hi, uint3
 
 struct Base81TC {
     BaselineSpec B;
+    ExposeSpec X;
     float2 tap2[2 * HAL_R + 2];
     tc::Tables T;
 };
@@ -1047,8 +1093,8 @@ struct Base81TC {
 __device__ unsigned g_tc_timeouts = 0;
 
 __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 2) scan81_tc_kernel(
-    const float* __restrict__ a, const float* __restrict__ hr, const float* __restrict__ noise,
-    const double* __restrict__ sumsq, int W, int H, const __grid_constant__ Base81TC c, float* __restrict__ rgb) {
+    const float* __restrict__ hr, const float* __restrict__ noise, const double* __restrict__ sumsq, int W, int H,
+    const __grid_constant__ Base81TC c, float* __restrict__ rgb) {
     using namespace tc;
     static_assert(R64_COL_GROUPS == 8, "two warpgroups of four warps");
     extern __shared__ __align__(1024) uint8_t dsm[];
@@ -1110,8 +1156,8 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 2) scan81_tc_kern
     // Per step j (row y0 + rb + j of every warp: 128 pixels a warpgroup) the
     // MMAs of one step overlap the CUDA-core work of its neighbours: MMA2 of
     // step j runs while the densities of step j+1 are formed, MMA1 of step
-    // j+1 while step j's pixels are stored.  Exposure and noise are loaded a
-    // step ahead.
+    // j+1 while step j's pixels are stored.  RGB and noise are loaded a step
+    // ahead (each pixel is read and written by the same thread).
     float la[3] = {0.f, 0.f, 0.f}, lz[3] = {0.f, 0.f, 0.f};  // inputs of the next step
     auto load_inputs = [&](int jj) {
         const int yy = y0 + rb + jj;
@@ -1119,7 +1165,7 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 2) scan81_tc_kern
             const size_t p = (size_t)yy * W + x;
 #pragma unroll
             for (int e = 0; e < 3; e++) {
-                la[e] = a[e * n + p];
+                la[e] = rgb[3 * p + e];
                 lz[e] = grain ? noise[e * n + p] : 0.0f;
             }
         }
@@ -1136,9 +1182,11 @@ __global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 2) scan81_tc_kern
                 if (2 * q == jj) bsum = bs[q].x;
                 if (2 * q + 1 == jj) bsum = bs[q].y;
             }
+            float w[3];
+            basis_weights(c.X, la[0], la[1], la[2], w);
 #pragma unroll
             for (int e = 0; e < 3; e++) {
-                const float E = la[e] + c.B.hal_strength * c.B.bleed[e] * bsum;
+                const float E = layer_exposure(c.X, w, e) + c.B.hal_strength * c.B.bleed[e] * bsum;
                 D[e] = curve_density(E, c.B.dmax[e], c.B.k[e], c.B.x0[e]);
                 if (grain) D[e] += c.B.grain_sigma * lz[e] * norm[e];
             }
@@ -1258,6 +1306,7 @@ static float host_bf16_value(uint16_t h) {
 static void build_base81_tc(const Stock& st, Base81TC* hp) {
     std::memset(hp, 0, sizeof(*hp));
     hp->B = st.base;
+    hp->X = st.expose;
     for (int k = 0; k <= 2 * HAL_R + 1; k++)
         hp->tap2[k] = make_float2(k <= 2 * HAL_R ? st.hal_taps[k] : 0.0f, k >= 1 ? st.hal_taps[k - 1] : 0.0f);
     const ScanSpec81& S = st.scan81;
@@ -1286,6 +1335,7 @@ static void build_base81_tc(const Stock& st, Base81TC* hp) {
 // Host: the pair tables of the 81-bin scan and halation taps.
 static void build_base81(const Stock& st, Base81* hp) {
     hp->B = st.base;
+    hp->X = st.expose;
     const ScanSpec81& S = st.scan81;
     for (int e = 0; e < 3; e++) {
         for (int l = 0; l < NP81; l++) hp->P.ne[e][l] = make_float2(-S.eps[e][2 * l], -S.eps[e][2 * l + 1]);
@@ -1533,12 +1583,13 @@ int stage_ctx(const ImopsFilmParams* P, int W, int H, size_t extra, cudaStream_t
 namespace imops {
 namespace film {
 
-// Bytes of the baseline preset's working set for a W x H image: the three
-// layer exposures, the halation source and its row pass, three grain fields,
-// the grain's block sums (and the Arena's 256-byte alignment).
+// Bytes of the baseline preset's working set for a W x H image: the
+// halation row pass, three grain fields, the grain's block sums (and the
+// Arena's 256-byte alignment).  The layer exposures and the halation source
+// are formed from the RGB where they are read.
 size_t baseline_scratch_bytes(int W, int H) {
     const size_t n = (size_t)W * H;
-    return (3 + 1 + 1 + 3) * n * 4 + grain_partials(W, H, 3) * 8 + 4096;
+    return (1 + 3) * n * 4 + grain_partials(W, H, 3) * 8 + 4096;
 }
 
 int baseline_stock(int W, const ImopsBaselineFilm& P, Stock* st) {
@@ -1608,19 +1659,18 @@ int baseline_forward_in(float* rgb, int W, int H, const ImopsBaselineFilm& P, co
                         cudaStream_t s) {
     int rc;
     const size_t n = (size_t)W * H;
+    if (st.expose.E != 3 || !st.expose.hal_src)
+        return fail(IMOPS_ERR_INVALID_STOCK, "film: the baseline preset's exposure is three layers with halation");
     Arena A{static_cast<char*>(scratch), 0};
     double* sums = A.take<double>(4);
-    float* a = A.take<float>(3 * n);
-    float* hal = A.take<float>(n);
     float* hr = A.take<float>(n);
     float* noise = A.take<float>(3 * n);
     double* gpart = A.take<double>(grain_partials(W, H, 3));
     Base81 hp;
     build_base81(st, &hp);
-    int g = grid_for(n);
     if (P.grain_on && P.grain_sigma != 0.0f) {
-        // grain fields on the side stream while the exposure and the row pass
-        // run on s; the scan waits for both.  The lock keeps one call's
+        // grain fields on the side stream while the halation row pass runs on
+        // s; the scan waits for both.  The lock keeps one call's
         // record / wait pairs of the shared events together.
         Taps tp;
         if ((rc = taps_for(fmaxf(P.grain_blur, 1.0f), &tp))) return rc;
@@ -1631,14 +1681,10 @@ int baseline_forward_in(float* rgb, int W, int H, const ImopsBaselineFilm& P, co
         IMOPS_CUDA_TRY(cudaStreamWaitEvent(ss->side, ss->fork, 0), "cudaStreamWaitEvent(film fork)");
         if ((rc = grain_fields(noise, W, H, P.seed, 0, 3, tp, gpart, sums, ss->side))) return rc;
         IMOPS_CUDA_TRY(cudaEventRecord(ss->join, ss->side), "cudaEventRecord(film join)");
-        expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
-        note_launch();
-        if ((rc = blur_rows(hal, hr, W, H, st.hal_taps, HAL_R, s))) return rc;
+        if ((rc = blur_rows_halation(rgb, st.expose.hal_threshold, hr, W, H, st.hal_taps, s))) return rc;
         IMOPS_CUDA_TRY(cudaStreamWaitEvent(s, ss->join, 0), "cudaStreamWaitEvent(film join)");
     } else {
-        expose_kernel<<<g, 256, 0, s>>>(rgb, n, st.expose, a, hal);
-        note_launch();
-        if ((rc = blur_rows(hal, hr, W, H, st.hal_taps, HAL_R, s))) return rc;
+        if ((rc = blur_rows_halation(rgb, st.expose.hal_threshold, hr, W, H, st.hal_taps, s))) return rc;
     }
     dim3 cb(R64_COL_TW, R64_COL_GROUPS), cg((W + R64_COL_TW - 1) / R64_COL_TW, (H + R64_COL_TH - 1) / R64_COL_TH);
     if (P.scan == IMOPS_SCAN_BF16_TC) {
@@ -1647,9 +1693,9 @@ int baseline_forward_in(float* rgb, int W, int H, const ImopsBaselineFilm& P, co
         IMOPS_CUDA_TRY(cudaFuncSetAttribute(scan81_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)tc::SMEM_REQ),
                        "cudaFuncSetAttribute(tensor-core scan)");
-        scan81_tc_kernel<<<cg, cb, tc::SMEM_REQ, s>>>(a, hr, noise, sums, W, H, tp, rgb);
+        scan81_tc_kernel<<<cg, cb, tc::SMEM_REQ, s>>>(hr, noise, sums, W, H, tp, rgb);
     } else {
-        scan81_fused_kernel<<<cg, cb, 0, s>>>(a, hr, noise, sums, W, H, hp, rgb);
+        scan81_fused_kernel<<<cg, cb, 0, s>>>(hr, noise, sums, W, H, hp, rgb);
     }
     note_launch();
     IMOPS_CUDA_TRY(cudaGetLastError(), "baseline film kernels");

@@ -16,11 +16,11 @@
 
 namespace {
 
-// Largest image: 2 MP (a 1920 x 1080 preview fits).  The preset needs 32
-// bytes a pixel (eight f32 planes) plus the grain's block sums (three doubles
-// a 128 x 32 tile), which for 2 MP stay below 1.5 MiB at any aspect ratio.
+// Largest image: 2 MP (a 1920 x 1080 preview fits).  The preset needs 16
+// bytes a pixel (four f32 planes) plus the grain's block sums (three doubles
+// a 128 x 39 tile), which for 2 MP stay below 1.5 MiB at any aspect ratio.
 constexpr size_t kMaxPixels = (size_t)1 << 21;
-constexpr size_t kScratchBytes = 32 * kMaxPixels + ((size_t)2 << 20);
+constexpr size_t kScratchBytes = 16 * kMaxPixels + ((size_t)2 << 20);
 
 }  // namespace
 
