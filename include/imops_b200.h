@@ -252,8 +252,8 @@ int imops_film_process(float *rgb, int w, int h, int color_space, const ImopsFil
  * a fixed memory budget through its own allocator must not have the library
  * allocate behind its back, and a real-time preview loop cannot take the
  * device-wide synchronisation cudaMalloc and cudaFree may cause.  The
- * preset's working planes (32 bytes a pixel) live in one fixed array of
- * device memory, about 65 MiB, which every GPU that loads the library holds
+ * preset's working planes (16 bytes a pixel) live in one fixed array of
+ * device memory, about 34 MiB, which every GPU that loads the library holds
  * until the process exits; the caller still passes the image.
  *  - Images above imops_film_noalloc_max_pixels() pixels (2,097,152: a
  *    1920 x 1080 preview fits) are rejected with IMOPS_ERR_UNSUPPORTED_SIZE.
