@@ -180,8 +180,15 @@ template <class P>
 __device__ void fill(const P& p, const Geo& g, float* mos) {
     const int top = g.top, left = g.left, W = p.W, H = p.H;
     if (g.rrmin == 0 && g.ccmin == 0 && g.rrmax == g.rr1 && g.ccmax == g.cc1) {
-        fill_pass(mos, 0, g.rr1, 0, g.cc1, [](int rr, int cc) { return rr * TS + cc; },
-                  [&](int rr, int cc) { return get_in(p, rr + top, cc + left); });
+        // a whole 128 x 128 tile inside the image: every load in flight
+        // before the first store
+        constexpr int RPT = TS / (NTHREADS / TS);
+        const int cc = (int)(threadIdx.x & (TS - 1)), r0 = (int)(threadIdx.x / TS);
+        float v[RPT];
+#pragma unroll
+        for (int i = 0; i < RPT; i++) v[i] = p.in(top + r0 + i * (NTHREADS / TS), left + cc);
+#pragma unroll
+        for (int i = 0; i < RPT; i++) mos[(r0 + i * (NTHREADS / TS)) * TS + cc] = v[i];
         return;
     }
     if (g.rrmin > 0)
@@ -275,12 +282,17 @@ extern __shared__ __align__(16) float amaze_smem[];
 // [lo, rr1-lo) x cols [lo, cc1-lo):
 //     alt = (w(r-1,c-1) + w(r-1,c+1) + w(r+1,c-1) + w(r+1,c+1)) / 4
 //     if |0.5 - w(r,c)| < |0.5 - alt|: w(r,c) = alt
-// where row r-1 holds already-updated values.  Lane L owns sites k = L and
-// L+32 of every row and keeps the updated row in registers; the neighbours
-// (r-1, c-+1) are sites k-1/k/k+1 of the previous row, fetched by shuffle.
-// Sites outside the updated range keep their stored values.  Division by 4
-// is exact, so * 0.25f gives the same bits.  post(r, c, w_new) runs after
-// each update.  The array is amaze_smem[woff ...].
+// where row r-1 holds already-updated values.  Site k of a row is column
+// lo + par + 2k (par: the row's R/B column parity, alternating by row); lane
+// L owns sites 2L and 2L+1 of every row.  The upper neighbours of site k are
+// sites k-1, k (par 0) or k, k+1 (par 1) of the row above, so a lane needs
+// one value of one neighbouring lane a row.  Each lane carries its two sites
+// of the row above: the updated value where that row was updated, else the
+// stored one (sites past the row's range, and the row before lo); site -1
+// (lane 0, par 0) is read from memory.  The lower neighbours and the own
+// value are the stored ones, loaded a row ahead.  Division by 4 is exact,
+// so * 0.25f gives the same bits.  post(r, c, i, w_new) runs after each
+// update.  The array is amaze_smem[woff ...] (R/B half array).
 template <class P, class Post>
 __device__ void wavefront(const P& p, const Geo& g, int woff, int lo, Post post) {
     float* const w = amaze_smem + woff;
@@ -289,61 +301,68 @@ __device__ void wavefront(const P& p, const Geo& g, int woff, int lo, Post post)
     // Bayer rows alternate the column parity of their R/B sites
     int par = p.cfa.at(g.top + lo, g.left + 2) & 1;
     const int n0 = (chi - lo + 1) >> 1, n1 = (chi - lo) >> 1;
-    // row being updated: own value, stored upper neighbours (used where the
-    // previous row was not updated) and the lower neighbours (not updated yet)
-    float own[2], upl[2], upr[2], lwl[2], lwr[2];
-    auto load = [&](int rr, int pr, float* o, float* ul, float* ur, float* dl, float* dr) {
-        const int c0 = lo + pr, n = pr ? n1 : n0;
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const int i = rr * TS + c0 + 2 * min(lane + 32 * j, n - 1);
-            o[j] = w[i >> 1];
-            ul[j] = w[(i - M1) >> 1];
-            ur[j] = w[(i - P1) >> 1];
-            dl[j] = w[(i + P1) >> 1];
-            dr[j] = w[(i + M1) >> 1];
-        }
+    const int kA = 2 * lane, kB = 2 * lane + 1;
+    // stored value of site k of row r (parity pr); columns past the tile
+    // (sites that are never a neighbour) read the last column
+    auto at = [&](int r, int pr, int k) { return w[(r * TS + min(lo + pr + 2 * k, TS - 1)) >> 1]; };
+    // the row above lo, never updated
+    float pA = at(lo - 1, par ^ 1, kA), pB = at(lo - 1, par ^ 1, kB);
+    // own and lower neighbours (r+1, c-1), (r+1, c+1) of the row being updated
+    auto load = [&](int r, int pr, float& oA, float& oB, float& dlA, float& drA, float& dlB, float& drB) {
+        const int cA = min(lo + pr + 2 * kA, TS - 1), cB = min(lo + pr + 2 * kB, TS - 1);
+        oA = w[(r * TS + cA) >> 1];
+        oB = w[(r * TS + cB) >> 1];
+        dlA = w[(r * TS + cA + P1) >> 1];
+        drA = w[(r * TS + cA + M1) >> 1];
+        dlB = w[(r * TS + cB + P1) >> 1];
+        drB = w[(r * TS + cB + M1) >> 1];
     };
-    load(lo, par, own, upl, upr, lwl, lwr);
-    float prevA = 0.f, prevB = 0.f;  // updated previous row, sites lane / lane+32
-    int nprev = 0;
+    float oA, oB, dlA, drA, dlB, drB;
+    load(lo, par, oA, oB, dlA, drA, dlB, drB);
     for (int rr = lo; rr < rhi; rr++) {
         const int n = par ? n1 : n0, c0 = lo + par;
-        float nown[2], nul[2], nur[2], ndl[2], ndr[2];
-        if (rr + 1 < rhi) load(rr + 1, par ^ 1, nown, nul, nur, ndl, ndr);
-        const float aM = __shfl_up_sync(0xffffffffu, prevA, 1), aP = __shfl_down_sync(0xffffffffu, prevA, 1);
-        const float bM = __shfl_up_sync(0xffffffffu, prevB, 1), bP = __shfl_down_sync(0xffffffffu, prevB, 1);
-        const float a31 = __shfl_sync(0xffffffffu, prevA, 31), b0 = __shfl_sync(0xffffffffu, prevB, 0);
-        float nv[2];
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const int k = lane + 32 * j;
-            const float vm1 = j == 0 ? aM : (lane == 0 ? a31 : bM);  // previous-row site k-1
-            const float v0 = j == 0 ? prevA : prevB;                 // site k
-            const float vp1 = j == 0 ? (lane == 31 ? b0 : aP) : bP;  // site k+1
-            const int kl = par == 0 ? k - 1 : k, kr = par == 0 ? k : k + 1;
-            const float ul = (kl >= 0 && kl < nprev) ? (par == 0 ? vm1 : v0) : upl[j];
-            const float ur = (kr >= 0 && kr < nprev) ? (par == 0 ? v0 : vp1) : upr[j];
-            const float alt = (ul + ur + lwl[j] + lwr[j]) * 0.25f;
-            const float v = fabsf(0.5f - own[j]) < fabsf(0.5f - alt) ? alt : own[j];
-            nv[j] = v;
-            if (k < n) {
-                w[(rr * TS + c0 + 2 * k) >> 1] = v;
-                post(rr, c0 + 2 * k, rr * TS + c0 + 2 * k, v);
-            }
+        float noA, noB, ndlA, ndrA, ndlB, ndrB;
+        if (rr + 1 < rhi) load(rr + 1, par ^ 1, noA, noB, ndlA, ndrA, ndlB, ndrB);
+        float ulA, urA, ulB, urB;
+        if (par == 0) {
+            // site 2L-1 above: lane L-1's second site; site -1 from memory
+            float left = __shfl_up_sync(0xffffffffu, pB, 1);
+            if (lane == 0) left = w[((rr - 1) * TS + lo - 1) >> 1];
+            ulA = left;
+            urA = pA;
+            ulB = pA;
+            urB = pB;
+        } else {
+            // site 2L+2 above: lane L+1's first site
+            const float right = __shfl_down_sync(0xffffffffu, pA, 1);
+            ulA = pA;
+            urA = pB;
+            ulB = pB;
+            urB = right;
         }
-        prevA = nv[0];
-        prevB = nv[1];
-        nprev = n;
+        const float altA = (ulA + urA + dlA + drA) * 0.25f;
+        const float altB = (ulB + urB + dlB + drB) * 0.25f;
+        const float vA = fabsf(0.5f - oA) < fabsf(0.5f - altA) ? altA : oA;
+        const float vB = fabsf(0.5f - oB) < fabsf(0.5f - altB) ? altB : oB;
+        if (kA < n) {
+            const int i = rr * TS + c0 + 2 * kA;
+            w[i >> 1] = vA;
+            post(rr, c0 + 2 * kA, i, vA);
+        }
+        if (kB < n) {
+            const int i = rr * TS + c0 + 2 * kB;
+            w[i >> 1] = vB;
+            post(rr, c0 + 2 * kB, i, vB);
+        }
+        pA = kA < n ? vA : oA;
+        pB = kB < n ? vB : oB;
         par ^= 1;
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            own[j] = nown[j];
-            upl[j] = nul[j];
-            upr[j] = nur[j];
-            lwl[j] = ndl[j];
-            lwr[j] = ndr[j];
-        }
+        oA = noA;
+        oB = noB;
+        dlA = ndlA;
+        drA = ndrA;
+        dlB = ndlB;
+        drB = ndrB;
     }
     __syncwarp();
 }
@@ -496,7 +515,7 @@ __device__ void st_vpass(const P& p, const Geo& g, const Bufs& b, uint8_t* segma
         float rawp[2] = {0.f, 0.f}, altp[4] = {0.f, 0.f, 0.f, 0.f}, dgp[4] = {0.f, 0.f, 0.f, 0.f};
         float vwp[2] = {0.f, 0.f}, Ap[4] = {0.f, 0.f, 0.f, 0.f}, Bp[4] = {0.f, 0.f, 0.f, 0.f};
         const int nk = r1 - r0 + 4;  // steps t = r0-2 .. r1+1
-#pragma unroll 1
+#pragma unroll 2
         for (int k = 0; k < nk; k++) {
             const int t = r0 - 2 + k;
             float raw = 0.f, alt = 0.f, dg = 0.f, vw = 0.f, A = 0.f, B = 0.f;
@@ -1263,8 +1282,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) amaze_kernel(const __grid_constan
 
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
         Geo g = tile_geo(p.W, p.H, -16 + (tile / p.ntx) * 96, -16 + (tile % p.ntx) * 96);
-        for (int k = threadIdx.x; k < NF; k += blockDim.x) b.mos[k] = 0.0f;
-        __syncthreads();
+        if (!(g.rrmin == 0 && g.ccmin == 0 && g.rrmax == g.rr1 && g.ccmax == g.cc1)) {
+            // edge tiles: the border fill leaves parts of the tile zero
+            for (int k = threadIdx.x; k < NF; k += blockDim.x) b.mos[k] = 0.0f;
+            __syncthreads();
+        }
         fill(p, g, b.mos);
         __syncthreads();
         st_vpass(p, g, b, segmap);
