@@ -101,10 +101,17 @@ __device__ void mean3(const Img& im, int r, int c, float* o) {
 // estimate on the frame less 2, red / blue on radius 6, refinement on 5, red /
 // blue on 4, refinement on 3, red / blue and Lab on 2, the difference on 1,
 // each stage over the cells the next one reads.  The directions run one
-// after another through the same buffers; each thread keeps its four
-// outputs' red, green and blue of every direction in registers for the vote,
-// and the four difference planes stay in shared memory.  Every cell is the
-// same f32 arithmetic, in the same order, as the staged specification.
+// after another through the same buffers; each thread keeps its two
+// outputs' red, green and blue of every direction for the vote, and the four
+// difference planes stay in shared memory.  Every cell is the same f32
+// arithmetic, in the same order, as the staged specification.
+//
+// Work a cell does not need is not done: the green stages (step 1 and the
+// refinements) return the sample at green cells, so the green planes hold
+// the mosaic there from the start and those stages run over per-tile lists
+// of the non-green cells; and the red / blue sums take each phase's list of
+// red and blue window sites (at most four of each: two or three in the
+// X-Trans pattern) instead of testing all nine.
 namespace fused {
 
 constexpr int T = 32;              // outputs a tile side
@@ -123,16 +130,32 @@ __constant__ int OFF[4] = {1, S, S + 1, S - 1};  // frame step of each direction
 //   bits 11-19  blue sites of the window
 //   bits 20-23  green orthogonal neighbours (0,+1) (0,-1) (+1,0) (-1,0)
 //   bits 24+4d  direction d: green at +1, +2, -1, -2 steps
+//
+// and the red / blue window sites of each phase in row-major order (rbn):
+//   bits 0-1    its colour
+//   bits 2-4    number of red sites (centre excluded), bits 5-7 blue
+//   bits 8+7t   frame offset + 64 of red site t (t < 4), bits 36+7t blue
+// `lists` is 0 when a phase has more than four of either (a 6x6 CFA other
+// than X-Trans), and the red / blue step then tests the window masks.
 struct Masks {
     unsigned long long m[36];
+    unsigned long long rbn[36];
+    int lists;
 };
 constexpr int MB_R = 2, MB_B = 11, MB_GO = 20, MB_DIR = 24;
 
-// shared memory: mosaic, two green buffers, red, blue, two Lab planes (the
-// third takes the free green buffer), four difference planes, the phase
-// table and each frame cell's phase: 91 KB, two blocks an SM
-constexpr size_t SMEM = (size_t)(7 * N + 4 * DS * DS) * sizeof(float) + 36 * 8 + N;
-static_assert((7 * N + 4 * DS * DS) % 2 == 0, "the mask table is 8-byte aligned");
+// per-tile lists of the non-green frame cells in [LO, S - LO)^2 for the
+// green stages, LO = 2, 4, 6
+constexpr int NL0 = (S - 4) * (S - 4), NL1 = (S - 8) * (S - 8), NL2 = (S - 12) * (S - 12);
+constexpr int NLCAP = NL0 + NL1 + NL2;
+
+// shared memory: mosaic, two green planes, red, blue, two Lab planes (the
+// third is the red plane, overwritten in place), four difference planes,
+// the two phase tables, the non-green lists and their lengths, and each
+// frame cell's phase: 100 KB, two blocks an SM
+constexpr size_t SMEM = (size_t)(7 * N + 4 * DS * DS) * sizeof(float) + 2 * 36 * 8 + NLCAP * 2 + 16 + N;
+static_assert((7 * N + 4 * DS * DS) % 2 == 0, "the phase tables are 8-byte aligned");
+static_assert(NLCAP % 2 == 0, "the list lengths are 4-byte aligned");
 
 // host: the colour facts of the 36 phases of a 6x6 CFA
 inline Masks build_masks(const CfaDev& c) {
@@ -158,13 +181,31 @@ inline Masks build_masks(const CfaDev& c) {
             }
             M.m[py * 6 + px] = v;
         }
+    M.lists = 1;
+    for (int py = 0; py < 6; py++)
+        for (int px = 0; px < 6; px++) {
+            auto col = [&](int y, int x) { return c.at(py + y, px + x); };
+            unsigned long long v = (unsigned long long)col(0, 0);
+            int nr = 0, nb = 0;
+            for (int a = -1; a <= 1; a++)
+                for (int b = -1; b <= 1; b++) {
+                    if (a == 0 && b == 0) continue;
+                    const unsigned long long o = (unsigned long long)(a * S + b + 64);
+                    if (col(a, b) == 0 && nr++ < 4) v |= o << (8 + 7 * (nr - 1));
+                    if (col(a, b) == 2 && nb++ < 4) v |= o << (36 + 7 * (nb - 1));
+                }
+            if (nr > 4 || nb > 4) M.lists = 0;
+            v |= (unsigned long long)(nr & 7) << 2 | (unsigned long long)(nb & 7) << 5;
+            M.rbn[py * 6 + px] = v;
+        }
     return M;
 }
 
 struct Frame {
     float *m, *ga, *gb, *r, *b, *l1, *l2, *d;
     const uint8_t* ph;                 // phase of each frame cell
-    const unsigned long long* masks;   // Masks, in shared memory
+    const unsigned long long* masks;   // Masks::m, in shared memory
+    const unsigned long long* rbn;     // Masks::rbn, in shared memory
 };
 
 // min / max / sum / count of the green orthogonal neighbours, branch-free in
@@ -203,8 +244,31 @@ __device__ __forceinline__ float green1_f(const Frame& F, int f, int d, int off)
 }
 
 // red and blue at f from the green plane G: their sums over the window's
-// red / blue sites in row-major order
+// red / blue sites in row-major order.  LISTS: from the phase's site lists
+// (each list in the same row-major order as the masks).
+template <bool LISTS>
 __device__ __forceinline__ void rb_f(const Frame& F, const float* G, int f, float& R, float& B) {
+    if constexpr (LISTS) {
+        const unsigned long long L = F.rbn[F.ph[f]];
+        const int own = (int)(L & 3ull), nr = (int)((L >> 2) & 7ull), nb = (int)((L >> 5) & 7ull);
+        float sr = 0.0f, sbl = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 4; t++)
+            if (t < nr) {
+                const int j = f + (int)((L >> (8 + 7 * t)) & 127ull) - 64;
+                sr = sr + (F.m[j] - G[j]);
+            }
+#pragma unroll
+        for (int t = 0; t < 4; t++)
+            if (t < nb) {
+                const int j = f + (int)((L >> (36 + 7 * t)) & 127ull) - 64;
+                sbl = sbl + (F.m[j] - G[j]);
+            }
+        const float g = G[f];
+        R = own == 0 ? F.m[f] : (nr ? g + sr / (float)nr : g);
+        B = own == 2 ? F.m[f] : (nb ? g + sbl / (float)nb : g);
+        return;
+    }
     const unsigned long long M = F.masks[F.ph[f]];
     const unsigned mr = (unsigned)(M >> MB_R) & 511u, mb = (unsigned)(M >> MB_B) & 511u;
     float sr = 0.0f, sbl = 0.0f;
@@ -243,6 +307,13 @@ __device__ __forceinline__ void over(Fn fn) {
     for (int k = threadIdx.x; k < W * W; k += THREADS) fn((LO + k / W) * S + LO + k % W);
 }
 
+// the cells of a list, spread over the block
+template <class Fn>
+__device__ __forceinline__ void over_list(const uint16_t* list, int n, Fn fn) {
+    for (int k = threadIdx.x; k < n; k += THREADS) fn((int)list[k]);
+}
+
+template <bool LISTS>
 __global__ void __launch_bounds__(THREADS, 2) tile_kernel(const __grid_constant__ Img im, const __grid_constant__ Masks mk,
                                                          float* __restrict__ out) {
     extern __shared__ __align__(16) float fsm[];
@@ -256,11 +327,18 @@ __global__ void __launch_bounds__(THREADS, 2) tile_kernel(const __grid_constant_
     F.l2 = fsm + 6 * N;
     F.d = fsm + 7 * N;
     unsigned long long* msk = reinterpret_cast<unsigned long long*>(fsm + 7 * N + 4 * DS * DS);
-    uint8_t* phw = reinterpret_cast<uint8_t*>(msk + 36);
+    unsigned long long* rbn = msk + 36;
+    uint16_t* ngl = reinterpret_cast<uint16_t*>(rbn + 36);  // non-green lists, LO = 2, 4, 6
+    int* nng = reinterpret_cast<int*>(ngl + NLCAP);         // their lengths
+    uint8_t* phw = reinterpret_cast<uint8_t*>(nng + 4);
     F.masks = msk;
+    F.rbn = rbn;
     F.ph = phw;
     const int oy = BAND + blockIdx.y * T, ox = BAND + blockIdx.x * T;  // first output of the tile
-    if (threadIdx.x < 36) msk[threadIdx.x] = mk.m[threadIdx.x];
+    if (threadIdx.x < 36) {
+        msk[threadIdx.x] = mk.m[threadIdx.x];
+        rbn[threadIdx.x] = mk.rbn[threadIdx.x];
+    }
     // frame: image rows oy-9 .. oy+T+8 (clamped at the far edges of a partial
     // tile, whose cells there feed only outputs outside the interior); the
     // phase of each cell in the period (periodic, unclamped)
@@ -271,38 +349,72 @@ __global__ void __launch_bounds__(THREADS, 2) tile_kernel(const __grid_constant_
         F.m[k] = im.m[(size_t)y * im.W + x];
         phw[k] = (uint8_t)(((py0 + fy) % 6) * 6 + (px0 + fx) % 6);
     }
+    __syncthreads();
+    // green cells: both green planes hold the sample, which the green
+    // stages would return there; warps 0-2 list the non-green cells of the
+    // green stages' regions in row-major order
+    for (int k = threadIdx.x; k < N; k += THREADS)
+        if ((msk[phw[k]] & 3ull) == 1ull) F.ga[k] = F.gb[k] = F.m[k];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < 3) {
+        const int lo = 2 + 2 * warp, w = S - 2 * lo;
+        uint16_t* list = ngl + (warp == 0 ? 0 : (warp == 1 ? NL0 : NL0 + NL1));
+        int n = 0;
+        for (int fy = lo; fy < S - lo; fy++)
+            for (int c0 = 0; c0 < w; c0 += 32) {
+                const int f = fy * S + lo + c0 + lane;
+                const bool ng = c0 + lane < w && (msk[phw[f]] & 3ull) != 1ull;
+                const unsigned bal = __ballot_sync(0xffffffffu, ng);
+                if (ng) list[n + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)f;
+                n += __popc(bal);
+            }
+        if (lane == 0) nng[warp] = n;
+    }
     float keep[4][3][OUT];
     __syncthreads();
+    const int n0 = nng[0], n1 = nng[1], n2 = nng[2];
+    const uint16_t *l0 = ngl, *l1 = ngl + NL0, *l2 = ngl + NL0 + NL1;
 #pragma unroll 1
     for (int d = 0; d < 4; d++) {
         const int off = OFF[d];
-        over<2>([&](int f) { F.ga[f] = green1_f(F, f, d, off); });
+        over_list(l0, n0, [&](int f) { F.ga[f] = green1_f(F, f, d, off); });
         __syncthreads();
-        over<3>([&](int f) { rb_f(F, F.ga, f, F.r[f], F.b[f]); });
+        over<3>([&](int f) { rb_f<LISTS>(F, F.ga, f, F.r[f], F.b[f]); });
         __syncthreads();
-        over<4>([&](int f) { F.gb[f] = refine_f(F, F.ga, f, off); });
+        over_list(l1, n1, [&](int f) { F.gb[f] = refine_f(F, F.ga, f, off); });
         __syncthreads();
-        over<5>([&](int f) { rb_f(F, F.gb, f, F.r[f], F.b[f]); });
+        over<5>([&](int f) { rb_f<LISTS>(F, F.gb, f, F.r[f], F.b[f]); });
         __syncthreads();
-        over<6>([&](int f) { F.ga[f] = refine_f(F, F.gb, f, off); });
+        over_list(l2, n2, [&](int f) { F.ga[f] = refine_f(F, F.gb, f, off); });
         __syncthreads();
-        over<7>([&](int f) { rb_f(F, F.ga, f, F.r[f], F.b[f]); });
+        over<7>([&](int f) { rb_f<LISTS>(F, F.ga, f, F.r[f], F.b[f]); });
         __syncthreads();
-        // Lab of this direction's RGB: L into the free green buffer
+#pragma unroll
+        for (int q = 0; q < OUT; q++) {
+            const int o = threadIdx.x + q * THREADS, f = (o / T + 9) * S + o % T + 9;
+            keep[d][0][q] = F.r[f];
+            keep[d][1][q] = F.ga[f];
+            keep[d][2][q] = F.b[f];
+        }
+        __syncthreads();
+        // Lab of this direction's RGB, in place: L over red, a and b into
+        // the Lab planes (the green planes keep their green cells)
         over<7>([&](int f) {
             const float r = F.r[f], g = F.ga[f], b = F.b[f];
             const float x = 0.4338873455660398f * r + 0.3762240091374988f * g + 0.18988864529646143f * b;
             const float y = 0.21263900587151027f * r + 0.715168678767756f * g + 0.07219231536073371f * b;
             const float z = 0.017750040070973232f * r + 0.10944762085523847f * g + 0.8728023390737883f * b;
             const float fx = lab_f(x), fy = lab_f(y), fz = lab_f(z);
-            F.gb[f] = 116.0f * fy - 16.0f;
+            F.r[f] = 116.0f * fy - 16.0f;
             F.l1[f] = 500.0f * (fx - fy);
             F.l2[f] = 200.0f * (fy - fz);
         });
         __syncthreads();
+        // the next direction's first stage touches none of the planes read
+        // here, and its second waits at a barrier after the first
         float* Dd = F.d + d * DS * DS;
         over<8>([&](int f) {
-            const float* L[3] = {F.gb, F.l1, F.l2};
+            const float* L[3] = {F.r, F.l1, F.l2};
             float sp = 0.0f, sm = 0.0f;
 #pragma unroll
             for (int k = 0; k < 3; k++) {
@@ -312,15 +424,8 @@ __global__ void __launch_bounds__(THREADS, 2) tile_kernel(const __grid_constant_
             }
             Dd[(f / S - 8) * DS + (f % S - 8)] = sp + sm;
         });
-#pragma unroll
-        for (int q = 0; q < OUT; q++) {
-            const int o = threadIdx.x + q * THREADS, f = (o / T + 9) * S + o % T + 9;
-            keep[d][0][q] = F.r[f];
-            keep[d][1][q] = F.ga[f];
-            keep[d][2][q] = F.b[f];
-        }
-        __syncthreads();
     }
+    __syncthreads();
     // vote over the 3x3 window of the four difference planes
 #pragma unroll
     for (int q = 0; q < OUT; q++) {
@@ -413,9 +518,11 @@ extern "C" int imops_demosaic_markesteijn3(const float* mosaic, int w, int h, co
     if (iw > 0 && ih > 0) {
         namespace F = xtrans::fused;
         const dim3 grd((iw + F::T - 1) / F::T, (ih + F::T - 1) / F::T);
-        IMOPS_CUDA_TRY(cudaFuncSetAttribute(F::tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F::SMEM),
+        const F::Masks mk = F::build_masks(c);
+        auto kern = mk.lists ? F::tile_kernel<true> : F::tile_kernel<false>;
+        IMOPS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F::SMEM),
                        "cudaFuncSetAttribute(markesteijn3)");
-        F::tile_kernel<<<grd, F::THREADS, F::SMEM, s>>>(im, F::build_masks(c), rgb);
+        kern<<<grd, F::THREADS, F::SMEM, s>>>(im, mk, rgb);
         note_launch();
     }
     const int top = h < BAND ? h : BAND, bottom = h - top < BAND ? h - top : BAND;
