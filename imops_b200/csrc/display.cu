@@ -224,8 +224,20 @@ __device__ __forceinline__ void sigmoid(const Op& o, float& r, float& g, float& 
     l2 = cbrt_fast(l2);
     const float ha = fmaf(OK_M2[5], l2, fmaf(OK_M2[4], l1, OK_M2[3] * l0));
     const float hb = fmaf(OK_M2[8], l2, fmaf(OK_M2[7], l1, OK_M2[6] * l0));
-    float h = atan2_fast(hb, ha) * 57.29577951308232f;
-    if (h < 0.0f) h = h + 360.0f;
+    // the hue enters only through its cosine and sine: (a, b) / |(a, b)|.
+    // Where that is 0 / 0 or not finite, the angle itself (atan2 in
+    // degrees on [0, 360), as the reference forms it) and its sine and cosine.
+    float sn, cs;
+    const float n2 = fmaf(ha, ha, hb * hb);
+    if (n2 > 0.0f && n2 < INFINITY) {
+        const float inv = rsqrtf(n2);
+        cs = ha * inv;
+        sn = hb * inv;
+    } else {
+        float h = atan2_fast(hb, ha) * 57.29577951308232f;
+        if (h < 0.0f) h = h + 360.0f;
+        sincos_deg(h, &sn, &cs);
+    }
     float p0 = square_sigmoid(gc0), p1 = square_sigmoid(gc1), p2 = square_sigmoid(gc2);
     float s = 0.2722287168f * p0 + 0.6740817658f * p1 + 0.0536895174f * p2;
     const float s2 = s * s;
@@ -238,8 +250,6 @@ __device__ __forceinline__ void sigmoid(const Op& o, float& r, float& g, float& 
     mv_fma(OK_M2, p0, p1, p2);
     const float cm = sqrtf(p1 * p1 + p2 * p2) * m;
     // (L, C m, h) -> Oklab -> LMS -> ACEScg
-    float sn, cs;
-    sincos_deg(h, &sn, &cs);
     float L = p0, A = cm * cs, B = cm * sn;
     mv_fma(OK_M2I, L, A, B);
     L = L * L * L;

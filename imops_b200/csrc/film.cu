@@ -1618,8 +1618,7 @@ int baseline_forward_impl(float* rgb, int W, int H, const ImopsBaselineFilm* Pp,
 // there is written earlier in the same call.
 // A second stream per device for work that does not depend on the image
 // (the grain fields), forked from and joined back to the caller's stream with
-// events: the grain (one 148 KB block an SM) then runs beside the exposure
-// and the halation row pass, which need the HBM but few SM resources.
+// events: the grain then runs beside the halation row pass.
 struct SideStream {
     bool init = false;
     cudaStream_t side = nullptr;
