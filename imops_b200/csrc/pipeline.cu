@@ -34,7 +34,9 @@ namespace pipe {
 
 // Each image gets one of a few library-owned streams, round robin, so the
 // frames a host submits one after another can overlap on the GPU (one
-// frame's compute with the previous frame's download).
+// frame's compute with the previous frame's download).  Six of them: an
+// upload synchronises its image's stream, and with three a host streaming
+// frames found the download of the frame three back still queued on it.
 //
 // Image buffers come from a memory pool of the library's own per device
 // (the default pool, shared with the rest of the process, is left as it
@@ -43,7 +45,7 @@ namespace pipe {
 // that stream, so an image reuses the buffers of the image that held its
 // stream before it, with no wait on other streams and no growth of the pool
 // that depends on timing.
-constexpr int POOL_STREAMS = 3;
+constexpr int POOL_STREAMS = 6;
 struct DevState {
     bool init = false;
     cudaStream_t streams[POOL_STREAMS] = {};
