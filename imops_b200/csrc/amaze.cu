@@ -247,6 +247,47 @@ __device__ __forceinline__ void for_rb(const P& p, const Geo& g, int r0, int r1,
     }
 }
 
+// The same sites dense over the block's threads: thread t takes sites t,
+// t + NTHREADS, ... in row-major order, so no lane idles at a row's end (the
+// inner stages' rows are 96-112 sites of 128, or 50-56 R/B sites of 64); the
+// row and column advance without a division.  Bayer rows alternate the
+// parity of their R/B columns.
+template <class F>
+__device__ __forceinline__ void for_rect_dense(int r0, int r1, int c0, int c1, F f) {
+    const int w = c1 - c0;
+    if (w <= 0 || r1 <= r0) return;
+    const int n = (r1 - r0) * w, dq = NTHREADS / w, dr = NTHREADS - dq * w;
+    int rr = r0 + (int)threadIdx.x / w, cc = c0 + (int)threadIdx.x % w;
+    for (int k = threadIdx.x; k < n; k += NTHREADS) {
+        f(rr, cc);
+        rr += dq;
+        cc += dr;
+        if (cc >= c1) {
+            cc -= w;
+            rr++;
+        }
+    }
+}
+
+template <class F, class P>
+__device__ __forceinline__ void for_rb_dense(const P& p, const Geo& g, int r0, int r1, int c0, int c1, F f) {
+    const int w = (c1 - c0 + 1) >> 1;  // R/B sites a row (one fewer in rows whose first is at c0 + 1, if odd)
+    if (w <= 0 || r1 <= r0) return;
+    const int par0 = p.cfa.at(g.top + r0, g.left + 2) & 1;
+    const int n = (r1 - r0) * w, dq = NTHREADS / w, dr = NTHREADS - dq * w;
+    int rr = r0 + (int)threadIdx.x / w, k = (int)threadIdx.x % w;
+    for (int j = threadIdx.x; j < n; j += NTHREADS) {
+        const int cc = c0 + (par0 ^ ((rr - r0) & 1)) + 2 * k;
+        if (cc < c1) f(rr, cc);
+        rr += dq;
+        k += dr;
+        if (k >= w) {
+            k -= w;
+            rr++;
+        }
+    }
+}
+
 // R/B sites of rows [8, rr1-8) per thread, for stages that keep their
 // results in registers across a barrier (two-phase in-place updates).
 constexpr int RB_PER_THREAD = (TS - 16) * TSH / NTHREADS + 1;
@@ -884,7 +925,7 @@ __device__ void wave_hvwt(const P& p, const Geo& g, const Bufs& b) {
 // reads them.
 template <class P>
 __device__ void st_green_rb(const P& p, const Geo& g, const Bufs& b) {
-    for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
+    for_rb_dense(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
         const int i = rr * TS + cc;
         // dgrb0 replaces vcd in place; the voted Nyquist sites keep vcd for
         // st_nyquist_green, which stores their dgrb0
@@ -1012,7 +1053,7 @@ __device__ void st_diag_weight(const P& p, const Geo& g, const Bufs& b) {
 // the Nyquist test, into a half array (frees the VCD region).
 template <class P>
 __device__ void st_compact_vcd(const P& p, const Geo& g, const Bufs& b) {
-    for_rb(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
+    for_rb_dense(p, g, 8, g.rr1 - 8, 8, g.cc1 - 8, [&](int rr, int cc) {
         const int i = rr * TS + cc;
         b.vcd_rb[i >> 1] = b.vcd[i];
     });
@@ -1114,7 +1155,7 @@ __device__ void wave_pmwt(const P& p, const Geo& g) {
 template <class P>
 __device__ void st_green_refine(const P& p, const Geo& g, const Bufs& b) {
     const float eps = 1e-5f, arth = 0.75f;
-    for_rb(p, g, 12, g.rr1 - 12, 12, g.cc1 - 12, [&](int rr, int cc) {
+    for_rb_dense(p, g, 12, g.rr1 - 12, 12, g.cc1 - 12, [&](int rr, int cc) {
         int i = rr * TS + cc, h = i >> 1;
         if (!(fabsf(0.5f - b.pmwt[h]) >= fabsf(0.5f - b.hvwt[h]))) {
             b.rg[h] = b.mos[i] + b.dgrb0[h];  // rgbgreen as st_green_rb / st_nyquist_green left it
@@ -1185,7 +1226,7 @@ __device__ void st_chroma(const P& p, const Geo& g, const Bufs& b) {
         }
     }
     __syncthreads();
-    for_rb(p, g, 14, g.rr1 - 14, 14, g.cc1 - 14, [&](int rr, int cc) {
+    for_rb_dense(p, g, 14, g.rr1 - 14, 14, g.cc1 - 14, [&](int rr, int cc) {
         int i = rr * TS + cc;
         int which = 1 - (p.cfa.at(g.top + rr, g.left + cc) / 2);
         float* d = which == 0 ? b.dgrb0 : b.dgrb1;
@@ -1207,7 +1248,7 @@ __device__ void st_chroma(const P& p, const Geo& g, const Bufs& b) {
 // demosaic.rs:1254-1366; the epilogue receives (row, col, r, g, b).
 template <class Epi, class P>
 __device__ void st_output(const P& p, const Geo& g, const Bufs& b, const Epi& epi) {
-    for_rect(16, g.rr1 - 16, 16, g.cc1 - 16, [&](int rr, int cc) {
+    for_rect_dense(16, g.rr1 - 16, 16, g.cc1 - 16, [&](int rr, int cc) {
         int row = rr + g.top, col = cc + g.left;
         if (!(col >= 0 && col < p.W && row >= 0 && row < p.H)) return;
         int i = rr * TS + cc;
