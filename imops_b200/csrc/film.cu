@@ -833,8 +833,10 @@ struct Base81 {
 // tap order as in blur_cols), then per pixel the exposure of the three layers
 // from its RGB, the logistic curves, grain and the 81-bin scan with its
 // tables as parameter-bank operands; the result replaces the pixel's RGB
-// (each pixel is read, a step ahead, and written by the same thread).
-__global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS) scan81_fused_kernel(
+// (each pixel is read, a step ahead, and written by the same thread).  Four
+// blocks an SM (64 registers a thread): the scan is bound by the MUFU, and
+// 32 warps keep more of its exponentials in flight than 24.
+__global__ void __launch_bounds__(R64_COL_TW * R64_COL_GROUPS, 4) scan81_fused_kernel(
     const float* __restrict__ hr, const float* __restrict__ noise, const double* __restrict__ sumsq, int W, int H,
     const __grid_constant__ Base81 c, float* __restrict__ rgb) {
     static_assert(HAL_R == R64, "the fused scan's column pass is the radius-64 window");
