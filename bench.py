@@ -538,7 +538,9 @@ def main():
         if errors:
             raise errors[0]
 
-    e2e_batch(3)
+    # warm-up: a frame on each of the library's image streams (six a device),
+    # so that every stream's film working set exists before the timed frames
+    e2e_batch(6)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()

@@ -105,27 +105,31 @@ StreamCache::StreamCache(const char* what) : what_(what) {
     caches().push_back(this);
 }
 
+// Buffers are allocated and replaced in stream order (cudaMallocAsync /
+// cudaFreeAsync on s): unlike cudaMalloc, neither waits for the work
+// already queued on the device, so the first call on a stream, or a larger
+// image, does not stall frames in flight on other streams.  Work on other
+// streams that uses the buffer is ordered after s with events.
 int StreamCache::get(cudaStream_t s, size_t bytes, void** out) {
     if (fault_injected("alloc")) return fail(IMOPS_ERR_OUT_OF_MEMORY, std::string("injected allocation failure (") + what_ + ")");
     int dev = 0;
     IMOPS_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
-    const std::string m = std::string("cudaMalloc(") + what_ + ")";
+    const std::string m = std::string("cudaMallocAsync(") + what_ + ")";
     std::lock_guard<std::mutex> lock(mu_);
     for (auto& e : v_)
         if (e.dev == dev && e.s == s) {
             if (e.bytes < bytes) {
-                IMOPS_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-                IMOPS_CUDA_TRY(cudaFree(e.p), "cudaFree");
+                IMOPS_CUDA_TRY(cudaFreeAsync(e.p, s), "cudaFreeAsync");
                 e.p = nullptr;
                 e.bytes = 0;
-                IMOPS_CUDA_TRY(cudaMalloc(&e.p, bytes), m.c_str());
+                IMOPS_CUDA_TRY(cudaMallocAsync(&e.p, bytes, s), m.c_str());
                 e.bytes = bytes;
             }
             *out = e.p;
             return IMOPS_OK;
         }
     void* p = nullptr;
-    IMOPS_CUDA_TRY(cudaMalloc(&p, bytes), m.c_str());
+    IMOPS_CUDA_TRY(cudaMallocAsync(&p, bytes, s), m.c_str());
     v_.push_back({dev, s, p, bytes});
     *out = p;
     return IMOPS_OK;
