@@ -288,6 +288,41 @@ __device__ __forceinline__ void for_rb_dense(const P& p, const Geo& g, int r0, i
     }
 }
 
+// The R/B sites of rows [r0, r1) x cols [c0, c1) (c0 even) numbered densely
+// in row-major order, for stages whose threads keep per-site values in
+// registers across a barrier: site k of the enumeration is row r0 + k / w,
+// R/B column k % w of it, the division a multiply-high by ceil(2^32 / w)
+// (exact for k < 2^16 and w <= 64).
+struct RbDense {
+    int r0, c0, c1, w, n, par0;
+    unsigned magic;
+};
+
+template <class P>
+__device__ __forceinline__ RbDense rb_dense(const P& p, const Geo& g, int r0, int r1, int c0, int c1) {
+    RbDense d;
+    const int w = (c1 - c0 + 1) >> 1;
+    d.r0 = r0;
+    d.c0 = c0;
+    d.c1 = c1;
+    d.w = w > 0 ? w : 1;
+    d.n = (w > 0 && r1 > r0) ? (r1 - r0) * w : 0;
+    d.par0 = p.cfa.at(g.top + r0, g.left + 2) & 1;
+    d.magic = 0xFFFFFFFFu / (unsigned)d.w + 1u;
+    return d;
+}
+
+// Flat index of site k, or false past the end (or the one missing site of
+// the rows with fewer).
+__device__ __forceinline__ bool rb_dense_site(const RbDense& d, int k, int& i) {
+    if (k >= d.n) return false;
+    const int q = (int)__umulhi((unsigned)k, d.magic), kk = k - q * d.w;
+    const int cc = d.c0 + (d.par0 ^ (q & 1)) + 2 * kk;
+    if (cc >= d.c1) return false;
+    i = (d.r0 + q) * TS + cc;
+    return true;
+}
+
 // R/B sites of rows [8, rr1-8) per thread, for stages that keep their
 // results in registers across a barrier (two-phase in-place updates).
 constexpr int RB_PER_THREAD = (TS - 16) * TSH / NTHREADS + 1;
@@ -1109,36 +1144,31 @@ __device__ __forceinline__ void diag_rb(const float* m, int i, float clip, float
 // warps 0 and 1 run the weight wavefronts, keep them in registers, and form
 // rbint once the wavefronts are done.
 constexpr int RB_WORKERS = NTHREADS - 64;
-constexpr int RB_SLOTS = ((TS - 20) * TSH + RB_WORKERS - 1) / RB_WORKERS;
+constexpr int RB_SLOTS = ((TS - 20) * ((TS - 20) / 2) + RB_WORKERS - 1) / RB_WORKERS;
 
-template <class P>
-__device__ __forceinline__ bool rb_slot(const P& p, const Geo& g, int s, int& i) {
-    const int k = (int)threadIdx.x - 64 + s * RB_WORKERS;
-    if (k >= (g.rr1 - 20) * TSH) return false;
-    const int rr = 10 + (k >> 6);
-    const int cc = 10 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k & (TSH - 1));
-    if (cc >= g.cc1 - 10) return false;
-    i = rr * TS + cc;
-    return true;
+__device__ __forceinline__ bool rb_slot(const RbDense& d, int s, int& i) {
+    return rb_dense_site(d, (int)threadIdx.x - 64 + s * RB_WORKERS, i);
 }
 
 template <class P>
 __device__ void st_rb_early(const P& p, const Geo& g, const Bufs& b, float (&rbm)[RB_SLOTS], float (&rbp)[RB_SLOTS]) {
+    const RbDense d = rb_dense(p, g, 10, g.rr1 - 10, 10, g.cc1 - 10);
 #pragma unroll
     for (int s = 0; s < RB_SLOTS; s++) {
         int i;
         rbm[s] = rbp[s] = 0.0f;
-        if (rb_slot(p, g, s, i)) diag_rb(b.mos, i, p.clip, rbm[s], rbp[s]);
+        if (rb_slot(d, s, i)) diag_rb(b.mos, i, p.clip, rbm[s], rbp[s]);
     }
 }
 
 template <class P>
 __device__ void st_rbint_late(const P& p, const Geo& g, const Bufs& b, const float (&rbm)[RB_SLOTS],
                               const float (&rbp)[RB_SLOTS]) {
+    const RbDense d = rb_dense(p, g, 10, g.rr1 - 10, 10, g.cc1 - 10);
 #pragma unroll
     for (int s = 0; s < RB_SLOTS; s++) {
         int i;
-        if (!rb_slot(p, g, s, i)) continue;
+        if (!rb_slot(d, s, i)) continue;
         const float pm = b.pmwt[i >> 1];
         b.rbint[i >> 1] = (b.mos[i] + rbm[s] * (1.0f - pm) + rbp[s] * pm) * 0.5f;
     }
