@@ -121,6 +121,10 @@ constexpr int DS = T + 2;          // difference planes: radius 1
 constexpr int THREADS = 512;
 constexpr int OUT = T * T / THREADS;  // outputs a thread
 __constant__ int OFF[4] = {1, S, S + 1, S - 1};  // frame step of each direction
+// 1/n for the method's counts n (the specification multiplies by these
+// instead of dividing), each rounded once to f32; index 0 is unused
+__constant__ float RECIP[9] = {1.0f,        1.0f,        1.0f / 2.0f, 1.0f / 3.0f, 1.0f / 4.0f,
+                               1.0f / 5.0f, 1.0f / 6.0f, 1.0f / 7.0f, 1.0f / 8.0f};
 
 // Colour facts of a site, by its phase in the 6x6 period (a cell of the
 // frame whose neighbourhood lies inside the image, which every cell an
@@ -237,8 +241,8 @@ __device__ __forceinline__ float green1_f(const Frame& F, int f, int d, int off)
     const int kp = p1 ? 1 : (p2 ? 2 : 0), km = m1 ? 1 : (m2 ? 2 : 0);
     const float vp1 = F.m[f + off], vp2 = F.m[f + 2 * off], vm1 = F.m[f - off], vm2 = F.m[f - 2 * off];
     const float a = p1 ? vp1 : (p2 ? vp2 : 0.0f), b = m1 ? vm1 : (m2 ? vm2 : 0.0f);
-    const float both = (a * (float)km + b * (float)kp) / (float)(kp + km > 0 ? kp + km : 1);
-    const float mean = sum / (float)(cnt > 0 ? cnt : 1);
+    const float both = (a * (float)km + b * (float)kp) * RECIP[kp + km];
+    const float mean = sum * RECIP[cnt];
     const float g = (kp && km) ? both : (kp ? a : (km ? b : (cnt ? mean : F.m[f])));
     return (M & 3ull) == 1ull ? F.m[f] : clampg(g, lo, hi, cnt);
 }
@@ -265,8 +269,8 @@ __device__ __forceinline__ void rb_f(const Frame& F, const float* G, int f, floa
                 sbl = sbl + (F.m[j] - G[j]);
             }
         const float g = G[f];
-        R = own == 0 ? F.m[f] : (nr ? g + sr / (float)nr : g);
-        B = own == 2 ? F.m[f] : (nb ? g + sbl / (float)nb : g);
+        R = own == 0 ? F.m[f] : (nr ? g + sr * RECIP[nr] : g);
+        B = own == 2 ? F.m[f] : (nb ? g + sbl * RECIP[nb] : g);
         return;
     }
     const unsigned long long M = F.masks[F.ph[f]];
@@ -284,7 +288,7 @@ __device__ __forceinline__ void rb_f(const Frame& F, const float* G, int f, floa
     const int nr = __popc(mr), nb = __popc(mb);
     const int own = (int)(M & 3ull);
     const float g = G[f];
-    const float qr = sr / (float)(nr > 0 ? nr : 1), qb = sbl / (float)(nb > 0 ? nb : 1);
+    const float qr = sr * RECIP[nr], qb = sbl * RECIP[nb];
     R = own == 0 ? F.m[f] : (nr ? g + qr : g);
     B = own == 2 ? F.m[f] : (nb ? g + qb : g);
 }
@@ -459,9 +463,9 @@ __global__ void __launch_bounds__(THREADS, 2) tile_kernel(const __grid_constant_
         const int fc = (ty + 9) * S + tx + 9;
         const int own = (int)(F.masks[F.ph[fc]] & 3ull);
         float* po = out + 3 * ((size_t)y * im.W + x);
-        po[0] = own == 0 ? F.m[fc] : s0 / (float)cnt;
-        po[1] = own == 1 ? F.m[fc] : s1 / (float)cnt;
-        po[2] = own == 2 ? F.m[fc] : s2 / (float)cnt;
+        po[0] = own == 0 ? F.m[fc] : s0 * RECIP[cnt];
+        po[1] = own == 1 ? F.m[fc] : s1 * RECIP[cnt];
+        po[2] = own == 2 ? F.m[fc] : s2 * RECIP[cnt];
     }
 }
 

@@ -25,6 +25,9 @@
  *  2. red / blue: at a site of that colour C_d = m; elsewhere
  *     G_d + the mean of (m - G_d) over the 3x3 sites of that colour
  *     (rows then columns), or G_d if there are none.
+ *  Every division by a count n here and in the vote is a product with
+ *  XT_RECIP[n], 1/n rounded to the working precision: one multiply on the
+ *  GPU instead of an IEEE division, the same value on both sides.
  *  3. green refinement at R/B sites (colour c): the colour difference
  *     K = ((C_d - G_d)(p + s_d) + (C_d - G_d)(p - s_d)) * 0.5 of plane c,
  *     G_d = clamp(m - K, min, max) as in step 1.
@@ -53,6 +56,11 @@
 
 static const int XT_DY[4] = {0, 1, 1, 1};
 static const int XT_DX[4] = {1, 0, 1, -1};
+
+/* 1/n for the counts of the method (at most 8 sites of a colour in a 3x3
+ * window), each rounded once to the working precision; index 0 is unused */
+static const real XT_RECIP[9] = {K(1.0),         K(1.0),         K(1.0) / K(2.0), K(1.0) / K(3.0), K(1.0) / K(4.0),
+                                 K(1.0) / K(5.0), K(1.0) / K(6.0), K(1.0) / K(7.0), K(1.0) / K(8.0)};
 
 typedef struct {
     const real *m;
@@ -115,10 +123,10 @@ static real xt_green1(const XtImg *im, int r, int c, int d)
             b = im->m[xt_at(im, r - k * XT_DY[d], c - k * XT_DX[d])];
         }
     real g;
-    if (kp && km) g = (a * (real)km + b * (real)kp) / (real)(kp + km);
+    if (kp && km) g = (a * (real)km + b * (real)kp) * XT_RECIP[kp + km];
     else if (kp) g = a;
     else if (km) g = b;
-    else g = n ? sum / (real)n : im->m[i];
+    else g = n ? sum * XT_RECIP[n] : im->m[i];
     return xt_clamp(g, lo, hi, n);
 }
 
@@ -136,7 +144,7 @@ static real xt_rb(const XtImg *im, const real *G, int r, int c, int ch)
             s = s + (im->m[j] - G[j]);
             n++;
         }
-    return n ? G[i] + s / (real)n : G[i];
+    return n ? G[i] + s * XT_RECIP[n] : G[i];
 }
 
 /* step 3 */
@@ -306,7 +314,7 @@ int OSYM(oracle_markesteijn3)(const real *m, int W, int H, const OracleCfa *cfa,
                 }
             int hx = hm[0];
             for (int d = 1; d < 4; d++) hx = hm[d] > hx ? hm[d] : hx;
-            int thr = hx - hx / 8, cnt = 0;
+            int thr = hx - hx / 8, cnt = 0;  /* a count, not a division of values */
             real s0 = K(0.0), s1 = K(0.0), s2 = K(0.0);
             for (int d = 0; d < 4; d++) {
                 if (hm[d] < thr) continue;
@@ -315,9 +323,9 @@ int OSYM(oracle_markesteijn3)(const real *m, int W, int H, const OracleCfa *cfa,
                 s2 = s2 + B[d * n + i];
                 cnt++;
             }
-            o[0] = s0 / (real)cnt;
-            o[1] = s1 / (real)cnt;
-            o[2] = s2 / (real)cnt;
+            o[0] = s0 * XT_RECIP[cnt];
+            o[1] = s1 * XT_RECIP[cnt];
+            o[2] = s2 * XT_RECIP[cnt];
             o[ocfa_color(cfa, r, c)] = m[i];  /* the site's own colour is its sample */
         }
     free(buf);
