@@ -355,24 +355,68 @@ __global__ void __launch_bounds__(THREADS, 2) tile_kernel(const __grid_constant_
     }
     __syncthreads();
     // green cells: both green planes hold the sample, which the green
-    // stages would return there; warps 0-2 list the non-green cells of the
-    // green stages' regions in row-major order
+    // stages would return there
     for (int k = threadIdx.x; k < N; k += THREADS)
         if ((msk[phw[k]] & 3ull) == 1ull) F.ga[k] = F.gb[k] = F.m[k];
+    // the non-green cells of the green stages' regions [LO, S - LO)^2, LO =
+    // 2, 4, 6, listed row-major by all warps: each frame row's non-green
+    // bits and per region its count, the rows' offsets (a warp scan per
+    // region), then each row's entries.  The difference planes, not used
+    // before the first direction's last stage, hold the row tables.
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned* rowbal = reinterpret_cast<unsigned*>(F.d);  // [S][2]: columns 0-31, 32-49
+    int* rowcnt = reinterpret_cast<int*>(F.d) + 2 * S;    // [3][S]
+    int* rowoff = rowcnt + 3 * S;                          // [3][S]
+    // the columns [lo, S - lo) among 32 starting at 32 * chunk
+    auto regmask = [](int lo, int chunk) -> unsigned {
+        const int a = max(lo - 32 * chunk, 0), b = min(S - lo - 32 * chunk, 32);
+        if (b <= a) return 0u;
+        return (b >= 32 ? 0xffffffffu : ((1u << b) - 1u)) & ~((1u << a) - 1u);
+    };
+    for (int fy = warp; fy < S; fy += THREADS / 32) {
+        const bool g0 = (msk[phw[fy * S + lane]] & 3ull) != 1ull;
+        const bool g1 = 32 + lane < S && (msk[phw[fy * S + 32 + lane]] & 3ull) != 1ull;
+        const unsigned b0 = __ballot_sync(0xffffffffu, g0), b1 = __ballot_sync(0xffffffffu, g1);
+        if (lane == 0) {
+            rowbal[2 * fy] = b0;
+            rowbal[2 * fy + 1] = b1;
+        }
+        if (lane < 3) {
+            const int lo = 2 + 2 * lane;
+            rowcnt[lane * S + fy] =
+                (fy >= lo && fy < S - lo) ? __popc(b0 & regmask(lo, 0)) + __popc(b1 & regmask(lo, 1)) : 0;
+        }
+    }
+    __syncthreads();
     if (warp < 3) {
-        const int lo = 2 + 2 * warp, w = S - 2 * lo;
-        uint16_t* list = ngl + (warp == 0 ? 0 : (warp == 1 ? NL0 : NL0 + NL1));
-        int n = 0;
-        for (int fy = lo; fy < S - lo; fy++)
-            for (int c0 = 0; c0 < w; c0 += 32) {
-                const int f = fy * S + lo + c0 + lane;
-                const bool ng = c0 + lane < w && (msk[phw[f]] & 3ull) != 1ull;
-                const unsigned bal = __ballot_sync(0xffffffffu, ng);
-                if (ng) list[n + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)f;
-                n += __popc(bal);
+        const int* rc = rowcnt + warp * S;
+        const int a = rc[lane], b = 32 + lane < S ? rc[32 + lane] : 0;
+        int sa = a, sb = b;  // inclusive scans of rows 0-31 and 32-49
+        for (int o = 1; o < 32; o <<= 1) {
+            const int ua = __shfl_up_sync(0xffffffffu, sa, o), ub = __shfl_up_sync(0xffffffffu, sb, o);
+            if (lane >= o) {
+                sa += ua;
+                sb += ub;
             }
-        if (lane == 0) nng[warp] = n;
+        }
+        const int ta = __shfl_sync(0xffffffffu, sa, 31), tb = __shfl_sync(0xffffffffu, sb, 31);
+        rowoff[warp * S + lane] = sa - a;
+        if (32 + lane < S) rowoff[warp * S + 32 + lane] = ta + sb - b;
+        if (lane == 0) nng[warp] = ta + tb;
+    }
+    __syncthreads();
+    for (int fy = warp; fy < S; fy += THREADS / 32) {
+        const unsigned b0 = rowbal[2 * fy], b1 = rowbal[2 * fy + 1], lt = (1u << lane) - 1u;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const int lo = 2 + 2 * q;
+            if (fy < lo || fy >= S - lo) continue;
+            const unsigned m0 = b0 & regmask(lo, 0), m1 = b1 & regmask(lo, 1);
+            uint16_t* list = ngl + (q == 0 ? 0 : (q == 1 ? NL0 : NL0 + NL1));
+            const int base = rowoff[q * S + fy];
+            if ((m0 >> lane) & 1u) list[base + __popc(m0 & lt)] = (uint16_t)(fy * S + lane);
+            if ((m1 >> lane) & 1u) list[base + __popc(m0) + __popc(m1 & lt)] = (uint16_t)(fy * S + 32 + lane);
+        }
     }
     float keep[4][3][OUT];
     __syncthreads();
