@@ -98,3 +98,16 @@ def test_other_6x6_cfa_generic_tiles(oracle_lib, gpu):
     ref = oracle_lib.markesteijn3(m, pattern, shift=(1, 2))
     out = im.demosaic_markesteijn3(_gpu(gpu, m), pattern, shift=(1, 2)).cpu().numpy()
     assert np.array_equal(out, ref)
+
+
+def test_other_6x6_cfa_window_masks(oracle_lib, gpu):
+    """A 6x6 CFA with more than four red sites in some 3x3 window (up to eight
+    around the green sites of row 1) is beyond the per-phase site lists, so the
+    red / blue step tests the window masks instead: bit for bit the same
+    method."""
+    import imops_b200 as im
+    pattern = "RRRRRR" "RGRBRG" "RRRRRR" "GBGBGB" "RRRRRR" "BGBGBG"
+    m = synthetic.mosaic_f32(90, 118, seed=6, pattern=pattern)
+    ref = oracle_lib.markesteijn3(m, pattern, shift=(2, 1))
+    out = im.demosaic_markesteijn3(_gpu(gpu, m), pattern, shift=(2, 1)).cpu().numpy()
+    assert np.array_equal(out, ref)
