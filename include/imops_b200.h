@@ -70,8 +70,8 @@ const char *imops_last_error(void);
 const char *imops_version(void);
 
 /* Frees the working sets the stage entry points cache per (device, stream)
- * on the current device (film, adjoint, the fused develop's
- * mosaic buffer), after waiting for the device; the next call allocates
+ * on the current device (film, adjoint, the scaled mosaics of the u16
+ * develop paths), after waiting for the device; the next call allocates
  * again.  No counterpart in the reference (its buffers are Rust Vecs freed
  * with each module).  Call it when no work of this library is in flight on
  * the device from another thread. */
@@ -316,9 +316,9 @@ int imops_film_invert(float *rgb, int w, int h, const ImopsFilmParams *params, i
 /* ---- fused forward -------------------------------------------------------
  * The path Demosaic -> CFACoeffs -> Exp -> CST -> Film (the module chain of
  * run_pixel_pipeline, pichromatic-pipeline/src/pipeline.rs:4-13, with the
- * modules of modules.rs:529-668 and 841-876) as one call: demosaic with the
- * black/white scaling fused into its tile load and WB / exposure / camera CST
- * fused into its output stage, then the film simulation.  Outputs are the
+ * modules of modules.rs:529-668 and 841-876) as one call: the black/white
+ * scaling of the frame, the demosaic with WB / exposure / camera CST fused
+ * into its output stage, then the film simulation.  Outputs are the
  * same as calling the stage entry points one after another. */
 typedef struct {
     int demosaic;           /* IMOPS_DEMOSAIC_AMAZE or IMOPS_DEMOSAIC_MARKESTEIJN */
