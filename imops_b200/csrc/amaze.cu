@@ -320,22 +320,6 @@ struct Team {
     int t, n;
 };
 __device__ __forceinline__ Team whole_block() { return Team{(int)threadIdx.x, NTHREADS}; }
-// warps 1.. of the block, while warp 0 runs a wavefront
-constexpr int WORKERS = NTHREADS - 32;
-__device__ __forceinline__ Team workers() { return Team{(int)threadIdx.x - 32, WORKERS}; }
-__device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, %0;" ::"r"(WORKERS) : "memory"); }
-
-// R/B sites of rows [r0,r1) x cols [c0,c1) split over a team (c0 even).
-template <class F, class P>
-__device__ __forceinline__ void for_rb_team(const P& p, const Geo& g, Team tm, int r0, int r1, int c0, int c1,
-                                            F f) {
-    const int n = (r1 - r0) * TSH;
-    for (int k = tm.t; k < n; k += tm.n) {
-        int rr = r0 + (k >> 6);
-        int cc = c0 + (p.cfa.at(g.top + rr, g.left + 2) & 1) + 2 * (k & (TSH - 1));
-        if (cc < c1) f(rr, cc);
-    }
-}
 
 // The kernel's dynamic shared memory, named at namespace scope so that the
 // wavefronts index it directly (shared-memory loads, not generic ones).
